@@ -1,0 +1,55 @@
+"""Seeded, discretely divergence-free initial velocity fields on the staggered grid.
+
+The reference has no spectral initial condition (it starts from NGA restart
+files, src/data/initial_conditions.py:57-77); this generator produces the
+decaying-turbulence fields the benchmarks use and writes them through the same
+restart path.  Host-side numpy FP64; it is input generation, not hot path.
+
+Recipe (per seed):
+  1. white Gaussian noise per component, ``np.random.default_rng(seed)``;
+  2. shape its DFT to the 3-D energy spectrum E(k) ~ k^4 exp(-2 (k/k0)^2), i.e.
+     amplitude sqrt(E(k) / (4 pi k^2)), zero mean;
+  3. project onto the kernel of the staggered divergence
+     D = sum_d (U_d[i+e_d] - U_d[i]) / h_d, exactly in DFT space:
+     U_d <- U_d - conj(g_d) (sum_e g_e U_e) / sum_e |g_e|^2, g_d = (e^{i theta_d} - 1)/h_d,
+     so the discrete divergence (src/metric/metric_staggered.py:438-453) is zero
+     to round-off;
+  4. rescale so <u^2 + v^2 + w^2>/3 = urms^2.
+"""
+import numpy as np
+
+
+def spectral_velocity(shape, lengths=(2 * np.pi,) * 3, k0=4.0, urms=1.0,
+                      seed=0):
+    """Return (u, v, w) float64 arrays of ``shape`` = (nx, ny, nz), layout
+    [x][y][z] with z contiguous; u on x-faces, v on y-faces, w on z-faces."""
+    nx, ny, nz = (int(n) for n in shape)
+    rng = np.random.default_rng(seed)
+    noise = [rng.standard_normal((nx, ny, nz)) for _ in range(3)]
+    h = [lengths[d] / shape[d] for d in range(3)]
+    # physical wavenumbers (integers for a 2*pi box)
+    kax = [np.fft.fftfreq(shape[d], d=h[d]) * 2 * np.pi for d in range(3)]
+    KX, KY, KZ = np.meshgrid(*kax, indexing="ij")
+    kmag = np.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ek = kmag ** 4 * np.exp(-2.0 * (kmag / k0) ** 2)
+        amp = np.where(kmag > 0, np.sqrt(ek / (4 * np.pi * kmag ** 2)), 0.0)
+    hat = [np.fft.fftn(n) * amp for n in noise]
+    # exact staggered projection
+    th = [2 * np.pi * np.fft.fftfreq(shape[d]) for d in range(3)]
+    TX, TY, TZ = np.meshgrid(*th, indexing="ij")
+    g = [(np.exp(1j * T) - 1.0) / h[d] for d, T in enumerate((TX, TY, TZ))]
+    div = g[0] * hat[0] + g[1] * hat[1] + g[2] * hat[2]
+    g2 = (np.abs(g[0]) ** 2 + np.abs(g[1]) ** 2 + np.abs(g[2]) ** 2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        phi = np.where(g2 > 0, div / g2, 0.0)
+    hat = [hat[d] - np.conj(g[d]) * phi for d in range(3)]
+    vel = [np.real(np.fft.ifftn(a)) for a in hat]
+    e = (np.mean(vel[0] ** 2) + np.mean(vel[1] ** 2) + np.mean(vel[2] ** 2)) / 3
+    s = urms / np.sqrt(e) if e > 0 else 0.0
+    return tuple(np.ascontiguousarray(a * s) for a in vel)
+
+
+def box_lengths(shape, lengths=None):
+    """Periodic box lengths; default is [0, 2*pi]^3."""
+    return tuple(lengths) if lengths is not None else (2 * np.pi,) * 3

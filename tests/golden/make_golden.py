@@ -1,0 +1,254 @@
+"""Generate golden fixtures by running the unmodified reference PyFlow.
+
+Run in a container that has the reference source tree (default
+``/root/reference``, override with PF_REFERENCE_ROOT):
+
+    python tests/golden/make_golden.py
+
+Writes ``tests/golden/*.npz``.  The fixtures pin the CPU oracle
+(oracle/pf_oracle.c) to the reference, and the CUDA path to the oracle.  The
+reference runs on CPU in FP64 through ref_harness.py's single-rank shims.
+
+Fixtures
+--------
+ops_12x16x20.npz   per-operator cases on a non-cubic, anisotropic periodic box:
+                   rhs_NavierStokes.evaluate with constant VISC and with a
+                   variable VISC plus 'tensor' SFS stresses, div_vel,
+                   applyOperator, RK4.step / Euler.step predictors,
+                   solver_bicgstab.solve, vel_corr.
+jacobi_16.npz      solver_jacobi.solve on a cubic 16^3 box (the reference's
+                   Jacobi assumes dx = dy = dz).
+run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
+                   nu = 0.01, dt = 0.005, RK4 + BiCGStab to 1e-10, 5 steps:
+                   final u, v, w, p and per-step max residual, iteration count
+                   and monitor statistics.
+"""
+import os
+import sys
+import types
+import warnings
+
+import numpy as np
+
+warnings.filterwarnings("ignore")
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+sys.path.insert(0, REPO)
+
+import ref_harness as H  # noqa: E402
+
+
+def _state(ns, d, a):
+    return ns.state.state_P(d, np.ascontiguousarray(a).copy())
+
+
+def ops_case(out):
+    import torch
+    nx, ny, nz = 12, 16, 20
+    lengths = (2 * np.pi, 2.1, 3.3)
+    S = H.make_setup(nx, ny, nz, *lengths)
+    ns, d = S.ns, S.decomp
+    rng = np.random.default_rng(1234)
+    # smooth-ish random fields: low-pass filtered noise plus white noise
+    u, v, w = (rng.standard_normal((nx, ny, nz)) for _ in range(3))
+    visc = 0.01 + 0.005 * rng.random((nx, ny, nz))
+    sfs = [0.1 * rng.standard_normal((nx, ny, nz)) for _ in range(6)]
+    mu, rho, dt = 0.01, 1.3, 2.0e-3
+    res = dict(shape=np.array([nx, ny, nz]),
+               spacing=np.array([S.geo.dx, S.geo.dy, S.geo.dz]),
+               u=u, v=v, w=w, visc=visc, sfs=np.stack(sfs),
+               mu=mu, rho=rho, dt=dt)
+
+    class Blank:
+        modelType = "eddyVisc"
+
+    class Tensor:
+        modelType = "tensor"
+
+    # rhs with constant VISC (src/data/domain.py:130-131)
+    VISC = torch.ones(nx + 4, ny + 4, nz + 4, dtype=torch.float64) * mu
+    rhs = ns.velocity.rhs_NavierStokes(d, S.metric, rho, VISC, Blank())
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    rhs.evaluate(su, sv, sw)
+    res["rhs_const"] = np.stack([rhs.rhs_u.numpy(), rhs.rhs_v.numpy(),
+                                 rhs.rhs_w.numpy()])
+    # rhs with variable VISC + tensor SFS
+    m = Tensor()
+    for nm, a in zip(["FXX", "FYY", "FZZ", "FXY", "FXZ", "FYZ"], sfs):
+        setattr(m, nm, H.padded(d, a))
+    rhs2 = ns.velocity.rhs_NavierStokes(d, S.metric, rho, H.padded(d, visc), m)
+    rhs2.evaluate(su, sv, sw)
+    res["rhs_visc_sfs"] = np.stack([rhs2.rhs_u.numpy(), rhs2.rhs_v.numpy(),
+                                    rhs2.rhs_w.numpy()])
+    # divergence and Laplacian
+    dv = torch.zeros(nx, ny, nz, dtype=torch.float64)
+    S.metric.div_vel(su, sv, sw, dv)
+    res["div"] = dv.numpy().copy()
+    P = ns.pressure.Pressure_Base(d, S.metric)
+    B = torch.zeros(nx, ny, nz, dtype=torch.float64)
+    P.applyOperator(H.padded(d, u), B)
+    res["lap_u"] = B.numpy().copy()
+
+    # RK4 and Euler predictors (constant VISC)
+    class RHSSet:
+        pass
+
+    rs = RHSSet()
+    rs.rhs1, rs.rhs2, rs.rhs3, rs.rhs4 = (
+        ns.velocity.rhs_NavierStokes(d, S.metric, rho, VISC, Blank())
+        for _ in range(4))
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    tu, tv, tw = (_state(ns, d, a) for a in (u, v, w))
+    ns.advancer.RK4(su, tu, sv, tv, sw, tw, rs).step(dt)
+    res["rk4"] = np.stack([su.interior().numpy(), sv.interior().numpy(),
+                           sw.interior().numpy()])
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    ns.advancer.Euler(su, sv, sw, rs).step(dt)
+    res["euler"] = np.stack([su.interior().numpy(), sv.interior().numpy(),
+                             sw.interior().numpy()])
+
+    # BiCGStab on the divergence of the RK4 predictor, then the projection
+    pu, pv, pw = res["rk4"]
+    su, sv, sw = (_state(ns, d, a) for a in (pu, pv, pw))
+    src = torch.zeros(nx, ny, nz, dtype=torch.float64)
+    S.metric.div_vel(su, sv, sw, src)
+    res["bicg_source"] = src.numpy().copy()
+    p0 = 0.1 * rng.standard_normal((nx, ny, nz))
+    res["p0"] = p0
+    sDP = _state(ns, d, np.zeros((nx, ny, nz)))
+    sp = _state(ns, d, p0)
+    iters = [0]
+    orig = P.__class__.applyOperator
+
+    def counting(self, A, Bo):
+        iters[0] += 1
+        return orig(self, A, Bo)
+
+    solver = ns.pressure.solver_bicgstab(S.comms, d, S.metric, S.geo, rho, dt,
+                                         1e-10, 500)
+    solver.pressure.applyOperator = types.MethodType(counting, solver.pressure)
+    r = solver.solve(sDP, sp, src)
+    res["bicg_DP"] = sDP.interior().numpy().copy()
+    res["bicg_p"] = sp.interior().numpy().copy()
+    res["bicg_max_res"] = float(r)
+    res["bicg_iters"] = iters[0] // 2
+    S.metric.grad_P(sDP)
+    su.vel_corr(sDP.grad_x, dt / rho)
+    sv.vel_corr(sDP.grad_y, dt / rho)
+    sw.vel_corr(sDP.grad_z, dt / rho)
+    res["corr"] = np.stack([su.interior().numpy(), sv.interior().numpy(),
+                            sw.interior().numpy()])
+    np.savez_compressed(os.path.join(out, "ops_12x16x20.npz"), **res)
+    print("ops: bicgstab iters", res["bicg_iters"], "max_res", r)
+
+
+def jacobi_case(out):
+    import torch
+    n = 16
+    S = H.make_setup(n, n, n, 2 * np.pi, 2 * np.pi, 2 * np.pi)
+    ns, d = S.ns, S.decomp
+    rng = np.random.default_rng(77)
+    src = rng.standard_normal((n, n, n))
+    src -= src.mean()
+    rho, dt, n_it = 1.0, 0.01, 30
+    sDP = _state(ns, d, np.zeros((n, n, n)))
+    sp = _state(ns, d, rng.standard_normal((n, n, n)))
+    solver = ns.pressure.solver_jacobi(S.comms, d, S.metric, S.geo, rho, dt,
+                                       n_it)
+    srcT = torch.from_numpy(src.copy())
+    r = solver.solve(sDP, sp, srcT)
+    np.savez_compressed(
+        os.path.join(out, "jacobi_16.npz"), shape=np.array([n, n, n]),
+        spacing=np.array([S.geo.dx] * 3), source=src, rho=rho, dt=dt,
+        n_it=n_it, DP=sDP.interior().numpy().copy(),
+        p=sp.interior().numpy().copy(), max_res=float(r))
+    print("jacobi: max_res", r)
+
+
+def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005):
+    import torch
+    ns = H.load_reference()
+    import pyflow_b200.initial as ic
+    u0, v0, w0 = ic.spectral_velocity((n, n, n), k0=4.0, urms=1.0, seed=seed)
+    p0 = np.zeros_like(u0)
+    wd = os.path.join(ns.tmp, "run_%d" % n)
+    os.makedirs(wd, exist_ok=True)
+    g = np.linspace(0.0, 2 * np.pi, n + 1)
+    H.write_config(os.path.join(wd, "config"), g, g, g)
+    H.write_restart(os.path.join(wd, "data"), [u0, v0, w0, p0], dt=dt)
+
+    class Cfg:
+        pass
+
+    c = Cfg()
+    c.configName = "restart"
+    c.configFileStr = os.path.join(wd, "config")
+    c.dataFileStr = os.path.join(wd, "data")
+    c.dataFileType = "restart"
+    c.fNameOut = os.path.join(wd, "out")
+    c.numItDataOut = 1000
+    c.nproc_x = c.nproc_y = c.nproc_z = 1
+    c.mu, c.rho = nu, 1.0
+    c.simDt, c.numIt, c.startTime = dt, steps, 0.0
+    c.SFSmodel = "none"
+    c.advancerName, c.equationMode = "RK4", "NS"
+    c.pSolverMode = "bicgstab"
+    c.min_pressure_residual, c.max_pressure_iterations = 1e-10, 1000
+    c.genericOrder = 2
+    c.dtypeTorch, c.dtypeNumpy = torch.float64, np.float64
+    c.plotState, c.numItPlotOut = False, 20
+
+    record = dict(dom=None, max_res=[], iters=[], stats=[])
+    Dom = ns.domain.Domain
+    orig_fs = Dom.forwardStep
+    orig_apply = ns.pressure.Pressure_Base.applyOperator
+    count = [0]
+
+    def apply_counting(self, A, B):
+        count[0] += 1
+        return orig_apply(self, A, B)
+
+    def fs(self, simDt):
+        record["dom"] = self
+        count[0] = 0
+        orig_fs(self, simDt)
+        record["max_res"].append(float(self.max_resP))
+        record["iters"].append(count[0] // 2)
+        u = self.state_u_P.interior()
+        v = self.state_v_P.interior()
+        w = self.state_w_P.interior()
+        st = [float(torch.max(torch.abs(a))) for a in (u, v, w)]
+        tke = float(torch.sum(u ** 2 + v ** 2 + w ** 2)) / float(n ** 3) * 0.5
+        dv = torch.zeros(n, n, n, dtype=torch.float64)
+        self.metric.div_vel(self.state_u_P, self.state_v_P, self.state_w_P, dv)
+        record["stats"].append(st + [tke, float(torch.max(torch.abs(dv)))])
+
+    Dom.forwardStep = fs
+    ns.pressure.Pressure_Base.applyOperator = apply_counting
+    os.environ["PF_FAKE_RANK"] = "1"  # skip rank-0 monitor/restart file output
+    try:
+        ns.PyFlow.run(c)
+    finally:
+        Dom.forwardStep = orig_fs
+        ns.pressure.Pressure_Base.applyOperator = orig_apply
+        os.environ.pop("PF_FAKE_RANK", None)
+    D = record["dom"]
+    np.savez_compressed(
+        os.path.join(out, "run_%d.npz" % n), shape=np.array([n, n, n]),
+        spacing=np.array([2 * np.pi / n] * 3), seed=seed, nu=nu, rho=1.0,
+        dt=dt, steps=steps, u0=u0, v0=v0, w0=w0,
+        u=D.state_u_P.interior().numpy().copy(),
+        v=D.state_v_P.interior().numpy().copy(),
+        w=D.state_w_P.interior().numpy().copy(),
+        p=D.state_p_P.interior().numpy().copy(),
+        max_res=np.array(record["max_res"]), iters=np.array(record["iters"]),
+        stats=np.array(record["stats"]))
+    print("run: iters", record["iters"], "max_res", record["max_res"])
+
+
+if __name__ == "__main__":
+    out = HERE
+    ops_case(out)
+    jacobi_case(out)
+    run_case(out)
