@@ -1,0 +1,146 @@
+/*
+ * pyflow_b200.h -- C ABI of the B200-native PyFlow time-advance hot path.
+ *
+ * All field pointers are DEVICE pointers to ghost-free [nx][ny][nz] arrays
+ * (z contiguous): the interior of the reference's state_P.var
+ * (src/data/state.py:142-146).  Periodic boundaries are index wraps inside the
+ * kernels (the reference's decomp.communicate_border, src/library/parallel.py:301-414).
+ *
+ * Conventions
+ *  - Every entry point is asynchronous on the given stream unless stated.
+ *  - The library never allocates device memory: scratch space is a caller
+ *    buffer of at least pf_workspace_bytes() bytes, 256-byte aligned.
+ *  - Return value: PF_OK or a pf_status code; no C++ exception crosses the ABI.
+ *  - prec: PF_FP64 computes every operator in FP64 in the reference's
+ *    operation order; PF_MIXED keeps the velocity/pressure state in FP64, runs
+ *    fluxes, RK4 stages and the Poisson matvec in FP32, and keeps FP64 for the
+ *    Poisson residual recomputation, the BiCGStab inner products, the
+ *    iterative-refinement outer loop and all global sums.
+ */
+#ifndef PYFLOW_B200_H
+#define PYFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pf_grid {
+    int nx, ny, nz;     /* interior cells */
+    double dx, dy, dz;  /* uniform spacings (geometry.uniform, src/geometry/geometry.py:97-99) */
+} pf_grid;
+
+enum pf_status {
+    PF_OK = 0,
+    PF_ERR_BAD_ARG = 1,     /* null pointer, bad size, workspace too small */
+    PF_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    PF_BREAKDOWN = 3,       /* BiCGStab gamma == 0 or (t,t) == 0 (src/solver/pressure.py:247-248,266-267) */
+    PF_MAXIT = 4,           /* iteration limit reached before the tolerance */
+    PF_NONFINITE = 5,       /* NaN/Inf seen in a residual */
+    PF_STAGNATION = 6       /* mixed-precision refinement stopped improving */
+};
+
+enum pf_prec { PF_FP64 = 0, PF_MIXED = 1 };
+
+/* Result of a Poisson solve (host struct, filled by the synchronous calls). */
+typedef struct pf_solve_info {
+    double max_res;      /* max|r| / max|r0|, the reference's return value */
+    int iterations;      /* BiCGStab iterations (inner iterations for PF_MIXED) */
+    int outer;           /* refinement passes (PF_MIXED), 1 for PF_FP64 */
+    int status;          /* pf_status */
+} pf_solve_info;
+
+int pf_version(void);
+const char* pf_status_string(int status);
+
+/* Scratch bytes needed by pf_rk4_step / pf_bicgstab_solve / pf_forward_step
+ * for this grid and precision. */
+size_t pf_workspace_bytes(const pf_grid* g, int prec);
+
+/* rhs_NavierStokes.evaluate (src/solver/velocity.py:221-355): viscous +
+ * convective staggered fluxes.  visc: NULL for the constant mu
+ * (src/data/domain.py:130-131) or a cell-centred viscosity field; sfs: NULL or
+ * six consecutive cell-centred fields FXX,FYY,FZZ,FXY,FXZ,FYZ of a 'tensor'
+ * SFS model (src/solver/velocity.py:262-267,286-291,310-315).  Fields are
+ * double for PF_FP64, float for PF_MIXED (u,v,w,visc,sfs,rhs all float). */
+int pf_rhs_ns(const pf_grid* g, int prec, const void* u, const void* v,
+              const void* w, const void* visc, double mu, double rho,
+              const void* sfs, void* ru, void* rv, void* rw, void* stream);
+
+/* metric_uniform.div_vel (src/metric/metric_staggered.py:438-453), FP64. */
+int pf_div_vel(const pf_grid* g, const double* u, const double* v,
+               const double* w, double* div, void* stream);
+
+/* Pressure_Base.applyOperator (src/solver/pressure.py:54-84): B = (-vol L) A,
+ * FP64. */
+int pf_laplace_apply(const pf_grid* g, const double* A, double* B,
+                     void* stream);
+
+/* RK4.step (src/solver/advancer.py:75-113) including the reference's stage-4
+ * state u + dt/2 k3; u, v, w (FP64) updated in place.  Euler.step
+ * (src/solver/advancer.py:49-57) when rk4 == 0. */
+int pf_predictor_step(const pf_grid* g, int prec, int rk4, double* u,
+                      double* v, double* w, const double* visc, double mu,
+                      double rho, const double* sfs, double dt, void* ws,
+                      size_t ws_bytes, void* stream);
+
+/* solver_bicgstab.solve (src/solver/pressure.py:196-297) on
+ * (-vol L) DP = -vol rho/dt source, DP0 = 0, stop on max|r|/max|r0| <= min_res
+ * or iterations >= max_it; then p += DP.  source (FP64, the divergence) is not
+ * modified.  Synchronous: returns after the solve with *info filled. */
+int pf_bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
+                      double min_res, int max_it, const double* source,
+                      double* DP, double* p, void* ws, size_t ws_bytes,
+                      void* stream, pf_solve_info* info);
+
+/* solver_jacobi.solve (src/solver/pressure.py:115-161): n_it sweeps of
+ * p <- (sum of neighbours - dx^2 rho/dt source)/6 from p = 0; p holds the last
+ * iterate and pold the one before it; *max_res gets the reference's residual
+ * ratio.  FP64, synchronous. */
+int pf_jacobi_solve(const pf_grid* g, double rho, double dt, int n_it,
+                    const double* source, double* pold, double* p,
+                    void* ws, size_t ws_bytes, void* stream, double* max_res);
+
+/* grad_P + vel_corr (src/metric/metric_staggered.py:390-401,
+ * src/data/state.py:198-211): u_d -= scale * backward difference of DP. */
+int pf_vel_corr(const pf_grid* g, const double* DP, double scale, double* u,
+                double* v, double* w, void* stream);
+
+/* Domain.forwardStep with the SFS model off or 'tensor'
+ * (src/data/domain.py:342-402): predictor, divergence, Poisson solve
+ * (solver 0 = BiCGStab, 1 = Jacobi with max_it sweeps), projection.
+ * Synchronous; *info gets the solve result. */
+int pf_forward_step(const pf_grid* g, int prec, int rk4, int solver,
+                    double* u, double* v, double* w, double* p, double* DP,
+                    const double* visc, double mu, double rho,
+                    const double* sfs, double dt, double min_res, int max_it,
+                    void* ws, size_t ws_bytes, void* stream,
+                    pf_solve_info* info);
+
+/* Per-step monitor statistics (src/core/PyFlow.py:379-395), FP64:
+ * out_dev[0..4] = max|u|, max|v|, max|w|, TKE, max|div u| written to DEVICE
+ * memory (5 doubles) asynchronously. */
+int pf_stats(const pf_grid* g, const double* u, const double* v,
+             const double* w, double* out_dev, void* ws, size_t ws_bytes,
+             void* stream);
+
+/* Optional per-kernel device-time accounting: when enabled, each kernel launch
+ * of the library is bracketed by CUDA events on its stream.  pf_profile_read
+ * waits for pending events and fills up to max_entries records (per kernel
+ * name: launches and summed milliseconds); *count gets the number of names. */
+typedef struct pf_kernel_time {
+    char name[48];
+    long long launches;
+    double ms;
+} pf_kernel_time;
+
+int pf_profile_enable(int enable);
+int pf_profile_read(pf_kernel_time* out, int max_entries, int* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYFLOW_B200_H */

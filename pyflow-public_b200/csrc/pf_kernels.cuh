@@ -1,0 +1,40 @@
+// pf_kernels.cuh -- host-side launchers shared between the library's .cu files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/pyflow_b200.h"
+
+namespace pf {
+
+cudaError_t launch_rhs(const pf_grid* g, int prec, const void* u,
+                       const void* v, const void* w, const void* visc,
+                       double mu, double rho, const void* sfs, void* ru,
+                       void* rv, void* rw, cudaStream_t s);
+
+size_t predictor_ws_bytes(const pf_grid* g, int prec);
+cudaError_t launch_predictor(const pf_grid* g, int prec, int rk4, double* u,
+                             double* v, double* w, const void* visc,
+                             double mu, double rho, const void* sfs,
+                             double dt, void* ws, cudaStream_t s);
+
+size_t poisson_ws_bytes(const pf_grid* g, int prec);
+int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
+                   double min_res, int max_it, const double* source,
+                   double* DP, double* p, void* ws, cudaStream_t s,
+                   pf_solve_info* info);
+int jacobi_solve(const pf_grid* g, double rho, double dt, int n_it,
+                 const double* source, double* pold, double* p, void* ws,
+                 cudaStream_t s, double* max_res);
+
+cudaError_t launch_div(const pf_grid* g, const double* u, const double* v,
+                       const double* w, double* div, cudaStream_t s);
+cudaError_t launch_laplace(const pf_grid* g, const double* A, double* B,
+                           cudaStream_t s);
+cudaError_t launch_vel_corr(const pf_grid* g, const double* DP, double scale,
+                            double* u, double* v, double* w, cudaStream_t s);
+size_t stats_ws_bytes(const pf_grid* g);
+cudaError_t launch_stats(const pf_grid* g, const double* u, const double* v,
+                         const double* w, double* out, void* ws,
+                         cudaStream_t s);
+
+}  // namespace pf

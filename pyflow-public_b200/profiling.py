@@ -1,0 +1,114 @@
+"""Per-kernel device timing and the HBM roofline byte model.
+
+``enable(True)`` makes the library bracket each of its kernel launches with
+CUDA events on the launching stream; ``read()`` returns {kernel: {launches,
+ms}}.  ``roofline()`` turns those times into achieved GB/s with the
+algorithmic (compulsory) bytes each kernel must move per launch: every field
+it reads or writes counted once per cell, stencil neighbours not recounted.
+"""
+import ctypes
+import json
+import os
+
+from . import _lib as L
+
+
+class _KT(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_longlong),
+                ("ms", ctypes.c_double)]
+
+
+_lib = L.lib()
+_lib.pf_profile_enable.argtypes = [ctypes.c_int]
+_lib.pf_profile_enable.restype = ctypes.c_int
+_lib.pf_profile_read.argtypes = [ctypes.POINTER(_KT), ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_int)]
+_lib.pf_profile_read.restype = ctypes.c_int
+
+
+def enable(on=True):
+    _lib.pf_profile_enable(1 if on else 0)
+
+
+def read():
+    cnt = ctypes.c_int(0)
+    _lib.pf_profile_read(None, 0, ctypes.byref(cnt))
+    arr = (_KT * max(1, cnt.value))()
+    _lib.pf_profile_read(arr, cnt.value, ctypes.byref(cnt))
+    return {arr[i].name.decode(): {"launches": int(arr[i].launches),
+                                   "ms": float(arr[i].ms)}
+            for i in range(cnt.value)}
+
+
+def bytes_per_cell(name):
+    """Algorithmic bytes per cell of one launch of ``name``."""
+    f64 = name.endswith("_f64")
+    s = 8 if f64 else 4
+    table = {
+        # BiCGStab phases: A reads pp, vv, res, res0, writes pp', vv';
+        # B reads res, vv', writes t; C reads pp', vv', res, t, x, res0,
+        # writes x, res  -> 17 field passes per iteration
+        "bicg_phase_a": 6 * s, "bicg_phase_b": 3 * s, "bicg_phase_c": 8 * s,
+        # init: read source (f64), write res, res0, zero x, pp0, pp1, vv0, vv1
+        "bicg_init": 8 + 7 * s,
+        # RK4 stages: FP64 state u,v,w (24 B) + stage state / k-sum (3 fields)
+        "rhs_first": 24 + 6 * s, "rhs_mid": 24 + 12 * s,
+        "rhs_last": 24 + 6 * s + 24, "rhs_euler": 48, "rhs_rhs": 6 * s,
+    }
+    for k, v in table.items():
+        if name.startswith(k):
+            return v
+    fixed = {"mixed_b_init": 24, "mixed_update": 20, "mixed_residual": 24,
+             "add_inplace": 24, "div_vel": 32, "vel_corr": 56, "stats": 24,
+             "laplace_apply": 16, "jacobi_sweep": 24, "jacobi_prep": 24,
+             "jacobi_residual": 16}
+    return fixed.get(name)
+
+
+def peaks():
+    """Measured HBM bandwidth (GB/s) of this pool's B200s, with its source."""
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = os.path.join(here, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM bytes of the kernels captured with ncu (committed
+    summary, scaled to cells); {kernel: bytes_per_cell} or {}."""
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = os.path.join(here, "profiles", "dram_bytes_per_cell.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def roofline(ktimes, ncells, prec):
+    """Roofline record of the kernel with the largest total device time."""
+    peak, src = peaks()
+    best = None
+    for name, kt in ktimes.items():
+        b = bytes_per_cell(name)
+        if b is None or kt["launches"] == 0:
+            continue
+        if best is None or kt["ms"] > best[1]["ms"]:
+            best = (name, kt, b)
+    if best is None:
+        return None
+    name, kt, b = best
+    per_launch_ms = kt["ms"] / kt["launches"]
+    achieved = b * ncells / (per_launch_ms * 1e-3) / 1e9
+    tr = traffic_table().get(name)
+    total = sum(k["ms"] for k in ktimes.values())
+    return {"kernel": name, "bound": "hbm", "achieved": achieved,
+            "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": None if tr is None else tr * ncells,
+            "algorithmic_bytes_per_launch": b * ncells,
+            "launch_ms": per_launch_ms, "share_of_device_time": kt["ms"] / total}
