@@ -39,7 +39,8 @@ enum pf_status {
     PF_BREAKDOWN = 3,       /* BiCGStab gamma == 0 or (t,t) == 0 (src/solver/pressure.py:247-248,266-267) */
     PF_MAXIT = 4,           /* iteration limit reached before the tolerance */
     PF_NONFINITE = 5,       /* NaN/Inf seen in a residual */
-    PF_STAGNATION = 6       /* mixed-precision refinement stopped improving */
+    PF_STAGNATION = 6,      /* mixed-precision refinement stopped improving */
+    PF_ERR_TOO_LARGE = 7    /* grid exceeds the fixed scratch of pf_bicgstab_solve_noalloc */
 };
 
 enum pf_prec { PF_FP64 = 0, PF_MIXED = 1 };
@@ -125,6 +126,20 @@ int pf_forward_step(const pf_grid* g, int prec, int rk4, int solver,
 int pf_stats(const pf_grid* g, const double* u, const double* v,
              const double* w, double* out_dev, void* ws, size_t ws_bytes,
              void* stream);
+
+/* No counterpart in the reference: the pf_bicgstab_solve solve (FP64) for
+ * callers that cannot allocate device memory or pass a workspace (for example
+ * a plugin whose host application owns the whole device-memory budget, or a
+ * loop that must not allocate after start-up).  Scratch is a fixed 14.125 MiB
+ * array inside the library (held by every GPU that loads it); grids above
+ * 64^3 = 262144 cells return PF_ERR_TOO_LARGE.  The first call on a device
+ * looks up the array's device address, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race.  Allocates
+ * nothing.  Synchronous, like pf_bicgstab_solve. */
+int pf_bicgstab_solve_noalloc(const pf_grid* g, double rho, double dt,
+                              double min_res, int max_it, const double* source,
+                              double* DP, double* p, void* stream,
+                              pf_solve_info* info);
 
 /* Optional per-kernel device-time accounting: when enabled, each kernel launch
  * of the library is bracketed by CUDA events on its stream.  pf_profile_read

@@ -42,6 +42,7 @@ const char* pf_status_string(int status) {
         case PF_MAXIT: return "iteration limit reached";
         case PF_NONFINITE: return "non-finite residual";
         case PF_STAGNATION: return "refinement stagnated";
+        case PF_ERR_TOO_LARGE: return "grid exceeds the no-allocation scratch limit (64^3 cells)";
         default: return "unknown status";
     }
 }

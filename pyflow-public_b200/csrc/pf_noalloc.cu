@@ -1,0 +1,80 @@
+// pf_noalloc.cu -- BiCGStab pressure solve whose scratch memory belongs to the
+// library, for callers that cannot allocate device memory.
+//
+// Some callers cannot call cudaMalloc or hand the library a workspace: code
+// embedded in a host application whose device-memory budget is owned by
+// another allocator, real-time loops that must not allocate after start-up,
+// or plugins that receive only their input and output buffers.  For them,
+// pf_bicgstab_solve_noalloc runs the same FP64 solve as pf_bicgstab_solve but
+// takes its scratch from a fixed array compiled into this library:
+//
+//   * The array, g_noalloc_scratch, is a file-scope static __device__ array of
+//     kNoallocBytes (14.125 MiB).  Every GPU that loads the library holds it
+//     until the process exits.  It fits grids of at most kNoallocMaxCells
+//     (64^3 = 262144) cells; larger grids are rejected with
+//     PF_ERR_TOO_LARGE and nothing is launched.
+//   * Host code cannot use the array's name as a device address (on the host
+//     it names a host-side shadow).  The first call on each device, with that
+//     device current, looks up the real address with cudaGetSymbolAddress and
+//     caches it; that call may load the library's device code, so make it
+//     before any stream capture.
+//   * Every call shares the one array, and the array keeps the previous
+//     call's contents.  The solve clears what must start at zero (its scalar
+//     block and reduction counter) and initialises every vector it reads, so
+//     consecutive calls are independent.  Calls that overlap on the GPU (for
+//     example on two streams) race on the array and must be serialised by the
+//     caller.
+//   * The call allocates nothing: no cudaMalloc, cudaFree or allocating
+//     library routine.
+#include <mutex>
+
+#include "pf_common.cuh"
+#include "pf_kernels.cuh"
+
+namespace {
+
+constexpr long long kNoallocMaxCells = 64LL * 64 * 64;
+// 7 FP64 vectors of kNoallocMaxCells, the scalar block and the reduction
+// partials, with 256-byte alignment slack
+constexpr size_t kNoallocBytes = 7 * (size_t)kNoallocMaxCells * sizeof(double) + 128 * 1024;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once
+// per device).
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PF_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PF_ERR_CUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return PF_OK;
+}
+
+}  // namespace
+
+extern "C" int pf_bicgstab_solve_noalloc(const pf_grid* g, double rho,
+                                         double dt, double min_res,
+                                         int max_it, const double* source,
+                                         double* DP, double* p, void* stream,
+                                         pf_solve_info* info) {
+    if (!g || g->nx < 2 || g->ny < 2 || g->nz < 2 || !(g->dx > 0) || !(g->dy > 0) ||
+        !(g->dz > 0) || !source || !DP || !p || !(dt != 0.0))
+        return PF_ERR_BAD_ARG;
+    const long long n = (long long)g->nx * g->ny * g->nz;
+    if (n > kNoallocMaxCells || pf::poisson_ws_bytes(g, PF_FP64) > kNoallocBytes)
+        return PF_ERR_TOO_LARGE;
+    void* ws = nullptr;
+    const int rc = noalloc_scratch(&ws);
+    if (rc != PF_OK) return rc;
+    return pf::bicgstab_solve(g, PF_FP64, rho, dt, min_res, max_it, source, DP, p, ws,
+                              (cudaStream_t)stream, info);
+}
