@@ -116,9 +116,19 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def make_fields(wl):
+def make_fields(wl, device=None):
+    """Seeded spectral initial field as float64 numpy arrays (host FFTs up to
+    256^3, device FFTs above)."""
     import pyflow_b200.initial as ic
     n = wl["n"]
+    if n > 256 and device is not None:
+        f = ic.spectral_velocity_device((n, n, n), k0=wl["k0"], urms=1.0,
+                                        seed=wl["seed"], device=device)
+        out = tuple(a.cpu().numpy() for a in f)
+        del f
+        import torch
+        torch.cuda.empty_cache()
+        return out
     u, v, w = ic.spectral_velocity((n, n, n), k0=wl["k0"], urms=1.0,
                                    seed=wl["seed"])
     return u, v, w
@@ -209,7 +219,7 @@ def run_b200(a):
     wl = WORKLOADS[a.workload]
     n = wl["n"]
     sp = (2 * np.pi / n,) * 3
-    u0, v0, w0 = make_fields(wl)
+    u0, v0, w0 = make_fields(wl, dev)
 
     def fresh():
         f = [torch.tensor(x, device=dev) for x in (u0, v0, w0)]

@@ -127,10 +127,25 @@ int pf_stats(const pf_grid* g, const double* u, const double* v,
              const double* w, double* out_dev, void* ws, size_t ws_bytes,
              void* stream);
 
+/* Cell-centred SGS closures (FP64), computed from the cell-centred velocity
+ * gradients of metric_uniform.grad_vel_center
+ * (src/metric/metric_staggered.py:215-268) with periodic wrap:
+ *   model 0: Smagorinsky eddy viscosity out[0] = coef * |S|
+ *            (stress_constCs.eddyVisc, src/sfsmodel/sfsmodel_smagorinsky.py:65-88;
+ *            coef = rho (Cs Delta)^2);
+ *   model 1: gradient-model stresses out[0..5] = coef du_i/dx_k du_j/dx_k for
+ *            ij = xx, yy, zz, xy, xz, yz (residual_stress.update,
+ *            src/sfsmodel/sfsmodel_gradient.py:70-148; coef = dx^2/12);
+ *   model 2: the nine gradients out[0..8] = du/dx, du/dy, du/dz, dv/dx, ...
+ * out holds 1, 6 or 9 consecutive fields. */
+int pf_sgs_closure(const pf_grid* g, int model, const double* u,
+                   const double* v, const double* w, double coef, double* out,
+                   void* stream);
+
 /* No counterpart in the reference: the pf_bicgstab_solve solve (FP64) for
  * callers that cannot allocate device memory or pass a workspace (for example
  * a plugin whose host application owns the whole device-memory budget, or a
- * loop that must not allocate after start-up).  Scratch is a fixed 14.125 MiB
+ * loop that must not allocate after start-up).  Scratch is a fixed 16.25 MiB
  * array inside the library (held by every GPU that loads it); grids above
  * 64^3 = 262144 cells return PF_ERR_TOO_LARGE.  The first call on a device
  * looks up the array's device address, so make it before any stream capture.

@@ -59,6 +59,7 @@ def _load():
         "pf_forward_step": ([G, I, I, I, P, P, P, P, P, P, D, D, P, D, D, I, P,
                              S, P, ctypes.POINTER(SolveInfo)], I),
         "pf_stats": ([G, P, P, P, P, P, S, P], I),
+        "pf_sgs_closure": ([G, I, P, P, P, D, P, P], I),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

@@ -57,9 +57,15 @@ __device__ inline double block_sum(double v, double* sh) {
     return r;  // valid in thread 0
 }
 
+// max that propagates NaN (a NaN residual must stop the solver, not hide)
+__device__ inline double nanmax(double a, double b) {
+    return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000LL) : fmax(a, b);
+}
+
+// block-wide max of non-negative values; a NaN anywhere gives NaN
 template <int NT>
 __device__ inline double block_max(double v, double* sh) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int wid = tid >> 5;
     if ((tid & 31) == 0) sh[wid] = v;
@@ -67,17 +73,10 @@ __device__ inline double block_max(double v, double* sh) {
     double r = 0.0;
     if (tid < 32) {
         r = (tid < NT / 32) ? sh[tid] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+        for (int o = 16; o > 0; o >>= 1) r = nanmax(r, __shfl_down_sync(0xffffffffu, r, o));
     }
     __syncthreads();
     return r;
 }
-
-// max that propagates NaN (a NaN residual must stop the solver, not hide)
-__device__ inline double nanmax(double a, double b) {
-    return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000LL) : fmax(a, b);
-}
-
-template <typename T> struct Vec;  // not used generically
 
 }  // namespace pf

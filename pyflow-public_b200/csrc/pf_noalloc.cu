@@ -9,7 +9,7 @@
 // takes its scratch from a fixed array compiled into this library:
 //
 //   * The array, g_noalloc_scratch, is a file-scope static __device__ array of
-//     kNoallocBytes (14.125 MiB).  Every GPU that loads the library holds it
+//     kNoallocBytes (16.25 MiB).  Every GPU that loads the library holds it
 //     until the process exits.  It fits grids of at most kNoallocMaxCells
 //     (64^3 = 262144) cells; larger grids are rejected with
 //     PF_ERR_TOO_LARGE and nothing is launched.
@@ -34,9 +34,10 @@
 namespace {
 
 constexpr long long kNoallocMaxCells = 64LL * 64 * 64;
-// 7 FP64 vectors of kNoallocMaxCells, the scalar block and the reduction
-// partials, with 256-byte alignment slack
-constexpr size_t kNoallocBytes = 7 * (size_t)kNoallocMaxCells * sizeof(double) + 128 * 1024;
+// the FP64 solve's 8 vectors of kNoallocMaxCells cells plus its scalar block
+// and reduction partials (with alignment slack); the call also checks the
+// exact size the solve needs against this bound at run time
+constexpr size_t kNoallocBytes = 8 * (size_t)kNoallocMaxCells * sizeof(double) + 256 * 1024;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 

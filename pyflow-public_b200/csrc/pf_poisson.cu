@@ -1,23 +1,38 @@
 // pf_poisson.cu -- pressure Poisson solvers, divergence, projection, stats.
 //
-// BiCGStab (solver_bicgstab.solve, src/solver/pressure.py:196-297) runs as
-// three fused kernels per iteration around its three global reductions:
-//   phase A: pp' = (pp - omega vv) beta + res, vv' = A pp', gamma = (vv', res0)
-//   phase B: s = res - alpha vv',             t = A s,     (s,t), (t,t)
-//   phase C: DP += alpha pp' + omega s, res = s - omega t, (res,res0), max|res|
-// A is the 7-point operator of Pressure_Base.applyOperator
-// (src/solver/pressure.py:54-84, coefficients metric_staggered.py:84-102).
-// Phases A and B evaluate their stencil operand on the fly: a block stages
-// one x-plane of the operand (with its y/z halo) in shared memory, computing
-// each value from res/pp/vv as it is loaded, and marches along x keeping the
-// i-1, i, i+1 planes of its own cells in registers.  Old/new pp and vv live in
-// ping-pong buffers chosen by the iteration parity read from device memory.
+// BiCGStab (solver_bicgstab.solve, src/solver/pressure.py:196-297) with the
+// operator of Pressure_Base.applyOperator (src/solver/pressure.py:54-84,
+// coefficients metric_staggered.py:84-102) runs as TWO fused kernels per
+// iteration, one per remaining global reduction:
 //
-// All scalars (rho1, rho2, alpha, omega, ...) stay in device memory; each
-// reduction is finished by the last block to arrive (fixed summation order,
-// so results are bitwise reproducible run to run), which also evaluates the
-// reference's stop tests and sets a `done` flag that makes every later
-// kernel of the solve return immediately.  The host only polls that flag.
+//   kernel CA (iteration k): finish iteration k-1 and start iteration k
+//     s   = res - alpha vv            (alpha, omega of iteration k-1)
+//     res = s - omega t               (the reference's residual update)
+//     DP += alpha pp + omega s        (two fused multiply-adds, same order)
+//     pp  = (pp - omega vv) beta + res,  beta = alpha rho1 / (rho2 omega)
+//     vv  = A pp,   gamma = (vv, res0),   max|res| -> stop test of k-1
+//   kernel B (iteration k):
+//     s = res - alpha vv,  t = A s,  (s,t), (t,t), (s,res0), (t,res0)
+//     omega = (s,t)/(t,t);  rho1 of iteration k+1 = (s,res0) - omega (t,res0)
+//
+// Every per-element operation is the reference's (same operands, same fused
+// multiply-adds: torch's add_(alpha, x) is one fma); only the scalar rho1 is
+// formed from two dot products instead of (res, res0), which changes its
+// rounding, not its value.  The reference needs three reductions and 17 field
+// passes per iteration; this needs two and 14.
+//
+// Both kernels evaluate their stencil operand on the fly: a block owns a
+// 32 (z) x 8R (y) tile, stages one x-plane of the operand plus its y/z halo in
+// shared memory, and marches along x keeping the i-1, i, i+1 operand values of
+// its own cells in registers.  The raw inputs of plane i+2 (and the halo of
+// plane i+1) are loaded one iteration ahead so each thread keeps 15-30 loads
+// in flight.  pp, vv and res, read at neighbours and rewritten by kernel CA,
+// live in two buffer sets chosen by the parity of a device-side counter.
+//
+// All scalars stay in device memory; each reduction is finished by the last
+// block to arrive (fixed summation order: bitwise reproducible), which also
+// applies the reference's stop tests and sets a `done` flag that makes every
+// later kernel of the solve return immediately.  The host only polls it.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -33,9 +48,13 @@ struct BicgScalars {
     double max_res0, max_res, min_res;
     double scale;      // mixed: max|r| of the current refinement pass
     double max_b;      // mixed: max|b|
-    int iter, done, status, max_it;
+    double true_res;   // mixed: max|b - A x| of the last refinement pass
+    int k;             // index of the next CA kernel
+    int iter;          // completed iterations
+    int done;          // 0 running, 1 stopped, 2 stop after DP += alpha pp
+    int status, max_it;
     unsigned int counter;
-    int pad[3];
+    int pad[2];
 };
 
 template <typename T>
@@ -58,6 +77,13 @@ static LapCoef<T> lap_coef(const pf_grid* g) {
     return c;
 }
 
+// rows of the tile owned by each thread: 4 for FP32, 2 for FP64
+template <typename T>
+struct Rows {
+    static constexpr int R = sizeof(T) == 4 ? 4 : 2;
+    static constexpr int TY = 8 * R;
+};
+
 struct Tiling {
     int ntz, nty, ntx, xc;
     long long ntiles;
@@ -74,14 +100,14 @@ static int num_sms() {
     return n;
 }
 
-static Tiling make_tiling(const Dims& d) {
+static Tiling make_tiling(const Dims& d, int ty) {
     Tiling t;
-    t.ntz = (d.nz + kTileZ - 1) / kTileZ;
-    t.nty = (d.ny + kTileY - 1) / kTileY;
+    t.ntz = (d.nz + 31) / 32;
+    t.nty = (d.ny + ty - 1) / ty;
     const long long yz = (long long)t.ntz * t.nty;
-    const long long want = (long long)num_sms() * 4;  // tiles to fill the GPU
+    const long long want = (long long)num_sms() * 3;  // tiles to fill the GPU
     long long xc = (yz * d.nx) / want;
-    xc = std::max<long long>(4, std::min<long long>(32, xc));
+    xc = std::max<long long>(4, std::min<long long>(64, xc));
     t.xc = (int)std::min<long long>(xc, d.nx);
     t.ntx = (d.nx + t.xc - 1) / t.xc;
     t.ntiles = yz * t.ntx;
@@ -89,7 +115,7 @@ static Tiling make_tiling(const Dims& d) {
 }
 
 static int tiled_grid(const Tiling& t) {
-    return (int)std::min<long long>(t.ntiles, std::min(num_sms() * 6, kMaxPartials));
+    return (int)std::min<long long>(t.ntiles, std::min(num_sms() * 2, kMaxPartials));
 }
 
 static int pointwise_grid(long long n) {
@@ -98,65 +124,124 @@ static int pointwise_grid(long long n) {
 }
 
 // --------------------------------------------------------------------------
-// Tiled 7-point sweep.  load(i,j,k) returns the operand at a cell; epi(i,j,k,
-// centre, Ax) consumes the operator value at each owned cell.  Block: 32 x 8
-// threads, tile 32 (z) x 16 (y) x xc (x); each thread owns rows ty, ty+8.
+// Tiled 7-point sweep with one-plane-ahead prefetch.  The phase object Ph
+// provides
+//   Raw raw(q)  -- loads the operand inputs of cell q,
+//   T   op(raw) -- the stencil operand,
+//   Ext ext(q)  -- loads the epilogue inputs of an owned cell,
+//   epi(q, centre operand, A operand, raw, ext) -- consumes an owned cell.
+// Block: 32 x 8 threads; tile 32 (z) x 8R (y) x xc (x).
 // --------------------------------------------------------------------------
-template <typename T, typename Load, typename Epi>
-__device__ __forceinline__ void sweep_tiles(const Dims& d, const Tiling& tl,
-                                            const LapCoef<T>& cf, Load& load,
-                                            Epi& epi) {
-    __shared__ T sm[kTileY + 2][kTileZ + 2];
-    const int tx = threadIdx.x, ty = threadIdx.y;
+template <typename T, class Ph>
+__device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
+                                      const LapCoef<T>& cf, Ph& ph) {
+    constexpr int R = Ph::R, TY = 8 * Ph::R;
+    using Raw = typename Ph::Raw;
+    using Ext = typename Ph::Ext;
+    __shared__ T sm[TY + 2][34];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const long long plane = (long long)d.ny * d.nz;
     for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int tz = (int)(t % tl.ntz);
-        const long long r = t / tl.ntz;
-        const int tyy = (int)(r % tl.nty);
-        const int txx = (int)(r / tl.nty);
-        const int k0 = tz * kTileZ, j0 = tyy * kTileY, i0 = txx * tl.xc;
+        const long long rr = t / tl.ntz;
+        const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
+        const int k0 = tz * 32, j0 = tyy * TY, i0 = txx * tl.xc;
         const int i1 = min(i0 + tl.xc, d.nx);
-        const int ez = min(kTileZ, d.nz - k0), ey = min(kTileY, d.ny - j0);
-        const int k = k0 + tx;
-        const int jr0 = j0 + ty, jr1 = j0 + ty + 8;
-        const bool v0 = (tx < ez) && (ty < ey), v1 = (tx < ez) && (ty + 8 < ey);
-        T p0 = T(0), p1 = T(0), c0 = T(0), c1 = T(0), n0 = T(0), n1 = T(0);
-        const int im = wrap(i0 - 1, d.nx);
-        if (v0) { p0 = load(im, jr0, k); c0 = load(i0, jr0, k); }
-        if (v1) { p1 = load(im, jr1, k); c1 = load(i0, jr1, k); }
+        const int ez = min(32, d.nz - k0), ey = min(TY, d.ny - j0);
+        bool vr[R];
+        long long off[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int jl = ty + 8 * r;
+            vr[r] = (tx < ez) && (jl < ey);
+            off[r] = (long long)(j0 + jl) * d.nz + (k0 + tx);
+        }
+        // this thread's halo cell of each plane (at most 2*32 + 2*TY cells)
+        bool hv = false;
+        int hy = 0, hz = 0;
+        long long hoff = 0;
+        if (tid < 64) {
+            const int h = tid & 31;
+            hv = h < ez;
+            hz = h + 1;
+            if (tid < 32) { hy = 0; hoff = (long long)wrap(j0 - 1, d.ny) * d.nz + k0 + h; }
+            else { hy = ey + 1; hoff = (long long)wrap(j0 + ey, d.ny) * d.nz + k0 + h; }
+        } else if (tid < 64 + 2 * TY) {
+            const int u = tid - 64, h = u % TY;
+            hv = h < ey;
+            hy = h + 1;
+            if (u < TY) { hz = 0; hoff = (long long)(j0 + h) * d.nz + wrap(k0 - 1, d.nz); }
+            else { hz = ez + 1; hoff = (long long)(j0 + h) * d.nz + wrap(k0 + ez, d.nz); }
+        }
+        T opP[R], opC[R], opN[R];
+        Raw rawC[R], rawN[R];
+        Ext extC[R];
+        Raw hraw{};
+        {
+            const long long bm = (long long)wrap(i0 - 1, d.nx) * plane;
+            const long long b0 = (long long)i0 * plane;
+            const long long b1 = (long long)wrap(i0 + 1, d.nx) * plane;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (vr[r]) {
+                    opP[r] = ph.op(ph.raw(bm + off[r]));
+                    rawC[r] = ph.raw(b0 + off[r]);
+                    rawN[r] = ph.raw(b1 + off[r]);
+                    extC[r] = ph.ext(b0 + off[r]);
+                    opC[r] = ph.op(rawC[r]);
+                }
+            }
+            if (hv) hraw = ph.raw(b0 + hoff);
+        }
         for (int i = i0; i < i1; ++i) {
-            const int ip = wrap(i + 1, d.nx);
-            if (v0) { n0 = load(ip, jr0, k); sm[ty + 1][tx + 1] = c0; }
-            if (v1) { n1 = load(ip, jr1, k); sm[ty + 9][tx + 1] = c1; }
-            if (ty == 0) {
-                if (tx < ez) sm[0][tx + 1] = load(i, wrap(j0 - 1, d.ny), k0 + tx);
-            } else if (ty == 1) {
-                if (tx < ez) sm[ey + 1][tx + 1] = load(i, wrap(j0 + ey, d.ny), k0 + tx);
-            } else if (ty == 2) {
-                if (tx < ey) sm[tx + 1][0] = load(i, j0 + tx, wrap(k0 - 1, d.nz));
-            } else if (ty == 3) {
-                if (tx < ey) sm[tx + 1][ez + 1] = load(i, j0 + tx, wrap(k0 + ez, d.nz));
+            const bool more = i + 1 < i1;
+            const long long bi = (long long)i * plane;
+            const long long bh = (long long)wrap(i + 1, d.nx) * plane;
+            const long long bn = (long long)wrap(i + 2, d.nx) * plane;
+            Raw rawNN[R];
+            Ext extN[R];
+            Raw hrawN{};
+            if (more) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (vr[r]) {
+                        rawNN[r] = ph.raw(bn + off[r]);
+                        extN[r] = ph.ext(bh + off[r]);
+                    }
+                }
+                if (hv) hrawN = ph.raw(bh + hoff);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (vr[r]) sm[ty + 8 * r + 1][tx + 1] = opC[r];
+            if (hv) sm[hy][hz] = ph.op(hraw);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (!vr[r]) continue;
+                opN[r] = ph.op(rawN[r]);
+                const int yy = ty + 8 * r + 1, zz = tx + 1;
+                T b = T(0);
+                b += opP[r] * cf.c[0][0];
+                b += opC[r] * cf.c[0][1];
+                b += opN[r] * cf.c[0][2];
+                b += sm[yy - 1][zz] * cf.c[1][0];
+                b += opC[r] * cf.c[1][1];
+                b += sm[yy + 1][zz] * cf.c[1][2];
+                b += sm[yy][zz - 1] * cf.c[2][0];
+                b += opC[r] * cf.c[2][1];
+                b += sm[yy][zz + 1] * cf.c[2][2];
+                ph.epi(bi + off[r], opC[r], b, rawC[r], extC[r]);
             }
             __syncthreads();
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const bool vq = q ? v1 : v0;
-                if (!vq) continue;
-                const int yy = ty + 8 * q + 1, zz = tx + 1;
-                const T pc = q ? p1 : p0, cc = q ? c1 : c0, nc = q ? n1 : n0;
-                T b = T(0);
-                b += pc * cf.c[0][0];
-                b += cc * cf.c[0][1];
-                b += nc * cf.c[0][2];
-                b += sm[yy - 1][zz] * cf.c[1][0];
-                b += cc * cf.c[1][1];
-                b += sm[yy + 1][zz] * cf.c[1][2];
-                b += sm[yy][zz - 1] * cf.c[2][0];
-                b += cc * cf.c[2][1];
-                b += sm[yy][zz + 1] * cf.c[2][2];
-                epi(i, q ? jr1 : jr0, k, cc, b);
+            for (int r = 0; r < R; ++r) {
+                opP[r] = opC[r];
+                opC[r] = opN[r];
+                rawC[r] = rawN[r];
+                if (more) { rawN[r] = rawNN[r]; extC[r] = extN[r]; }
             }
-            __syncthreads();
-            p0 = c0; c0 = n0; p1 = c1; c1 = n1;
+            if (more) hraw = hrawN;
         }
     }
 }
@@ -188,24 +273,39 @@ __device__ double finish(const double* part, double* sh) {
     return MAX ? block_max<kBlock>(v, sh) : block_sum<kBlock>(v, sh);
 }
 
+__device__ __forceinline__ bool tid0() { return threadIdx.x == 0 && threadIdx.y == 0; }
+
+// Solver vectors.  set 0/1: res, pp, vv written by kernel CA of even/odd k.
+template <typename T>
+struct BicgVecs {
+    T* res[2];
+    T* pp[2];
+    T* vv[2];
+    T *t, *res0;
+};
+
 // ---------------------------------------------------------------- init
 // FP64 path: res = res0 = (source * rho/dt) * (-vol); DP = pp = vv = 0.
 // Mixed inner pass: res = res0 = T(r / scale) where r is the FP64 residual.
+// Writes buffer set 1 (read by the first kernel CA).
 template <typename T, bool FROM_RESIDUAL>
 __global__ void __launch_bounds__(kBlock)
 bicg_init(Dims d, BicgScalars* sc, double* part, const double* src, double c1,
-          double c2, T* res, T* res0, T* xs, T* pp0, T* pp1, T* vv0, T* vv1,
-          int max_it, double min_res) {
+          double c2, BicgVecs<T> v, T* x, int max_it, double min_res) {
     __shared__ double sh[32];
     double s = 0.0, m = 0.0;
     const double inv = FROM_RESIDUAL ? 1.0 / sc->scale : 0.0;
+    T* res = v.res[1];
+    T* pp = v.pp[1];
+    T* vv = v.vv[1];
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += (long long)gridDim.x * blockDim.x) {
         T r;
         if (FROM_RESIDUAL) r = T(src[q] * inv);
         else r = T((src[q] * c1) * c2);
-        res[q] = r; res0[q] = r;
-        xs[q] = T(0); pp0[q] = T(0); pp1[q] = T(0); vv0[q] = T(0); vv1[q] = T(0);
+        res[q] = r;
+        v.res0[q] = r;
+        x[q] = T(0); pp[q] = T(0); vv[q] = T(0); v.t[q] = T(0);
         s += double(r) * double(r);
         m = nanmax(m, fabs(double(r)));
     }
@@ -217,153 +317,179 @@ bicg_init(Dims d, BicgScalars* sc, double* part, const double* src, double c1,
         const double mx = finish<true>(part + kMaxPartials, sh);
         if (threadIdx.x == 0) {
             sc->rho1 = tot; sc->rho2 = 1.0; sc->alpha = 0.0; sc->omega = 1.0;
-            sc->max_res0 = mx; sc->max_res = 0.0; sc->iter = 0; sc->done = 0;
-            sc->status = PF_OK; sc->max_it = max_it; sc->min_res = min_res;
-            sc->counter = 0u;
+            sc->max_res0 = mx; sc->max_res = 0.0; sc->k = 0; sc->iter = 0;
+            sc->done = 0; sc->status = PF_OK; sc->max_it = max_it;
+            sc->min_res = min_res; sc->counter = 0u;
         }
     }
 }
 
-// ---------------------------------------------------------------- phase A
+// ---------------------------------------------------------------- kernel CA
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
-bicg_phase_a(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
-             const T* __restrict__ res, const T* __restrict__ res0, T* pp0,
-             T* pp1, T* vv0, T* vv1) {
+struct PhaseCA {
+    static constexpr int R = 2;
+    const T *res_o, *pp_o, *vv_o, *t, *res0;
+    T *x, *res_n, *pp_n, *vv_n;
+    T alpha, omega, beta;
+    bool fin;  // finish the previous iteration (k > 0)
+    double gam, mx;
+    struct Raw { T r, p, v, t; };
+    struct Ext { T x, r0; };
+    __device__ Raw raw(long long q) const { return Raw{res_o[q], pp_o[q], vv_o[q], t[q]}; }
+    __device__ Ext ext(long long q) const { return Ext{fin ? x[q] : T(0), res0[q]}; }
+    __device__ T resid(const Raw& a) const {
+        if (!fin) return a.r;
+        const T s = fma(-alpha, a.v, a.r);  // s = res; s.sub_(alpha, vv)
+        return fma(-omega, a.t, s);         // res = s; res.sub_(omega, t)
+    }
+    __device__ T op(const Raw& a) const {
+        const T rn = resid(a);
+        T q = fma(-omega, a.v, a.p);        // pp.sub_(omega, vv)
+        q = q * beta;                       // pp.mul_(beta)
+        return q + rn;                      // pp.add_(res)
+    }
+    __device__ void epi(long long q, T c, T b, const Raw& a, const Ext& e) {
+        T rn = a.r;
+        if (fin) {
+            const T s = fma(-alpha, a.v, a.r);
+            rn = fma(-omega, a.t, s);
+            T xv = fma(alpha, a.p, e.x);    // DP.add_(alpha, pp)
+            x[q] = fma(omega, s, xv);       // DP.add_(omega, s)
+        }
+        res_n[q] = rn;
+        pp_n[q] = c;
+        vv_n[q] = b;
+        gam += double(b) * double(e.r0);
+        mx = nanmax(mx, fabs(double(rn)));
+    }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock, 2)
+bicg_ca(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
+        BicgVecs<T> v, T* __restrict__ x) {
     __shared__ double sh[32];
-    if (sc->done) return;
-    const int par = sc->iter & 1;
-    const T* ppo = par ? pp1 : pp0;
-    const T* vvo = par ? vv1 : vv0;
-    T* ppn = par ? pp0 : pp1;
-    T* vvn = par ? vv0 : vv1;
-    const double beta_d = (sc->alpha * sc->rho1) / (sc->rho2 * sc->omega);
-    const T beta = T(beta_d), omega = T(sc->omega);
-    double acc = 0.0;
-    auto load = [&](int i, int j, int k) -> T {
-        const long long q = idx(d, i, j, k);
-        T x = fma(-omega, vvo[q], ppo[q]);  // pp.sub_(omega, vv)
-        x = x * beta;                       // pp.mul_(beta)
-        return x + res[q];                  // pp.add_(res)
-    };
-    auto epi = [&](int i, int j, int k, T c, T b) {
-        const long long q = idx(d, i, j, k);
-        ppn[q] = c;
-        vvn[q] = b;
-        acc += double(b) * double(res0[q]);
-    };
-    sweep_tiles<T>(d, tl, cf, load, epi);
-    const double bs = block_sum<kBlock>(acc, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.x] = bs;
+    const int done = sc->done;
+    if (done == 1) return;
+    const int k = sc->k;
+    const bool odd = k & 1;  // CA(k) writes set k&1 and reads the other
+    if (done == 2) {
+        // (t,t) == 0 breakdown: the reference has applied DP += alpha pp and
+        // stops (src/solver/pressure.py:251,266-267)
+        const T alpha = T(sc->alpha);
+        const T* pp = odd ? v.pp[0] : v.pp[1];
+        const long long nt = (long long)gridDim.x * blockDim.x * blockDim.y;
+        for (long long q = blockIdx.x * (long long)blockDim.x * blockDim.y +
+                           threadIdx.y * blockDim.x + threadIdx.x;
+             q < d.n; q += nt)
+            x[q] = fma(alpha, pp[q], x[q]);
+        if (arrive_last(sc) && tid0()) { sc->done = 1; sc->counter = 0u; }
+        return;
+    }
+    PhaseCA<T> ph;
+    ph.res_o = odd ? v.res[0] : v.res[1];
+    ph.pp_o = odd ? v.pp[0] : v.pp[1];
+    ph.vv_o = odd ? v.vv[0] : v.vv[1];
+    ph.t = v.t; ph.res0 = v.res0; ph.x = x;
+    ph.res_n = odd ? v.res[1] : v.res[0];
+    ph.pp_n = odd ? v.pp[1] : v.pp[0];
+    ph.vv_n = odd ? v.vv[1] : v.vv[0];
+    ph.alpha = T(sc->alpha);
+    ph.omega = T(sc->omega);
+    ph.beta = T((sc->alpha * sc->rho1) / (sc->rho2 * sc->omega));
+    ph.fin = k > 0;
+    ph.gam = 0.0; ph.mx = 0.0;
+    sweep<T>(d, tl, cf, ph);
+    const double bs = block_sum<kBlock>(ph.gam, sh);
+    const double bm = block_max<kBlock>(ph.mx, sh);
+    if (tid0()) { part[blockIdx.x] = bs; part[kMaxPartials + blockIdx.x] = bm; }
     if (arrive_last(sc)) {
         const double gamma = finish<false>(part, sh);
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
-            sc->gamma = gamma;
-            if (gamma == 0.0) {
-                sc->done = 1;
-                sc->status = PF_BREAKDOWN;
-            } else {
-                sc->alpha = sc->rho1 / gamma;
+        const double mxr = finish<true>(part + kMaxPartials, sh);
+        if (tid0()) {
+            bool stop = false;
+            if (k > 0) {
+                // stop tests of iteration k (src/solver/pressure.py:279-287)
+                sc->iter = k;
+                const double mr = mxr / sc->max_res0;
+                sc->max_res = mr;
+                if (!(mr == mr) || isinf(mr)) { stop = true; sc->status = PF_NONFINITE; }
+                else if (mr <= sc->min_res) { stop = true; sc->status = PF_OK; }
+                else if (k >= sc->max_it) { stop = true; sc->status = PF_MAXIT; }
             }
+            if (!stop) {
+                sc->gamma = gamma;
+                if (gamma == 0.0) { stop = true; sc->status = PF_BREAKDOWN; }
+                else sc->alpha = sc->rho1 / gamma;
+            }
+            if (stop) sc->done = 1;
+            sc->k = k + 1;
             sc->counter = 0u;
         }
     }
 }
 
-// ---------------------------------------------------------------- phase B
+// ---------------------------------------------------------------- kernel B
 template <typename T>
-__global__ void __launch_bounds__(kBlock)
-bicg_phase_b(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
-             const T* __restrict__ res, const T* vv0, const T* vv1,
-             T* __restrict__ t) {
+struct PhaseB {
+    static constexpr int R = Rows<T>::R;
+    const T *res, *vv, *res0;
+    T* t;
+    T alpha;
+    double st, tt, sr, tr;
+    struct Raw { T r, v; };
+    struct Ext { T r0; };
+    __device__ Raw raw(long long q) const { return Raw{res[q], vv[q]}; }
+    __device__ Ext ext(long long q) const { return Ext{res0[q]}; }
+    __device__ T op(const Raw& a) const { return fma(-alpha, a.v, a.r); }
+    __device__ void epi(long long q, T c, T b, const Raw&, const Ext& e) {
+        t[q] = b;
+        st += double(c) * double(b);
+        tt += double(b) * double(b);
+        sr += double(c) * double(e.r0);
+        tr += double(b) * double(e.r0);
+    }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock, 2)
+bicg_b(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
+       BicgVecs<T> v) {
     __shared__ double sh[32];
     if (sc->done) return;
-    const int par = sc->iter & 1;
-    const T* vv = par ? vv0 : vv1;  // written by phase A of this iteration
-    const T alpha = T(sc->alpha);
-    double a1 = 0.0, a2 = 0.0;
-    auto load = [&](int i, int j, int k) -> T {
-        const long long q = idx(d, i, j, k);
-        return fma(-alpha, vv[q], res[q]);  // s = res; s.sub_(alpha, vv)
-    };
-    auto epi = [&](int i, int j, int k, T c, T b) {
-        t[idx(d, i, j, k)] = b;
-        a1 += double(c) * double(b);
-        a2 += double(b) * double(b);
-    };
-    sweep_tiles<T>(d, tl, cf, load, epi);
-    const double b1 = block_sum<kBlock>(a1, sh);
-    const double b2 = block_sum<kBlock>(a2, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        part[blockIdx.x] = b1;
-        part[kMaxPartials + blockIdx.x] = b2;
+    const bool odd = (sc->k - 1) & 1;  // set written by the CA kernel just run
+    PhaseB<T> ph;
+    ph.res = odd ? v.res[1] : v.res[0];
+    ph.vv = odd ? v.vv[1] : v.vv[0];
+    ph.res0 = v.res0; ph.t = v.t;
+    ph.alpha = T(sc->alpha);
+    ph.st = ph.tt = ph.sr = ph.tr = 0.0;
+    sweep<T>(d, tl, cf, ph);
+    const double b0 = block_sum<kBlock>(ph.st, sh);
+    const double b1 = block_sum<kBlock>(ph.tt, sh);
+    const double b2 = block_sum<kBlock>(ph.sr, sh);
+    const double b3 = block_sum<kBlock>(ph.tr, sh);
+    if (tid0()) {
+        part[blockIdx.x] = b0;
+        part[kMaxPartials + blockIdx.x] = b1;
+        part[2 * kMaxPartials + blockIdx.x] = b2;
+        part[3 * kMaxPartials + blockIdx.x] = b3;
     }
     if (arrive_last(sc)) {
         const double buf1 = finish<false>(part, sh);
         const double buf2 = finish<false>(part + kMaxPartials, sh);
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const double sr = finish<false>(part + 2 * kMaxPartials, sh);
+        const double tr = finish<false>(part + 3 * kMaxPartials, sh);
+        if (tid0()) {
             sc->buf1 = buf1; sc->buf2 = buf2;
             if (buf2 == 0.0) {
-                sc->done = 2;  // phase C applies DP += alpha pp, then stops
+                sc->done = 2;
                 sc->status = PF_BREAKDOWN;
             } else {
-                sc->omega = buf1 / buf2;
-            }
-            sc->counter = 0u;
-        }
-    }
-}
-
-// ---------------------------------------------------------------- phase C
-template <typename T>
-__global__ void __launch_bounds__(kBlock)
-bicg_phase_c(Dims d, BicgScalars* sc, double* part, T* __restrict__ res,
-             const T* __restrict__ res0, const T* pp0, const T* pp1,
-             const T* vv0, const T* vv1, const T* __restrict__ t,
-             T* __restrict__ x) {
-    __shared__ double sh[32];
-    const int done = sc->done;
-    if (done == 1) return;
-    const int par = sc->iter & 1;
-    const T* pp = par ? pp0 : pp1;
-    const T* vv = par ? vv0 : vv1;
-    const T alpha = T(sc->alpha), omega = T(sc->omega);
-    double s1 = 0.0, m = 0.0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
-         q += (long long)gridDim.x * blockDim.x) {
-        T dp = fma(alpha, pp[q], x[q]);  // DP.add_(alpha, pp)
-        if (done == 0) {
-            const T s = fma(-alpha, vv[q], res[q]);
-            dp = fma(omega, s, dp);             // DP.add_(omega, s)
-            const T r = fma(-omega, t[q], s);   // res = s; res.sub_(omega, t)
-            res[q] = r;
-            s1 += double(r) * double(res0[q]);
-            m = nanmax(m, fabs(double(r)));
-        }
-        x[q] = dp;
-    }
-    const double bs = block_sum<kBlock>(s1, sh);
-    const double bm = block_max<kBlock>(m, sh);
-    if (threadIdx.x == 0) { part[blockIdx.x] = bs; part[kMaxPartials + blockIdx.x] = bm; }
-    if (arrive_last(sc)) {
-        const double rho1 = finish<false>(part, sh);
-        const double mx = finish<true>(part + kMaxPartials, sh);
-        if (threadIdx.x == 0) {
-            if (done == 2) {
-                sc->done = 1;
-            } else {
+                const double omega = buf1 / buf2;
+                sc->omega = omega;
                 sc->rho2 = sc->rho1;
-                sc->rho1 = rho1;
-                const double mr = mx / sc->max_res0;
-                sc->max_res = mr;
-                sc->iter += 1;
-                if (!(mr == mr) || isinf(mr)) {
-                    sc->done = 1; sc->status = PF_NONFINITE;
-                } else if (mr <= sc->min_res) {
-                    sc->done = 1; sc->status = PF_OK;
-                } else if (sc->iter >= sc->max_it) {
-                    sc->done = 1; sc->status = PF_MAXIT;
-                }
+                sc->rho1 = sr - omega * tr;  // (s - omega t, res0)
             }
             sc->counter = 0u;
         }
@@ -392,9 +518,11 @@ mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
     }
 }
 
-// x += scale * e  (FP64 accumulate of the FP32 correction)
+// Refinement update: x += scale * e (FP64 accumulate of a pass's correction,
+// scale = max|r| of the residual the pass solved for).
+template <typename T>
 __global__ void __launch_bounds__(kBlock)
-mixed_update(Dims d, const BicgScalars* sc, const float* e, double* x) {
+fold_correction(Dims d, const BicgScalars* sc, const T* e, double* x) {
     const double s = sc->scale;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += (long long)gridDim.x * blockDim.x)
@@ -402,25 +530,35 @@ mixed_update(Dims d, const BicgScalars* sc, const float* e, double* x) {
 }
 
 // r = b - A x in FP64 and max|r| (the refinement's true residual)
-__global__ void __launch_bounds__(kBlock)
+struct PhaseResidual {
+    static constexpr int R = 2;
+    const double *x, *b;
+    double* r;
+    double mx;
+    struct Raw { double x; };
+    struct Ext { double b; };
+    __device__ Raw raw(long long q) const { return Raw{x[q]}; }
+    __device__ Ext ext(long long q) const { return Ext{b[q]}; }
+    __device__ double op(const Raw& a) const { return a.x; }
+    __device__ void epi(long long q, double, double ax, const Raw&, const Ext& e) {
+        const double v = e.b - ax;
+        r[q] = v;
+        mx = nanmax(mx, fabs(v));
+    }
+};
+
+__global__ void __launch_bounds__(kBlock, 2)
 mixed_residual(Dims d, Tiling tl, LapCoef<double> cf, BicgScalars* sc,
                double* part, const double* __restrict__ b,
                const double* __restrict__ x, double* __restrict__ r) {
     __shared__ double sh[32];
-    double m = 0.0;
-    auto load = [&](int i, int j, int k) -> double { return x[idx(d, i, j, k)]; };
-    auto epi = [&](int i, int j, int k, double c, double ax) {
-        const long long q = idx(d, i, j, k);
-        const double v = b[q] - ax;
-        r[q] = v;
-        m = nanmax(m, fabs(v));
-    };
-    sweep_tiles<double>(d, tl, cf, load, epi);
-    const double bm = block_max<kBlock>(m, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.x] = bm;
+    PhaseResidual ph{x, b, r, 0.0};
+    sweep<double>(d, tl, cf, ph);
+    const double bm = block_max<kBlock>(ph.mx, sh);
+    if (tid0()) part[blockIdx.x] = bm;
     if (arrive_last(sc)) {
         const double mx = finish<true>(part, sh);
-        if (threadIdx.x == 0 && threadIdx.y == 0) { sc->scale = mx; sc->counter = 0u; }
+        if (tid0()) { sc->true_res = mx; sc->scale = mx; sc->counter = 0u; }
     }
 }
 
@@ -433,38 +571,34 @@ add_inplace(long long n, const double* a, double* p) {
 }
 
 // ------------------------------------------------------------ workspace
-struct PoissonWs {
-    BicgScalars* sc;
-    double* part;      // 2 x kMaxPartials
-    void* vec;         // solver vectors
-};
-
 static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+static constexpr int kNumPartials = 4;
 
 size_t poisson_ws_bytes(const pf_grid* g, int prec) {
     const size_t n = (size_t)g->nx * g->ny * g->nz;
-    size_t b = align256(sizeof(BicgScalars)) + align256(2 * kMaxPartials * sizeof(double));
+    size_t b = align256(sizeof(BicgScalars)) +
+               align256(kNumPartials * kMaxPartials * sizeof(double));
     if (prec == PF_FP64) {
-        b += 7 * align256(n * sizeof(double));  // res res0 pp0 pp1 vv0 vv1 t
+        b += 8 * align256(n * sizeof(double));  // res[2] pp[2] vv[2] t res0
     } else {
-        b += 8 * align256(n * sizeof(float));   // + e
-        b += 2 * align256(n * sizeof(double));  // b, r
+        // inner vectors + correction: FP32 passes, or FP64 passes after an
+        // FP32 pass fails (the two sets share one region), then b and r
+        b += 9 * align256(n * sizeof(double));
+        b += 2 * align256(n * sizeof(double));
     }
     return b;
 }
 
 template <typename T>
-struct BicgVecs {
-    T *res, *res0, *pp0, *pp1, *vv0, *vv1, *t;
-};
-
-template <typename T>
 static BicgVecs<T> carve(char*& p, size_t n) {
     BicgVecs<T> v;
-    T** f[7] = {&v.res, &v.res0, &v.pp0, &v.pp1, &v.vv0, &v.vv1, &v.t};
+    T** f[8] = {&v.res[0], &v.res[1], &v.pp[0], &v.pp[1], &v.vv[0], &v.vv[1], &v.t, &v.res0};
     for (auto ptr : f) { *ptr = (T*)p; p += align256(n * sizeof(T)); }
     return v;
 }
+
+static LapCoef<double> cf64(const pf_grid* g) { return lap_coef<double>(g); }
 
 static int read_scalars(BicgScalars* dev, BicgScalars* host, cudaStream_t s) {
     if (cudaMemcpyAsync(host, dev, sizeof(BicgScalars), cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -474,25 +608,30 @@ static int read_scalars(BicgScalars* dev, BicgScalars* host, cudaStream_t s) {
 }
 
 // Enqueue BiCGStab iterations in chunks, polling the device `done` flag
-// between chunks.  Kernels of a finished solve return at once, so the
-// iterations enqueued past convergence cost only their launch.
+// between chunks; kernels of a finished solve return at once.  Launch order:
+// CA(0), then pairs (B(k), CA(k+1)), so every chunk ends with a CA and the
+// last iteration of a chunk is finished before polling.
 template <typename T>
-static int run_iterations(const Dims& d, const Tiling& tl, const LapCoef<T>& cf,
+static int run_iterations(const Dims& d, const LapCoef<T>& cf,
                           BicgScalars* sc, double* part, const BicgVecs<T>& v,
                           T* x, cudaStream_t s, BicgScalars* hs) {
-    const int gt = tiled_grid(tl), gp = pointwise_grid(d.n);
+    const Tiling ta = make_tiling(d, 8 * PhaseCA<T>::R);
+    const Tiling tb = make_tiling(d, 8 * PhaseB<T>::R);
+    const int ga = tiled_grid(ta), gb = tiled_grid(tb);
     dim3 blk2(32, 8);
+    const char* nca = sizeof(T) == 8 ? "bicg_ca_f64" : "bicg_ca_f32";
+    const char* nb = sizeof(T) == 8 ? "bicg_b_f64" : "bicg_b_f32";
+    PF_LAUNCH(nca, s, bicg_ca<T><<<ga, blk2, 0, s>>>(d, ta, cf, sc, part, v, x));
     int chunk = 4;
-    for (int guard = 0; guard < 1 << 20; ++guard) {
+    for (int guard = 0; guard < (1 << 20); ++guard) {
         for (int c = 0; c < chunk; ++c) {
-            PF_LAUNCH(sizeof(T) == 8 ? "bicg_phase_a_f64" : "bicg_phase_a_f32", s, bicg_phase_a<T><<<gt, blk2, 0, s>>>(d, tl, cf, sc, part, v.res, v.res0, v.pp0, v.pp1, v.vv0, v.vv1));
-            PF_LAUNCH(sizeof(T) == 8 ? "bicg_phase_b_f64" : "bicg_phase_b_f32", s, bicg_phase_b<T><<<gt, blk2, 0, s>>>(d, tl, cf, sc, part, v.res, v.vv0, v.vv1, v.t));
-            PF_LAUNCH(sizeof(T) == 8 ? "bicg_phase_c_f64" : "bicg_phase_c_f32", s, bicg_phase_c<T><<<gp, kBlock, 0, s>>>(d, sc, part, v.res, v.res0, v.pp0, v.pp1, v.vv0, v.vv1, v.t, x));
+            PF_LAUNCH(nb, s, bicg_b<T><<<gb, blk2, 0, s>>>(d, tb, cf, sc, part, v));
+            PF_LAUNCH(nca, s, bicg_ca<T><<<ga, blk2, 0, s>>>(d, ta, cf, sc, part, v, x));
         }
         if (cudaGetLastError() != cudaSuccess) return PF_ERR_CUDA;
         const int rc = read_scalars(sc, hs, s);
         if (rc) return rc;
-        if (hs->done) return PF_OK;
+        if (hs->done == 1) return PF_OK;
         chunk = std::min(chunk * 2, 32);
     }
     return PF_ERR_CUDA;
@@ -506,8 +645,7 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
     const size_t n = (size_t)d.n;
     char* ptr = (char*)ws;
     BicgScalars* sc = (BicgScalars*)ptr; ptr += align256(sizeof(BicgScalars));
-    double* part = (double*)ptr; ptr += align256(2 * kMaxPartials * sizeof(double));
-    const Tiling tl = make_tiling(d);
+    double* part = (double*)ptr; ptr += align256(kNumPartials * kMaxPartials * sizeof(double));
     const int gp = pointwise_grid(d.n);
     const double vol = (g->dx * g->dy) * g->dz;
     const double c1 = rho / dt, c2 = -1.0 * vol;
@@ -515,52 +653,82 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
     std::memset(&hs, 0, sizeof(hs));
     if (cudaMemsetAsync(sc, 0, sizeof(BicgScalars), s) != cudaSuccess) return PF_ERR_CUDA;
     pf_solve_info out{0.0, 0, 1, PF_OK};
+    // the reference loop always runs at least one iteration
+    max_it = std::max(max_it, 1);
     if (prec == PF_FP64) {
         BicgVecs<double> v = carve<double>(ptr, n);
         const LapCoef<double> cf = lap_coef<double>(g);
-        PF_LAUNCH("bicg_init_f64", s, bicg_init<double, false><<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, v.res, v.res0, DP,
-                                                       v.pp0, v.pp1, v.vv0, v.vv1, max_it, min_res));
-        // the reference loop always runs at least one iteration
-        int rc = run_iterations<double>(d, tl, cf, sc, part, v, DP, s, &hs);
+        PF_LAUNCH("bicg_init_f64", s, bicg_init<double, false><<<gp, kBlock, 0, s>>>(
+            d, sc, part, source, c1, c2, v, DP, max_it, min_res));
+        int rc = run_iterations<double>(d, cf, sc, part, v, DP, s, &hs);
         if (rc) return rc;
         out.max_res = hs.max_res; out.iterations = hs.iter; out.status = hs.status;
     } else {
-        BicgVecs<float> v = carve<float>(ptr, n);
-        float* e = (float*)ptr; ptr += align256(n * sizeof(float));
+        // Iterative refinement: each pass solves A e = r / max|r| with BiCGStab
+        // on FP32 vectors (FP64 dot products) to kInnerTol, then
+        // x += max|r| e and r = b - A x in FP64, until max|r| / max|b| reaches
+        // the reference's tolerance.  A pass that ends non-finite or in
+        // breakdown is discarded, and a pass that gains less than 2x switches
+        // the solve to FP64 inner passes, so the refinement always converges
+        // like the FP64 solver.
+        char* region = ptr;
+        BicgVecs<float> v32 = carve<float>(ptr, n);
+        float* e32 = (float*)ptr;
+        ptr = region + 9 * align256(n * sizeof(double));
+        char* r64 = region;
+        BicgVecs<double> v64 = carve<double>(r64, n);
+        double* e64 = (double*)r64;
         double* b = (double*)ptr; ptr += align256(n * sizeof(double));
         double* r = (double*)ptr; ptr += align256(n * sizeof(double));
+        const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
         const LapCoef<float> cf = lap_coef<float>(g);
         const LapCoef<double> cfd = lap_coef<double>(g);
-        dim3 blk2(32, 8);
-        const int gt = tiled_grid(tl);
+        const double kInnerTol = 1e-4;
+        const int kMaxOuter = 40;
         PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b, DP));
         if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
         const double max_b = hs.max_b;
-        // inner tolerance relative to the pass's initial residual; FP32
-        // BiCGStab reliably contracts by this much before it stagnates
-        const double inner_tol = 1e-4;
-        const int max_outer = 30;
-        int total = 0, status = PF_OK, outer = 0;
+        int status = PF_OK, outer = 0, total = 0;
+        bool use64 = false;
         double ratio = max_b > 0 ? 1.0 : 0.0, prev_ratio = 2.0;
-        for (;; ++outer) {
+        if (!(max_b == max_b)) status = PF_NONFINITE;
+        while (status == PF_OK && max_b > 0.0) {
             if (outer > 0) {
-                PF_LAUNCH("mixed_update", s, mixed_update<<<gp, kBlock, 0, s>>>(d, sc, e, DP));
-                PF_LAUNCH("mixed_residual", s, mixed_residual<<<gt, blk2, 0, s>>>(d, tl, cfd, sc, part, b, DP, r));
+                PF_LAUNCH("mixed_residual", s, mixed_residual<<<tiled_grid(tld), dim3(32, 8), 0, s>>>(
+                    d, tld, cfd, sc, part, b, DP, r));
                 if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
-                ratio = max_b > 0 ? hs.scale / max_b : 0.0;
+                ratio = hs.true_res / max_b;
             }
-            if (!(ratio == ratio)) { status = PF_NONFINITE; break; }
-            if (ratio <= min_res || max_b == 0.0) { status = PF_OK; break; }
-            if (outer >= max_outer || total >= max_it) { status = PF_MAXIT; break; }
-            if (outer > 1 && ratio > 0.5 * prev_ratio) { status = PF_STAGNATION; break; }
+            if (!(ratio == ratio) || std::isinf(ratio)) { status = PF_NONFINITE; break; }
+            if (ratio <= min_res) break;
+            if (outer >= kMaxOuter || total >= max_it) { status = PF_MAXIT; break; }
+            if (!use64 && outer > 1 && ratio > 0.5 * prev_ratio) use64 = true;
             prev_ratio = ratio;
-            PF_LAUNCH("bicg_init_f32", s, bicg_init<float, true><<<gp, kBlock, 0, s>>>(d, sc, part, outer == 0 ? b : r, 0.0, 0.0,
-                                                         v.res, v.res0, e, v.pp0, v.pp1, v.vv0, v.vv1,
-                                                         max_it - total, inner_tol));
-            const int rc = run_iterations<float>(d, tl, cf, sc, part, v, e, s, &hs);
-            if (rc) return rc;
-            total += hs.iter;
-            if (hs.status == PF_NONFINITE) { status = PF_NONFINITE; break; }
+            const double* rhs = outer == 0 ? b : r;
+            ++outer;
+            if (!use64) {
+                PF_LAUNCH("bicg_init_f32", s, bicg_init<float, true><<<gp, kBlock, 0, s>>>(
+                    d, sc, part, rhs, 0.0, 0.0, v32, e32, max_it - total, kInnerTol));
+                const int rc = run_iterations<float>(d, cf, sc, part, v32, e32, s, &hs);
+                if (rc) return rc;
+                total += hs.iter;
+                if (hs.status == PF_NONFINITE || hs.status == PF_BREAKDOWN) {
+                    use64 = true;  // discard this pass: x is unchanged
+                    continue;
+                }
+                PF_LAUNCH("fold_correction", s, fold_correction<float><<<gp, kBlock, 0, s>>>(d, sc, e32, DP));
+            } else {
+                // an FP64 pass finishes the solve: its tolerance is the
+                // remaining reduction
+                const double tol64 = std::min(0.5, 0.5 * min_res / ratio);
+                PF_LAUNCH("bicg_init_f64", s, bicg_init<double, true><<<gp, kBlock, 0, s>>>(
+                    d, sc, part, rhs, 0.0, 0.0, v64, e64, max_it - total, tol64));
+                const int rc = run_iterations<double>(d, cf64(g), sc, part, v64, e64, s, &hs);
+                if (rc) return rc;
+                total += hs.iter;
+                if (hs.status == PF_NONFINITE) { status = PF_NONFINITE; break; }
+                PF_LAUNCH("fold_correction", s, fold_correction<double><<<gp, kBlock, 0, s>>>(d, sc, e64, DP));
+            }
         }
         out.max_res = ratio; out.iterations = total; out.outer = outer; out.status = status;
     }
@@ -613,23 +781,33 @@ jacobi_prep(Dims d, BicgScalars* sc, double* part, const double* src, double c1,
 }
 
 // res = (A p) * -1 + source/dx^2, max|res| / max_res0
-__global__ void __launch_bounds__(kBlock)
+struct PhaseJacobiRes {
+    static constexpr int R = 2;
+    const double *p, *sdx;
+    double dx2, mx;
+    struct Raw { double p; };
+    struct Ext { double s; };
+    __device__ Raw raw(long long q) const { return Raw{p[q]}; }
+    __device__ Ext ext(long long q) const { return Ext{sdx[q]}; }
+    __device__ double op(const Raw& a) const { return a.p; }
+    __device__ void epi(long long, double, double ax, const Raw&, const Ext& e) {
+        const double v = ax * -1.0 + e.s / dx2;
+        mx = nanmax(mx, fabs(v));
+    }
+};
+
+__global__ void __launch_bounds__(kBlock, 2)
 jacobi_residual(Dims d, Tiling tl, LapCoef<double> cf, BicgScalars* sc,
                 double* part, const double* __restrict__ sdx, double dx2,
                 const double* __restrict__ p) {
     __shared__ double sh[32];
-    double m = 0.0;
-    auto load = [&](int i, int j, int k) -> double { return p[idx(d, i, j, k)]; };
-    auto epi = [&](int i, int j, int k, double c, double ax) {
-        const double v = ax * -1.0 + sdx[idx(d, i, j, k)] / dx2;
-        m = nanmax(m, fabs(v));
-    };
-    sweep_tiles<double>(d, tl, cf, load, epi);
-    const double bm = block_max<kBlock>(m, sh);
-    if (threadIdx.x == 0 && threadIdx.y == 0) part[blockIdx.x] = bm;
+    PhaseJacobiRes ph{p, sdx, dx2, 0.0};
+    sweep<double>(d, tl, cf, ph);
+    const double bm = block_max<kBlock>(ph.mx, sh);
+    if (tid0()) part[blockIdx.x] = bm;
     if (arrive_last(sc)) {
         const double mx = finish<true>(part, sh);
-        if (threadIdx.x == 0 && threadIdx.y == 0) { sc->max_res = mx / sc->max_res0; sc->counter = 0u; }
+        if (tid0()) { sc->max_res = mx / sc->max_res0; sc->counter = 0u; }
     }
 }
 
@@ -640,7 +818,7 @@ int jacobi_solve(const pf_grid* g, double rho, double dt, int n_it,
     const size_t n = (size_t)d.n;
     char* ptr = (char*)ws;
     BicgScalars* sc = (BicgScalars*)ptr; ptr += align256(sizeof(BicgScalars));
-    double* part = (double*)ptr; ptr += align256(2 * kMaxPartials * sizeof(double));
+    double* part = (double*)ptr; ptr += align256(kNumPartials * kMaxPartials * sizeof(double));
     double* sdx = (double*)ptr; ptr += align256(n * sizeof(double));
     double* tmp = (double*)ptr;
     const int gp = pointwise_grid(d.n);
@@ -661,8 +839,8 @@ int jacobi_solve(const pf_grid* g, double rho, double dt, int n_it,
             PF_LAUNCH("jacobi_sweep", s, jacobi_sweep<<<grd, blk, 0, s>>>(d, src_buf, sdx, dst_buf));
         }
     }
-    const Tiling tl = make_tiling(d);
-    PF_LAUNCH("jacobi_residual", 0, jacobi_residual<<<tiled_grid(tl), dim3(32, 8), 0, s>>>(d, tl, lap_coef<double>(g), sc, part, sdx, dx2, p));
+    const Tiling tl = make_tiling(d, 8 * PhaseJacobiRes::R);
+    PF_LAUNCH("jacobi_residual", s, jacobi_residual<<<tiled_grid(tl), dim3(32, 8), 0, s>>>(d, tl, lap_coef<double>(g), sc, part, sdx, dx2, p));
     if (cudaGetLastError() != cudaSuccess) return PF_ERR_CUDA;
     BicgScalars hs;
     if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;

@@ -53,3 +53,46 @@ def spectral_velocity(shape, lengths=(2 * np.pi,) * 3, k0=4.0, urms=1.0,
 def box_lengths(shape, lengths=None):
     """Periodic box lengths; default is [0, 2*pi]^3."""
     return tuple(lengths) if lengths is not None else (2 * np.pi,) * 3
+
+
+def spectral_velocity_device(shape, lengths=(2 * np.pi,) * 3, k0=4.0, urms=1.0,
+                             seed=0, device="cuda"):
+    """Same recipe as :func:`spectral_velocity` (same noise from the same
+    seed), with the FFTs done by torch on ``device``; for large grids.
+    Returns FP64 torch tensors."""
+    import torch
+    nx, ny, nz = (int(n) for n in shape)
+    rng = np.random.default_rng(seed)
+    h = [lengths[d] / shape[d] for d in range(3)]
+    kax = [torch.tensor(np.fft.fftfreq(shape[d], d=h[d]) * 2 * np.pi,
+                        device=device) for d in range(3)]
+    th = [torch.tensor(2 * np.pi * np.fft.fftfreq(shape[d]), device=device)
+          for d in range(3)]
+    KX, KY, KZ = kax[0][:, None, None], kax[1][None, :, None], kax[2][None, None, :]
+    kmag = torch.sqrt(KX ** 2 + KY ** 2 + KZ ** 2)
+    ek = kmag ** 4 * torch.exp(-2.0 * (kmag / k0) ** 2)
+    amp = torch.where(kmag > 0, torch.sqrt(ek / (4 * np.pi * kmag.clamp_min(1e-300) ** 2)),
+                      torch.zeros_like(kmag))
+    del ek, kmag
+    hat = []
+    for _ in range(3):
+        noise = torch.from_numpy(rng.standard_normal((nx, ny, nz))).to(device)
+        hat.append(torch.fft.fftn(noise) * amp)
+        del noise
+    g = [(torch.exp(1j * th[0]) - 1.0)[:, None, None] / h[0],
+         (torch.exp(1j * th[1]) - 1.0)[None, :, None] / h[1],
+         (torch.exp(1j * th[2]) - 1.0)[None, None, :] / h[2]]
+    div = g[0] * hat[0] + g[1] * hat[1] + g[2] * hat[2]
+    g2 = (g[0].abs() ** 2 + g[1].abs() ** 2 + g[2].abs() ** 2)
+    phi = torch.where(g2 > 0, div / torch.where(g2 > 0, g2, torch.ones_like(g2)),
+                      torch.zeros_like(div))
+    del div, g2
+    vel = []
+    for d in range(3):
+        a = hat[d] - torch.conj(g[d]) * phi
+        hat[d] = None
+        vel.append(torch.fft.ifftn(a).real.contiguous())
+        del a
+    e = sum(float((v * v).mean()) for v in vel) / 3
+    s = urms / np.sqrt(e) if e > 0 else 0.0
+    return tuple(v * s for v in vel)

@@ -195,3 +195,23 @@ def stats(u, v, w, spacing, out=None):
         ctypes.byref(g), _p(u), _p(v), _p(w), _p(out), _p(ws), ws.numel(),
         _stream(u)))
     return out
+
+
+SGS_MODELS = {"smagorinsky": (0, 1), "gradient": (1, 6), "gradients": (2, 9)}
+
+
+def sgs_closure(model, u, v, w, spacing, coef=1.0, out=None):
+    """Cell-centred SGS closure fields (pf_sgs_closure): 'smagorinsky' ->
+    (nx,ny,nz) eddy viscosity coef*|S|; 'gradient' -> (6,nx,ny,nz) stresses
+    coef du_i/dx_k du_j/dx_k; 'gradients' -> (9,nx,ny,nz) velocity gradients."""
+    mid, nf = SGS_MODELS[model]
+    for t, nm in ((u, "u"), (v, "v"), (w, "w")):
+        _check(t, u.shape, torch.float64, nm)
+    shape = tuple(u.shape) if nf == 1 else (nf,) + tuple(u.shape)
+    if out is None or tuple(out.shape) != shape:
+        out = torch.empty(shape, dtype=torch.float64, device=u.device)
+    g = grid(u.shape, spacing)
+    L.check("pf_sgs_closure", L.lib().pf_sgs_closure(
+        ctypes.byref(g), mid, _p(u), _p(v), _p(w), float(coef), _p(out),
+        _stream(u)))
+    return out

@@ -45,12 +45,12 @@ def bytes_per_cell(name):
     f64 = name.endswith("_f64")
     s = 8 if f64 else 4
     table = {
-        # BiCGStab phases: A reads pp, vv, res, res0, writes pp', vv';
-        # B reads res, vv', writes t; C reads pp', vv', res, t, x, res0,
-        # writes x, res  -> 17 field passes per iteration
-        "bicg_phase_a": 6 * s, "bicg_phase_b": 3 * s, "bicg_phase_c": 8 * s,
-        # init: read source (f64), write res, res0, zero x, pp0, pp1, vv0, vv1
-        "bicg_init": 8 + 7 * s,
+        # BiCGStab: kernel CA reads res, pp, vv, t, x, res0 and writes x,
+        # res', pp', vv'; kernel B reads res', vv', res0 and writes t
+        # -> 14 field passes per iteration
+        "bicg_ca": 10 * s, "bicg_b": 4 * s,
+        # init: read source (f64), write res, res0, x, pp, vv, t
+        "bicg_init": 8 + 6 * s,
         # RK4 stages: FP64 state u,v,w (24 B) + stage state / k-sum (3 fields)
         "rhs_first": 24 + 6 * s, "rhs_mid": 24 + 12 * s,
         "rhs_last": 24 + 6 * s + 24, "rhs_euler": 48, "rhs_rhs": 6 * s,

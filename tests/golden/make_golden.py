@@ -18,6 +18,10 @@ ops_12x16x20.npz   per-operator cases on a non-cubic, anisotropic periodic box:
                    solver_bicgstab.solve, vel_corr.
 jacobi_16.npz      solver_jacobi.solve on a cubic 16^3 box (the reference's
                    Jacobi assumes dx = dy = dz).
+sgs_12x16x20.npz   SGS closures on the same kind of box: Smagorinsky eddy
+                   viscosity (stress_constCs.eddyVisc), gradient-model stresses
+                   (residual_stress.update), and the RHS with each closure
+                   active (VISC_P = mu + mu_t; 'tensor' stresses added).
 run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
                    nu = 0.01, dt = 0.005, RK4 + BiCGStab to 1e-10, 5 steps:
                    final u, v, w, p and per-step max residual, iteration count
@@ -143,6 +147,51 @@ def ops_case(out):
     print("ops: bicgstab iters", res["bicg_iters"], "max_res", r)
 
 
+def sgs_case(out):
+    import torch
+    nx, ny, nz = 12, 16, 20
+    lengths = (2 * np.pi, 2.1, 3.3)
+    S = H.make_setup(nx, ny, nz, *lengths)
+    ns, d = S.ns, S.decomp
+    rng = np.random.default_rng(99)
+    u, v, w = (rng.standard_normal((nx, ny, nz)) for _ in range(3))
+    mu, rho = 0.01, 1.3
+
+    class IC:
+        Cs = 0.17
+        expFilterFac = 1.5
+
+    smag = ns.sfsmodel_smagorinsky.stress_constCs(IC(), S.geo)
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    mu_t = smag.eddyVisc(su, sv, sw, rho, S.metric)
+    res = dict(shape=np.array([nx, ny, nz]),
+               spacing=np.array([S.geo.dx, S.geo.dy, S.geo.dz]), u=u, v=v, w=w,
+               mu=mu, rho=rho, Cs=IC.Cs, expFilterFac=IC.expFilterFac,
+               mu_t=mu_t[2:-2, 2:-2, 2:-2].numpy().copy())
+    # RHS with VISC_P = mu + mu_t (src/data/domain.py:348-352)
+    VISC = torch.ones(nx + 4, ny + 4, nz + 4, dtype=torch.float64) * mu
+    VISC.copy_(mu + mu_t)
+    rhs = ns.velocity.rhs_NavierStokes(d, S.metric, rho, VISC, smag)
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    rhs.evaluate(su, sv, sw)
+    res["rhs_smag"] = np.stack([rhs.rhs_u.numpy(), rhs.rhs_v.numpy(),
+                                rhs.rhs_w.numpy()])
+    # gradient model
+    gm = ns.sfsmodel_gradient.residual_stress(d, S.geo, S.metric)
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    gm.update(su, sv, sw, S.metric)
+    res["grad_F"] = np.stack([getattr(gm, k)[2:-2, 2:-2, 2:-2].numpy().copy()
+                              for k in ("FXX", "FYY", "FZZ", "FXY", "FXZ", "FYZ")])
+    VISC = torch.ones(nx + 4, ny + 4, nz + 4, dtype=torch.float64) * mu
+    rhs = ns.velocity.rhs_NavierStokes(d, S.metric, rho, VISC, gm)
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    rhs.evaluate(su, sv, sw)
+    res["rhs_grad"] = np.stack([rhs.rhs_u.numpy(), rhs.rhs_v.numpy(),
+                                rhs.rhs_w.numpy()])
+    np.savez_compressed(os.path.join(out, "sgs_12x16x20.npz"), **res)
+    print("sgs: max mu_t", float(mu_t.abs().max()))
+
+
 def jacobi_case(out):
     import torch
     n = 16
@@ -249,6 +298,12 @@ def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005):
 
 if __name__ == "__main__":
     out = HERE
-    ops_case(out)
-    jacobi_case(out)
-    run_case(out)
+    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "run"]
+    if "ops" in which:
+        ops_case(out)
+    if "jacobi" in which:
+        jacobi_case(out)
+    if "sgs" in which:
+        sgs_case(out)
+    if "run" in which:
+        run_case(out)
