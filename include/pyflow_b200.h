@@ -142,6 +142,24 @@ int pf_sgs_closure(const pf_grid* g, int model, const double* u,
                    const double* v, const double* w, double coef, double* out,
                    void* stream);
 
+/* SGS MLP closure on the tensor cores (tcgen05, BF16 operands, FP32
+ * accumulation in TMEM): out[c*n + cell], c = 0..5 (FXX, FYY, FZZ, FXY, FXZ,
+ * FYZ, FP64) = scales[1] * MLP(scales[0] * grad u), where grad u are the nine
+ * cell-centred gradients of pf_sgs_closure model 2 and MLP is
+ * 9 -> 128 (tanh) -> 128 (tanh) -> 6.  The stresses go to the 'tensor' SFS
+ * slot (src/solver/velocity.py:262-267,286-291,310-315); the model itself has
+ * no reference code (the reference's ML closure, src/sfsmodel/sfsmodel_ML.py,
+ * is a different 'source'-type network).  wpack: device buffer of
+ * pf_mlp_pack_bytes() bytes, 16-byte aligned, holding W1 (128x16), W2
+ * (128x128), W3 (16x128) as BF16 in the K-major no-swizzle UMMA layout
+ * followed by b1[128], b2[128], b3[16] as float (see sfsmodel_mlp.pack);
+ * scales: 2 device floats; err: device int set to 1 if a tensor-core wait
+ * timed out. */
+size_t pf_mlp_pack_bytes(void);
+int pf_mlp_closure(const pf_grid* g, const double* u, const double* v,
+                   const double* w, const void* wpack, const float* scales,
+                   double* out, int* err, void* stream);
+
 /* No counterpart in the reference: the pf_bicgstab_solve solve (FP64) for
  * callers that cannot allocate device memory or pass a workspace (for example
  * a plugin whose host application owns the whole device-memory budget, or a

@@ -60,6 +60,8 @@ def _load():
                              S, P, ctypes.POINTER(SolveInfo)], I),
         "pf_stats": ([G, P, P, P, P, P, S, P], I),
         "pf_sgs_closure": ([G, I, P, P, P, D, P, P], I),
+        "pf_mlp_pack_bytes": ([], S),
+        "pf_mlp_closure": ([G, P, P, P, P, P, P, P, P], I),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

@@ -1,0 +1,391 @@
+// pf_mlp.cu -- the SGS MLP closure on the 5th-generation tensor cores.
+//
+// Per cell: the nine cell-centred velocity gradients (grad_vel_center,
+// src/metric/metric_staggered.py:215-268) scaled by 1/g_rms are the inputs of
+// a 9 -> 128 -> 128 -> 6 MLP with tanh hidden layers, BF16 weights and FP32
+// accumulation; its six outputs times out_scale are the stresses FXX, FYY, FZZ,
+// FXY, FXZ, FYZ of the 'tensor' SFS slot (src/solver/velocity.py:262-267,...).
+//
+// One CTA of 128 threads (4 warps) walks tiles of 128 consecutive cells; cell
+// m of a tile is accumulator row / TMEM lane m and belongs to thread m:
+//   1. each thread computes its cell's gradients and writes 16 BF16 features
+//      (9 + 7 zero pads) into the X tile in shared memory;
+//   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
+//   3. each thread reads its D1 row from TMEM (tcgen05.ld), adds b1, applies
+//      tanh, and writes the BF16 row into the H tile;
+//   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
+//   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
+//      its six stresses (FP64) to global memory.
+// Completion of each MMA group is signalled by tcgen05.commit to an mbarrier;
+// every wait on it is bounded and reports a timeout through an error flag.
+//
+// Shared-memory operands use the K-major, no-swizzle canonical layout of the
+// UMMA descriptors: 8-row x 16-byte core matrices, K chunks 128 B apart
+// (leading byte offset), 8-row groups 256 B apart (stride byte offset), one
+// 4 KiB (128 rows) or 512 B (16 rows) block per 16-wide K slice.  The weights
+// arrive pre-packed in exactly this layout (see pf_mlp_pack_bytes).
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "pf_common.cuh"
+#include "pf_kernels.cuh"
+#include "pf_profile.cuh"
+
+namespace pf {
+
+namespace mlp {
+
+constexpr int kHidden = 128;
+constexpr int kTile = 128;
+constexpr int kW1Bytes = 4096;      // 128 x 16 bf16
+constexpr int kW2Bytes = 32768;     // 128 x 128 bf16
+constexpr int kW3Bytes = 4096;      // 16 x 128 bf16
+constexpr int kBiasBytes = (128 + 128 + 16) * 4;
+constexpr int kPackBytes = kW1Bytes + kW2Bytes + kW3Bytes + kBiasBytes;
+constexpr int kXBytes = 4096;       // 128 x 16 bf16
+constexpr int kHBytes = 32768;      // 128 x 128 bf16
+constexpr unsigned kTmemCols = 256;
+constexpr long long kSpinLimit = 1LL << 22;
+
+// byte offset of element (row r, col k) in a K-major no-swizzle tile whose
+// 16-wide K slices are `slice` bytes apart
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int slice) {
+    return (uint32_t)((k >> 4) * slice + (r >> 3) * 256 + ((k >> 3) & 1) * 128 + (r & 7) * 16 +
+                      (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor: K-major, no swizzle, LBO 128 B, SBO 256 B,
+// descriptor version 1 (sm_100)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)(128 >> 4) << 16;
+    d |= (uint64_t)(256 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;  // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b,
+                                         uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(bar)) : "memory");
+}
+
+// bounded wait for the mbarrier phase; false on timeout
+__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t phase) {
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(a), "r"(phase) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+          "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+          "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+
+__device__ inline void cell_gradients(const Dims& d, const double* __restrict__ u,
+                                      const double* __restrict__ v,
+                                      const double* __restrict__ w, long long cell,
+                                      double dxi, double dyi, double dzi, double* g) {
+    const int k = (int)(cell % d.nz);
+    const long long r = cell / d.nz;
+    const int j = (int)(r % d.ny), i = (int)(r / d.ny);
+    const int ip = wrap(i + 1, d.nx), im = wrap(i - 1, d.nx);
+    const int jp = wrap(j + 1, d.ny), jm = wrap(j - 1, d.ny);
+    const int kp = wrap(k + 1, d.nz), km = wrap(k - 1, d.nz);
+    auto L = [&](const double* f, int a, int b, int c) { return __ldg(f + idx(d, a, b, c)); };
+    {
+        const double c0 = 0.5 * (L(u, ip, j, k) + L(u, i, j, k));
+        const double cym = 0.5 * (L(u, ip, jm, k) + L(u, i, jm, k));
+        const double cyp = 0.5 * (L(u, ip, jp, k) + L(u, i, jp, k));
+        const double czm = 0.5 * (L(u, ip, j, km) + L(u, i, j, km));
+        const double czp = 0.5 * (L(u, ip, j, kp) + L(u, i, j, kp));
+        g[0] = (L(u, ip, j, k) - L(u, i, j, k)) * dxi;
+        g[1] = (0.5 * (cyp + c0) - 0.5 * (c0 + cym)) * dyi;
+        g[2] = (0.5 * (czp + c0) - 0.5 * (c0 + czm)) * dzi;
+    }
+    {
+        const double c0 = 0.5 * (L(v, i, jp, k) + L(v, i, j, k));
+        const double cxm = 0.5 * (L(v, im, jp, k) + L(v, im, j, k));
+        const double cxp = 0.5 * (L(v, ip, jp, k) + L(v, ip, j, k));
+        const double czm = 0.5 * (L(v, i, jp, km) + L(v, i, j, km));
+        const double czp = 0.5 * (L(v, i, jp, kp) + L(v, i, j, kp));
+        g[3] = (0.5 * (cxp + c0) - 0.5 * (c0 + cxm)) * dxi;
+        g[4] = (L(v, i, jp, k) - L(v, i, j, k)) * dyi;
+        g[5] = (0.5 * (czp + c0) - 0.5 * (c0 + czm)) * dzi;
+    }
+    {
+        const double c0 = 0.5 * (L(w, i, j, kp) + L(w, i, j, k));
+        const double cxm = 0.5 * (L(w, im, j, kp) + L(w, im, j, k));
+        const double cxp = 0.5 * (L(w, ip, j, kp) + L(w, ip, j, k));
+        const double cym = 0.5 * (L(w, i, jm, kp) + L(w, i, jm, k));
+        const double cyp = 0.5 * (L(w, i, jp, kp) + L(w, i, jp, k));
+        g[6] = (0.5 * (cxp + c0) - 0.5 * (c0 + cxm)) * dxi;
+        g[7] = (0.5 * (cyp + c0) - 0.5 * (c0 + cym)) * dyi;
+        g[8] = (L(w, i, j, kp) - L(w, i, j, k)) * dzi;
+    }
+}
+
+// Writes 128 hidden values of this thread's row: tanh(acc + bias) as BF16.
+__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bias,
+                                                uint8_t* H, int row) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < kHidden; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr + c0, v);
+#pragma unroll
+        for (int q = 0; q < 16; q += 8) {
+            uint32_t packed[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float a = tanh_fast(v[q + 2 * e] + bias[c0 + q + 2 * e]);
+                const float b = tanh_fast(v[q + 2 * e + 1] + bias[c0 + q + 2 * e + 1]);
+                packed[e] = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
+            }
+            // 8 consecutive k of one row are one 16-byte chunk
+            *reinterpret_cast<uint4*>(H + kmajor_off(row, c0 + q, 4096)) =
+                make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        }
+    }
+}
+
+}  // namespace mlp
+
+// scales[0] = 1/g_rms (input normalisation), scales[1] = output scale
+__global__ void __launch_bounds__(128, 1)
+mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restrict__ v,
+                   const double* __restrict__ w, double dxi, double dyi, double dzi,
+                   const uint8_t* __restrict__ wpack, const float* __restrict__ scales,
+                   double* __restrict__ out, int* __restrict__ err) {
+    using namespace mlp;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* sW1 = smem;
+    uint8_t* sW2 = sW1 + kW1Bytes;
+    uint8_t* sW3 = sW2 + kW2Bytes;
+    float* sB = reinterpret_cast<float*>(sW3 + kW3Bytes);  // b1[128] b2[128] b3[16]
+    uint8_t* sX = reinterpret_cast<uint8_t*>(sB) + kBiasBytes;
+    uint8_t* sH = sX + kXBytes;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sH + kHBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // weights: a straight copy of the packed image
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(wpack);
+        uint4* dst = reinterpret_cast<uint4*>(smem);
+        for (int q = tid; q < kPackBytes / 16; q += blockDim.x) dst[q] = src[q];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t d1 = tmem, d2 = tmem + 128, d3 = tmem;  // column offsets
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const float in_scale = scales[0], out_scale = scales[1];
+    const uint32_t id128 = instr_desc(128, 128), id16 = instr_desc(128, 16);
+    uint32_t phase = 0;
+    bool ok = true;
+    const long long ntiles = (d.n + kTile - 1) / kTile;
+    for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const long long cell = t * kTile + tid;
+        const bool valid = cell < d.n;
+        // ---- features -> X (row tid)
+        {
+            double g[9];
+            if (valid) cell_gradients(d, u, v, w, cell, dxi, dyi, dzi, g);
+            uint32_t p[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int k0 = 2 * e, k1 = 2 * e + 1;
+                const float a = (valid && k0 < 9) ? float(g[k0]) * in_scale : 0.f;
+                const float b = (valid && k1 < 9) ? float(g[k1]) * in_scale : 0.f;
+                p[e] = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
+            }
+            *reinterpret_cast<uint4*>(sX + kmajor_off(tid, 0, 4096)) = make_uint4(p[0], p[1], p[2], p[3]);
+            *reinterpret_cast<uint4*>(sX + kmajor_off(tid, 8, 4096)) = make_uint4(p[4], p[5], p[6], p[7]);
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // ---- layer 1
+        if (tid == 0) {
+            tc_fence_after();
+            mma_bf16(d1, smem_desc(smem_u32(sX)), smem_desc(smem_u32(sW1)), id128, 0u);
+            commit(bar);
+        }
+        ok = __syncthreads_and(wait_phase(bar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        tc_fence_after();
+        hidden_epilogue(lane_base + d1, sB, sH, tid);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // ---- layer 2
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll 1
+            for (int kb = 0; kb < 8; ++kb)
+                mma_bf16(d2, smem_desc(smem_u32(sH) + kb * 4096), smem_desc(smem_u32(sW2) + kb * 4096),
+                         id128, kb > 0 ? 1u : 0u);
+            commit(bar);
+        }
+        ok = __syncthreads_and(wait_phase(bar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        tc_fence_after();
+        hidden_epilogue(lane_base + d2, sB + 128, sH, tid);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // ---- layer 3
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll 1
+            for (int kb = 0; kb < 8; ++kb)
+                mma_bf16(d3, smem_desc(smem_u32(sH) + kb * 4096), smem_desc(smem_u32(sW3) + kb * 512),
+                         id16, kb > 0 ? 1u : 0u);
+            commit(bar);
+        }
+        ok = __syncthreads_and(wait_phase(bar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        tc_fence_after();
+        {
+            float y[16];
+            mlp::tmem_ld16(lane_base + d3, y);
+            if (valid) {
+                const float* b3 = sB + 256;
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    out[(long long)c * d.n + cell] = double(y[c] + b3[c]) * double(out_scale);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (!ok) {
+        // an MMA group did not signal completion: record it, and give the
+        // tensor core one more bounded wait before the TMEM is released
+        if (tid == 0) atomicExch(err, 1);
+        wait_phase(bar, phase ^ 1u);  // the phase whose wait gave up
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(kTmemCols));
+    }
+}
+
+size_t mlp_smem_bytes() {
+    return (size_t)mlp::kPackBytes + mlp::kXBytes + mlp::kHBytes + 64;
+}
+
+cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
+                       const double* w, const void* wpack, const float* scales,
+                       double* out, int* err, cudaStream_t s) {
+    Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
+    const size_t smem = mlp_smem_bytes();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(mlp_closure_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long ntiles = (d.n + mlp::kTile - 1) / mlp::kTile;
+    // one CTA per SM: each holds 256 TMEM columns and ~75 KB of shared memory
+    const int grid = (int)std::min<long long>(ntiles, (long long)sms);
+    PF_LAUNCH("mlp_closure", s, mlp_closure_kernel<<<grid, 128, smem, s>>>(
+        d, u, v, w, 1.0 / g->dx, 1.0 / g->dy, 1.0 / g->dz, (const uint8_t*)wpack, scales,
+        out, err));
+    return cudaGetLastError();
+}
+
+}  // namespace pf
+
+extern "C" size_t pf_mlp_pack_bytes(void) { return (size_t)pf::mlp::kPackBytes; }
+
+extern "C" int pf_mlp_closure(const pf_grid* g, const double* u, const double* v,
+                              const double* w, const void* wpack,
+                              const float* scales, double* out, int* err,
+                              void* stream) {
+    if (!g || g->nx < 2 || g->ny < 2 || g->nz < 2 || !(g->dx > 0) || !(g->dy > 0) ||
+        !(g->dz > 0) || !u || !v || !w || !wpack || !scales || !out || !err)
+        return PF_ERR_BAD_ARG;
+    if (((uintptr_t)wpack & 15) != 0) return PF_ERR_BAD_ARG;
+    return pf::launch_mlp(g, u, v, w, wpack, scales, out, err, (cudaStream_t)stream) == cudaSuccess
+               ? PF_OK : PF_ERR_CUDA;
+}

@@ -1,0 +1,58 @@
+"""The tensor-core SGS MLP closure (pf_mlp_closure) vs a torch model of the
+same arithmetic (BF16 inputs, weights and hidden activations; FP32
+accumulation).  Tolerance: 3e-2 of the output range -- the kernel's hardware
+tanh (tanh.approx.f32, relative error ~1e-3.5) and the tensor core's FP32
+summation order can flip the BF16 rounding of a hidden activation, which
+moves an output by a few BF16 ulps of its inputs."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 20, 36), (5, 7, 9)])
+def test_mlp_closure_matches_bf16_model(shape):
+    import pyflow_b200.initial as ic
+    import pyflow_b200.ops as ops
+    import pyflow_b200.sfsmodel_mlp as M
+    sp = tuple(2 * np.pi / n for n in shape)
+    u, v, w = (torch.tensor(a, device="cuda") for a in
+               ic.spectral_velocity(shape, k0=3.0, seed=4))
+    params = M.xavier_init(1)
+    rng = np.random.default_rng(7)
+    for k in ("b1", "b2", "b3"):
+        params[k] = (0.1 * rng.standard_normal(params[k].shape)).astype(np.float32)
+    wpack = torch.as_tensor(M.pack(params)).cuda()
+    out, g9, scales, err = M.closure(u, v, w, sp, wpack, delta=sp[0])
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = M.reference_forward(g9.reshape(9, -1), params, float(scales[0]),
+                              float(scales[1])).reshape(out.shape)
+    got = out
+    scale = ref.abs().max().item()
+    assert scale > 0
+    err_max = (got - ref).abs().max().item()
+    assert err_max <= 3e-2 * scale, (err_max, scale)
+    # most cells agree to FP32 accumulation order
+    close = ((got - ref).abs() <= 1e-4 * scale).double().mean().item()
+    assert close > 0.9, close
+
+
+def test_mlp_in_rhs_slot_runs():
+    """The closure feeds the 'tensor' slot of the RHS like the gradient model."""
+    import pyflow_b200.initial as ic
+    import pyflow_b200.ops as ops
+    import pyflow_b200.sfsmodel_mlp as M
+    n = 16
+    sp = (2 * np.pi / n,) * 3
+    u, v, w = (torch.tensor(a, device="cuda") for a in
+               ic.spectral_velocity((n, n, n), k0=3.0, seed=2))
+    wpack = torch.as_tensor(M.pack(M.xavier_init(1))).cuda()
+    F, _, _, err = M.closure(u, v, w, sp, wpack, delta=sp[0])
+    r0 = ops.rhs_ns(u, v, w, sp, 0.001, 1.0)
+    r1 = ops.rhs_ns(u, v, w, sp, 0.001, 1.0, sfs=F)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    d = max((a - b).abs().max().item() for a, b in zip(r0, r1))
+    assert 0 < d < 1e3
