@@ -160,6 +160,22 @@ int pf_mlp_closure(const pf_grid* g, const double* u, const double* v,
                    const double* w, const void* wpack, const float* scales,
                    double* out, int* err, void* stream);
 
+/* Exact discrete adjoint of the constant-viscosity RHS: out = J(u)^T mu where
+ * J is the Jacobian of pf_rhs_ns (rhs_NavierStokes.evaluate,
+ * src/solver/velocity.py:221-355) at state (u, v, w).  Replaces the
+ * reference's adjoint RHS (rhs_adjPredictor.evaluate, src/solver/adjoint.py:94-227,
+ * adj_conv_*, src/metric/metric_staggered.py:537-799).  FP64. */
+int pf_rhs_adjoint(const pf_grid* g, const double* u, const double* v,
+                   const double* w, const double* mu_u, const double* mu_v,
+                   const double* mu_w, double mu, double rho, double* out_u,
+                   double* out_v, double* out_w, void* stream);
+
+/* Adjoint of the 'tensor' SFS stresses in the RHS
+ * (src/solver/velocity.py:262-267,286-291,310-315): out[0..5] += weight *
+ * dL/d(FXX, FYY, FZZ, FXY, FXZ, FYZ) for the RHS adjoint mu.  FP64. */
+int pf_sfs_adjoint(const pf_grid* g, const double* mu_u, const double* mu_v,
+                   const double* mu_w, double weight, double* out, void* stream);
+
 /* No counterpart in the reference: the pf_bicgstab_solve solve (FP64) for
  * callers that cannot allocate device memory or pass a workspace (for example
  * a plugin whose host application owns the whole device-memory budget, or a

@@ -22,6 +22,12 @@ sgs_12x16x20.npz   SGS closures on the same kind of box: Smagorinsky eddy
                    viscosity (stress_constCs.eddyVisc), gradient-model stresses
                    (residual_stress.update), and the RHS with each closure
                    active (VISC_P = mu + mu_t; 'tensor' stresses added).
+adjoint_12x16x20.npz  the reference's adjoint RHS (rhs_adjPredictor.evaluate,
+                   src/solver/adjoint.py:94-298) at a random state for a random
+                   adjoint field, its ML-closure term zeroed by a stand-in model
+                   that keeps the autograd graph; and one reference Euler
+                   adjoint step (adjoint projection, then the adjoint advancer;
+                   src/data/domain.py:409-438).
 run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
                    nu = 0.01, dt = 0.005, RK4 + BiCGStab to 1e-10, 5 steps:
                    final u, v, w, p and per-step max residual, iteration count
@@ -192,6 +198,64 @@ def sgs_case(out):
     print("sgs: max mu_t", float(mu_t.abs().max()))
 
 
+def adjoint_case(out):
+    import torch
+    nx, ny, nz = 12, 16, 20
+    lengths = (2 * np.pi, 2.1, 3.3)
+    S = H.make_setup(nx, ny, nz, *lengths)
+    ns, d = S.ns, S.decomp
+    rng = np.random.default_rng(4242)
+    u, v, w = (rng.standard_normal((nx, ny, nz)) for _ in range(3))
+    lu, lv, lw = (rng.standard_normal((nx, ny, nz)) for _ in range(3))
+    mu, rho, dt = 0.02, 1.1, 1.0e-3
+
+    class ZeroML:
+        """'source' closure whose output is 0 * u but stays on the graph."""
+        modelType = "source"
+
+        def update(self, u_V, v_V, w_V, requires_grad=True):
+            z = 0.0 * (u_V + v_V + w_V)
+            self.GX = z[..., None]
+            self.GY = z[..., None]
+            self.GZ = z[..., None]
+
+    VISC = torch.ones(nx + 4, ny + 4, nz + 4, dtype=torch.float64) * mu
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    radj = ns.adjoint.rhs_adjPredictor(d, S.metric, rho, VISC, ZeroML(), su, sv, sw)
+    au, av, aw = (_state(ns, d, a) for a in (lu, lv, lw))
+    radj.evaluate(au, av, aw)
+    res = dict(shape=np.array([nx, ny, nz]),
+               spacing=np.array([S.geo.dx, S.geo.dy, S.geo.dz]), u=u, v=v, w=w,
+               lu=lu, lv=lv, lw=lw, mu=mu, rho=rho, dt=dt,
+               rhs_adj=np.stack([radj.rhs_u.numpy().copy(), radj.rhs_v.numpy().copy(),
+                                 radj.rhs_w.numpy().copy()]))
+    # one Euler adjoint step: adjoint projection, then lam += dt rhs_adj(lam)
+    au, av, aw = (_state(ns, d, a) for a in (lu, lv, lw))
+    sDP = _state(ns, d, np.zeros((nx, ny, nz)))
+    sp = _state(ns, d, np.zeros((nx, ny, nz)))
+    src = torch.zeros(nx, ny, nz, dtype=torch.float64)
+    S.metric.div_vel(au, av, aw, src)
+    solver = ns.pressure.solver_bicgstab(S.comms, d, S.metric, S.geo, rho, dt,
+                                         1e-13, 2000)
+    solver.solve(sDP, sp, src)
+    S.metric.grad_P(sDP)
+    au.vel_corr(sDP.grad_x, +dt / rho)
+    av.vel_corr(sDP.grad_y, +dt / rho)
+    aw.vel_corr(sDP.grad_z, +dt / rho)
+
+    class RHSSet:
+        pass
+
+    rs = RHSSet()
+    rs.rhs1 = ns.adjoint.rhs_adjPredictor(d, S.metric, rho, VISC, ZeroML(), su, sv, sw)
+    ns.advancer.Euler(au, av, aw, rs).step(dt)
+    res["euler_adj_step"] = np.stack([au.interior().numpy().copy(),
+                                      av.interior().numpy().copy(),
+                                      aw.interior().numpy().copy()])
+    np.savez_compressed(os.path.join(out, "adjoint_12x16x20.npz"), **res)
+    print("adjoint: max |rhs_adj|", np.abs(res["rhs_adj"]).max())
+
+
 def jacobi_case(out):
     import torch
     n = 16
@@ -298,12 +362,14 @@ def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005):
 
 if __name__ == "__main__":
     out = HERE
-    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "run"]
+    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run"]
     if "ops" in which:
         ops_case(out)
     if "jacobi" in which:
         jacobi_case(out)
     if "sgs" in which:
         sgs_case(out)
+    if "adjoint" in which:
+        adjoint_case(out)
     if "run" in which:
         run_case(out)
