@@ -190,6 +190,26 @@ int pf_bicgstab_solve_noalloc(const pf_grid* g, double rho, double dt,
                               double* DP, double* p, void* stream,
                               pf_solve_info* info);
 
+/* A whole Domain.forwardStep (src/data/domain.py:342-402; constant viscosity,
+ * no SFS model) captured once as a CUDA graph bound to the given fields and
+ * workspace: predictor, divergence, Poisson solve with device-side
+ * convergence loops (conditional WHILE nodes), p += DP, projection and the
+ * monitor statistics (src/core/PyFlow.py:379-395).  Each launch advances one
+ * step with no host synchronisation; stats (device, 8 doubles) receives
+ * max|u|, max|v|, max|w|, TKE, max|div u|, max_res, iterations, status after
+ * every step.  The workspace (pf_step_plan_workspace_bytes, 256-byte aligned)
+ * belongs to the plan.  Plans of different fields may run concurrently on
+ * different streams. */
+typedef struct pf_step_plan pf_step_plan;
+size_t pf_step_plan_workspace_bytes(const pf_grid* g, int prec);
+int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u,
+                        double* v, double* w, double* p, double* DP, double mu,
+                        double rho, double dt, double min_res, int max_it,
+                        void* ws, size_t ws_bytes, double* stats,
+                        pf_step_plan** plan);
+int pf_step_plan_launch(pf_step_plan* plan, int nsteps, void* stream);
+int pf_step_plan_destroy(pf_step_plan* plan);
+
 /* Optional per-kernel device-time accounting: when enabled, each kernel launch
  * of the library is bracketed by CUDA events on its stream.  pf_profile_read
  * waits for pending events and fills up to max_entries records (per kernel

@@ -4,6 +4,7 @@
 // pf_rhs.cu and pf_poisson.cu.  No entry point allocates device memory and no
 // C++ exception crosses the ABI.
 #include <algorithm>
+#include <cstdint>
 
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
@@ -149,5 +150,33 @@ int pf_stats(const pf_grid* g, const double* u, const double* v,
     if (!ws || ws_bytes < stats_ws_bytes(g)) return PF_ERR_BAD_ARG;
     return cuda_rc(launch_stats(g, u, v, w, out_dev, ws, S(stream)));
 }
+
+size_t pf_step_plan_workspace_bytes(const pf_grid* g, int prec) {
+    if (!grid_ok(g) || !prec_ok(prec)) return 0;
+    return step_plan_ws_bytes(g, prec);
+}
+
+int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
+                        double* w, double* p, double* DP, double mu, double rho,
+                        double dt, double min_res, int max_it, void* ws,
+                        size_t ws_bytes, double* stats, pf_step_plan** plan) {
+    if (!grid_ok(g) || !prec_ok(prec) || !u || !v || !w || !p || !DP || !stats || !plan ||
+        !(rho != 0.0) || !(dt != 0.0) || max_it < 1)
+        return PF_ERR_BAD_ARG;
+    if (!ws || ws_bytes < step_plan_ws_bytes(g, prec) || ((uintptr_t)ws & 255) != 0)
+        return PF_ERR_BAD_ARG;
+    void* h = nullptr;
+    const int rc = step_plan_create(g, prec, rk4, u, v, w, p, DP, mu, rho, dt, min_res, max_it,
+                                    ws, stats, &h);
+    if (rc == PF_OK) *plan = (pf_step_plan*)h;
+    return rc;
+}
+
+int pf_step_plan_launch(pf_step_plan* plan, int nsteps, void* stream) {
+    if (!plan || nsteps < 0) return PF_ERR_BAD_ARG;
+    return step_plan_launch(plan, nsteps, S(stream));
+}
+
+int pf_step_plan_destroy(pf_step_plan* plan) { return step_plan_destroy(plan); }
 
 }  // extern "C"

@@ -37,4 +37,12 @@ cudaError_t launch_stats(const pf_grid* g, const double* u, const double* v,
                          const double* w, double* out, void* ws,
                          cudaStream_t s);
 
+size_t step_plan_ws_bytes(const pf_grid* g, int prec);
+int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
+                     double* w, double* p, double* DP, double mu, double rho,
+                     double dt, double min_res, int max_it, void* ws,
+                     double* stats, void** out);
+int step_plan_launch(void* plan, int nsteps, cudaStream_t s);
+int step_plan_destroy(void* plan);
+
 }  // namespace pf

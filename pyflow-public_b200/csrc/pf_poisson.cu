@@ -49,6 +49,7 @@ struct BicgScalars {
     double scale;      // mixed: max|r| of the current refinement pass
     double max_b;      // mixed: max|b|
     double true_res;   // mixed: max|b - A x| of the last refinement pass
+    int outer, total;  // mixed graph mode: refinement passes, inner iterations
     int k;             // index of the next CA kernel
     int iter;          // completed iterations
     int done;          // 0 running, 1 stopped, 2 stop after DP += alpha pp
@@ -294,7 +295,7 @@ bicg_init(Dims d, BicgScalars* sc, double* part, const double* src, double c1,
           double c2, BicgVecs<T> v, T* x, int max_it, double min_res) {
     __shared__ double sh[32];
     double s = 0.0, m = 0.0;
-    const double inv = FROM_RESIDUAL ? 1.0 / sc->scale : 0.0;
+    const double inv = (FROM_RESIDUAL && sc->scale > 0.0) ? 1.0 / sc->scale : 0.0;
     T* res = v.res[1];
     T* pp = v.pp[1];
     T* vv = v.vv[1];
@@ -367,10 +368,14 @@ struct PhaseCA {
 template <typename T>
 __global__ void __launch_bounds__(kBlock, 2)
 bicg_ca(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
-        BicgVecs<T> v, T* __restrict__ x) {
+        BicgVecs<T> v, T* __restrict__ x, int use_cond = 0,
+        cudaGraphConditionalHandle cond = 0) {
     __shared__ double sh[32];
     const int done = sc->done;
-    if (done == 1) return;
+    if (done == 1) {
+        if (use_cond && blockIdx.x == 0 && tid0()) cudaGraphSetConditional(cond, 0);
+        return;
+    }
     const int k = sc->k;
     const bool odd = k & 1;  // CA(k) writes set k&1 and reads the other
     if (done == 2) {
@@ -383,7 +388,11 @@ bicg_ca(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
                            threadIdx.y * blockDim.x + threadIdx.x;
              q < d.n; q += nt)
             x[q] = fma(alpha, pp[q], x[q]);
-        if (arrive_last(sc) && tid0()) { sc->done = 1; sc->counter = 0u; }
+        if (arrive_last(sc) && tid0()) {
+            sc->done = 1;
+            sc->counter = 0u;
+            if (use_cond) cudaGraphSetConditional(cond, 0);
+        }
         return;
     }
     PhaseCA<T> ph;
@@ -422,7 +431,10 @@ bicg_ca(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
                 if (gamma == 0.0) { stop = true; sc->status = PF_BREAKDOWN; }
                 else sc->alpha = sc->rho1 / gamma;
             }
-            if (stop) sc->done = 1;
+            if (stop) {
+                sc->done = 1;
+                if (use_cond) cudaGraphSetConditional(cond, 0);
+            }
             sc->k = k + 1;
             sc->counter = 0u;
         }
@@ -454,9 +466,13 @@ struct PhaseB {
 template <typename T>
 __global__ void __launch_bounds__(kBlock, 2)
 bicg_b(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
-       BicgVecs<T> v) {
+       BicgVecs<T> v, int use_cond = 0, cudaGraphConditionalHandle cond = 0) {
     __shared__ double sh[32];
-    if (sc->done) return;
+    if (sc->done) {
+        if (sc->done == 1 && use_cond && blockIdx.x == 0 && tid0())
+            cudaGraphSetConditional(cond, 0);
+        return;
+    }
     const bool odd = (sc->k - 1) & 1;  // set written by the CA kernel just run
     PhaseB<T> ph;
     ph.res = odd ? v.res[1] : v.res[0];
@@ -500,7 +516,7 @@ bicg_b(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
 // b = (source*rho/dt)*(-vol) in FP64, DP = 0, max|b|.
 __global__ void __launch_bounds__(kBlock)
 mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
-             double c1, double c2, double* b, double* x) {
+             double c1, double c2, double* b, double* x, double* r_copy) {
     __shared__ double sh[32];
     double m = 0.0;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
@@ -508,13 +524,17 @@ mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
         const double r = (src[q] * c1) * c2;
         b[q] = r;
         x[q] = 0.0;
+        if (r_copy) r_copy[q] = r;
         m = nanmax(m, fabs(r));
     }
     const double bm = block_max<kBlock>(m, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = bm;
     if (arrive_last(sc)) {
         const double mx = finish<true>(part, sh);
-        if (threadIdx.x == 0) { sc->max_b = mx; sc->scale = mx; sc->counter = 0u; }
+        if (threadIdx.x == 0) {
+            sc->max_b = mx; sc->scale = mx; sc->true_res = mx;
+            sc->outer = 0; sc->total = 0; sc->counter = 0u;
+        }
     }
 }
 
@@ -685,7 +705,7 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
         const LapCoef<double> cfd = lap_coef<double>(g);
         const double kInnerTol = 1e-4;
         const int kMaxOuter = 40;
-        PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b, DP));
+        PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b, DP, nullptr));
         if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
         const double max_b = hs.max_b;
         int status = PF_OK, outer = 0, total = 0;
@@ -979,6 +999,261 @@ cudaError_t launch_vel_corr(const pf_grid* g, const double* DP, double scale,
     PF_LAUNCH("vel_corr", 0, vel_corr_kernel<<<cgrid(d), dim3(32, 8), 0, s>>>(d, DP, scale, 1.0 / g->dx, 1.0 / g->dy,
                                                      1.0 / g->dz, u, v, w));
     return cudaGetLastError();
+}
+
+
+// ============================================================================
+// Whole time step as one CUDA graph.
+//
+// The step (predictor, divergence, Poisson solve, p += DP, projection,
+// statistics) is captured once per plan; the BiCGStab iteration loop is a
+// conditional WHILE node whose body is (kernel B, kernel CA): kernel CA clears
+// the condition when the solve stops (converged, iteration limit, breakdown,
+// non-finite), so a whole step runs without any host synchronisation.  The
+// mixed-precision refinement is an outer WHILE node (inner pass, fold,
+// FP64 residual, control) cleared by the control kernel.  Every kernel that
+// can find the solve already stopped clears the condition as well, so each
+// loop ends after at most max_it iterations.
+// ============================================================================
+
+// Refinement control (one thread): after the FP64 residual of a pass, count the
+// pass and its inner iterations and decide whether another pass runs.
+__global__ void mixed_control(BicgScalars* sc, double min_res, int max_outer,
+                              int max_it, cudaGraphConditionalHandle cond) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    sc->outer += 1;
+    sc->total += sc->iter;
+    const double ratio = sc->max_b > 0.0 ? sc->true_res / sc->max_b : 0.0;
+    bool stop = true;
+    if (!(ratio == ratio) || isinf(ratio)) sc->status = PF_NONFINITE;
+    else if (ratio <= min_res) sc->status = PF_OK;
+    else if (sc->outer >= max_outer || sc->total >= max_it) sc->status = PF_MAXIT;
+    else stop = false;
+    sc->max_res = ratio;
+    if (stop) cudaGraphSetConditional(cond, 0);
+}
+
+// copy the solve's result next to the monitor statistics:
+// info[0] = max_res, info[1] = iterations, info[2] = status
+__global__ void step_info(const BicgScalars* sc, int mixed, double* info) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    info[0] = sc->max_res;
+    info[1] = double(mixed ? sc->total : sc->iter);
+    info[2] = double(sc->status);
+}
+
+struct StepPlan {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static int capture_begin(cudaStream_t cs, cudaGraph_t target) {
+    cudaError_t e = target ? cudaStreamBeginCaptureToGraph(cs, target, nullptr, nullptr, 0,
+                                                          cudaStreamCaptureModeThreadLocal)
+                           : cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    return e == cudaSuccess ? PF_OK : PF_ERR_CUDA;
+}
+
+static int capture_end(cudaStream_t cs, cudaGraph_t* g) {
+    return cudaStreamEndCapture(cs, g) == cudaSuccess ? PF_OK : PF_ERR_CUDA;
+}
+
+// Re-arms a WHILE condition (the default value is applied only when the
+// whole graph is launched, not each time a nested loop is entered).
+__global__ void arm_condition(cudaGraphConditionalHandle h) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) cudaGraphSetConditional(h, 1);
+}
+
+// Adds a WHILE node after `dep` whose body is returned in *body.  With
+// `make_handle` the handle (default 1 at every graph launch) is created here
+// and written to *handle; otherwise *handle is used as given.
+static int add_while(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphNode_t* node,
+                     cudaGraph_t* body, cudaGraphConditionalHandle* handle,
+                     bool make_handle = true) {
+    if (make_handle &&
+        cudaGraphConditionalHandleCreate(handle, g, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+        return PF_ERR_CUDA;
+    cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
+    prm.conditional.handle = *handle;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    if (cudaGraphAddNode(node, g, dep ? &dep : nullptr, dep ? 1 : 0, &prm) != cudaSuccess)
+        return PF_ERR_CUDA;
+    *body = prm.conditional.phGraph_out[0];
+    return PF_OK;
+}
+
+static int add_child(cudaGraph_t g, cudaGraphNode_t dep, cudaGraph_t child,
+                     cudaGraphNode_t* node) {
+    return cudaGraphAddChildGraphNode(node, g, dep ? &dep : nullptr, dep ? 1 : 0, child) ==
+                   cudaSuccess ? PF_OK : PF_ERR_CUDA;
+}
+
+// Plan workspace: [div: n doubles][scalar block][reduction partials][region R]
+// R holds, at different times of the step, the predictor's stage buffers, the
+// solver vectors and the statistics scratch.  The scalar block is written only
+// by the solver kernels.
+size_t step_plan_ws_bytes(const pf_grid* g, int prec) {
+    const size_t n = (size_t)g->nx * g->ny * g->nz;
+    size_t vecs = prec == PF_FP64 ? 8 * align256(n * sizeof(double))
+                                  : 11 * align256(n * sizeof(double));
+    size_t r = std::max(std::max(predictor_ws_bytes(g, prec), vecs), stats_ws_bytes(g));
+    return align256(n * sizeof(double)) + align256(sizeof(BicgScalars)) +
+           align256(kNumPartials * kMaxPartials * sizeof(double)) + r;
+}
+
+int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
+                     double* w, double* p, double* DP, double mu, double rho,
+                     double dt, double min_res, int max_it, void* ws,
+                     double* stats, void** out) {
+    Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
+    const size_t n = (size_t)d.n;
+    char* ptr = (char*)ws;
+    double* div = (double*)ptr; ptr += align256(n * sizeof(double));
+    BicgScalars* sc = (BicgScalars*)ptr; ptr += align256(sizeof(BicgScalars));
+    double* part = (double*)ptr; ptr += align256(kNumPartials * kMaxPartials * sizeof(double));
+    char* R = ptr;
+    const int gp = pointwise_grid(d.n);
+    const double vol = (g->dx * g->dy) * g->dz;
+    const double c1 = rho / dt, c2 = -1.0 * vol;
+    max_it = std::max(max_it, 1);
+    dim3 blk2(32, 8);
+    // FP64 vectors, or FP32 vectors + correction followed by b and r (FP64)
+    char* vp = R;
+    BicgVecs<double> v64 = carve<double>(vp, n);
+    vp = R;
+    BicgVecs<float> v32 = carve<float>(vp, n);
+    float* e32 = (float*)vp;
+    double* bb = (double*)(R + 9 * align256(n * sizeof(double)));
+    double* rr = (double*)(R + 10 * align256(n * sizeof(double)));
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return PF_ERR_CUDA;
+    prof_suspend(true);
+    StepPlan* plan = new StepPlan();
+    int rc = PF_OK;
+    do {
+        if (cudaGraphCreate(&plan->graph, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
+        cudaGraph_t G = plan->graph;
+        // ---- segment 1: predictor, divergence, solver set-up
+        cudaGraph_t seg1 = nullptr;
+        if ((rc = capture_begin(cs, nullptr))) break;
+        launch_predictor(g, prec, rk4, u, v, w, nullptr, mu, rho, nullptr, dt, R, cs);
+        launch_div(g, u, v, w, div, cs);
+        if (prec == PF_FP64) {
+            const LapCoef<double> cf = lap_coef<double>(g);
+            const Tiling ta = make_tiling(d, 8 * PhaseCA<double>::R);
+            bicg_init<double, false><<<gp, kBlock, 0, cs>>>(d, sc, part, div, c1, c2, v64, DP,
+                                                           max_it, min_res);
+            bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v64, DP);
+        } else {
+            mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, div, c1, c2, bb, DP, rr);
+        }
+        if ((rc = capture_end(cs, &seg1))) break;
+        cudaGraphNode_t n1, nw;
+        if ((rc = add_child(G, nullptr, seg1, &n1))) break;
+        cudaGraphDestroy(seg1);
+        cudaGraph_t body;
+        cudaGraphConditionalHandle h;
+        if ((rc = add_while(G, n1, &nw, &body, &h))) break;
+        if (prec == PF_FP64) {
+            const LapCoef<double> cf = lap_coef<double>(g);
+            const Tiling ta = make_tiling(d, 8 * PhaseCA<double>::R);
+            const Tiling tb = make_tiling(d, 8 * PhaseB<double>::R);
+            if ((rc = capture_begin(cs, body))) break;
+            bicg_b<double><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, v64, 1, h);
+            bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v64, DP, 1, h);
+            if ((rc = capture_end(cs, &body))) break;
+        } else {
+            const LapCoef<float> cf = lap_coef<float>(g);
+            const LapCoef<double> cfd = lap_coef<double>(g);
+            const Tiling ta = make_tiling(d, 8 * PhaseCA<float>::R);
+            const Tiling tb = make_tiling(d, 8 * PhaseB<float>::R);
+            const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
+            const double kInnerTol = 1e-4;
+            // outer body: inner set-up, inner WHILE, fold + residual + control
+            cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;
+            if ((rc = capture_begin(cs, nullptr))) break;
+            bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, rr, 0.0, 0.0, v32, e32,
+                                                         max_it, kInnerTol);
+            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32);
+            if ((rc = capture_end(cs, &pre))) break;
+            cudaGraphNode_t b0, b1, bw, b3;
+            cudaGraphConditionalHandle hi;
+            if (cudaGraphConditionalHandleCreate(&hi, body, 1, cudaGraphCondAssignDefault) !=
+                cudaSuccess) { rc = PF_ERR_CUDA; break; }
+            {
+                // kernel node of the outer body (the graph that owns the
+                // inner loop) that re-arms the inner condition every pass
+                cudaKernelNodeParams kp;
+                std::memset(&kp, 0, sizeof(kp));
+                void* args[] = {&hi};
+                kp.func = (void*)arm_condition;
+                kp.gridDim = dim3(1);
+                kp.blockDim = dim3(32);
+                kp.kernelParams = args;
+                if (cudaGraphAddKernelNode(&b0, body, nullptr, 0, &kp) != cudaSuccess) {
+                    rc = PF_ERR_CUDA; break;
+                }
+            }
+            if ((rc = add_child(body, b0, pre, &b1))) break;
+            cudaGraphDestroy(pre);
+            if ((rc = add_while(body, b1, &bw, &inner_body, &hi, false))) break;
+            if ((rc = capture_begin(cs, inner_body))) break;
+            bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, v32, 1, hi);
+            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32, 1, hi);
+            if ((rc = capture_end(cs, &inner_body))) break;
+            if ((rc = capture_begin(cs, nullptr))) break;
+            fold_correction<float><<<gp, kBlock, 0, cs>>>(d, sc, e32, DP);
+            mixed_residual<<<tiled_grid(tld), blk2, 0, cs>>>(d, tld, cfd, sc, part, bb, DP, rr);
+            mixed_control<<<1, 32, 0, cs>>>(sc, min_res, 40, max_it, h);
+            if ((rc = capture_end(cs, &post))) break;
+            if ((rc = add_child(body, bw, post, &b3))) break;
+            cudaGraphDestroy(post);
+        }
+        // ---- segment 3: p += DP, projection, statistics
+        cudaGraph_t seg3 = nullptr;
+        cudaGraphNode_t n3;
+        if ((rc = capture_begin(cs, nullptr))) break;
+        step_info<<<1, 32, 0, cs>>>(sc, prec == PF_MIXED ? 1 : 0, stats + 5);
+        add_inplace<<<gp, kBlock, 0, cs>>>(d.n, DP, p);
+        launch_vel_corr(g, DP, dt / rho, u, v, w, cs);
+        launch_stats(g, u, v, w, stats, R, cs);
+        if ((rc = capture_end(cs, &seg3))) break;
+        if ((rc = add_child(G, nw, seg3, &n3))) break;
+        cudaGraphDestroy(seg3);
+        if (cudaGraphInstantiate(&plan->exec, G, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
+    } while (0);
+    prof_suspend(false);
+    if (rc == PF_OK &&
+        (cudaMemsetAsync(sc, 0, sizeof(BicgScalars), cs) != cudaSuccess ||
+         cudaStreamSynchronize(cs) != cudaSuccess))
+        rc = PF_ERR_CUDA;
+    cudaStreamDestroy(cs);
+    if (rc != PF_OK) {
+        if (plan->exec) cudaGraphExecDestroy(plan->exec);
+        if (plan->graph) cudaGraphDestroy(plan->graph);
+        delete plan;
+        cudaGetLastError();
+        return rc;
+    }
+    *out = plan;
+    return PF_OK;
+}
+
+int step_plan_launch(void* plan, int nsteps, cudaStream_t s) {
+    StepPlan* pl = (StepPlan*)plan;
+    for (int i = 0; i < nsteps; ++i)
+        if (cudaGraphLaunch(pl->exec, s) != cudaSuccess) return PF_ERR_CUDA;
+    return PF_OK;
+}
+
+int step_plan_destroy(void* plan) {
+    StepPlan* pl = (StepPlan*)plan;
+    if (!pl) return PF_OK;
+    if (pl->exec) cudaGraphExecDestroy(pl->exec);
+    if (pl->graph) cudaGraphDestroy(pl->graph);
+    delete pl;
+    return PF_OK;
 }
 
 }  // namespace pf

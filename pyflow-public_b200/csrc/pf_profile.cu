@@ -68,7 +68,13 @@ thread_local int t_slot = -1;
 
 }  // namespace
 
-bool prof_on() { return g_on; }
+// profiling is suspended while a step graph is being captured: event records
+// are not allowed inside conditional graph bodies
+static thread_local int t_suspend = 0;
+
+bool prof_on() { return g_on && t_suspend == 0; }
+
+void prof_suspend(bool on) { t_suspend += on ? 1 : -1; }
 
 void prof_begin(const char* name, cudaStream_t s) {
     std::lock_guard<std::mutex> lk(g_mu);

@@ -7,6 +7,7 @@
 namespace pf {
 
 bool prof_on();
+void prof_suspend(bool on);
 void prof_begin(const char* name, cudaStream_t s);
 void prof_end(cudaStream_t s);
 

@@ -1,0 +1,72 @@
+"""Graph-captured time steps (pf_step_plan_*).
+
+A StepPlan binds one set of device fields (u, v, w, p, DP) and captures a whole
+Domain.forwardStep -- predictor, divergence, Poisson solve with device-side
+convergence loops, projection and the monitor statistics -- as one CUDA graph.
+``launch(n)`` enqueues n steps without any host synchronisation; ``stats()``
+reads the last step's statistics (max|u|, max|v|, max|w|, TKE, max|div u|,
+max_res, iterations, status).
+"""
+import ctypes
+
+import torch
+
+from . import _lib as L
+from . import ops
+
+_lib = L.lib()
+_lib.pf_step_plan_workspace_bytes.argtypes = [ctypes.POINTER(L.Grid), ctypes.c_int]
+_lib.pf_step_plan_workspace_bytes.restype = ctypes.c_size_t
+_lib.pf_step_plan_create.argtypes = [
+    ctypes.POINTER(L.Grid), ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5 + [
+    ctypes.c_double] * 4 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+_lib.pf_step_plan_create.restype = ctypes.c_int
+_lib.pf_step_plan_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+_lib.pf_step_plan_launch.restype = ctypes.c_int
+_lib.pf_step_plan_destroy.argtypes = [ctypes.c_void_p]
+_lib.pf_step_plan_destroy.restype = ctypes.c_int
+
+STAT_NAMES = ("max_u", "max_v", "max_w", "tke", "max_div", "max_res",
+              "iterations", "status")
+
+
+class StepPlan:
+    def __init__(self, u, v, w, p, DP, spacing, mu, rho, dt, min_res=1e-10,
+                 max_it=20000, prec="fp64", rk4=True):
+        for t, nm in ((u, "u"), (v, "v"), (w, "w"), (p, "p"), (DP, "DP")):
+            ops._check(t, u.shape, torch.float64, nm)
+        self.fields = (u, v, w, p, DP)
+        self.grid = ops.grid(u.shape, spacing)
+        pr = ops.PREC[prec]
+        need = _lib.pf_step_plan_workspace_bytes(ctypes.byref(self.grid), pr)
+        self.ws = torch.empty(need, dtype=torch.uint8, device=u.device)
+        self.stats_dev = torch.zeros(8, dtype=torch.float64, device=u.device)
+        self.cells = u.numel()
+        self._h = ctypes.c_void_p(0)
+        # the fields must be ready: wait for the stream that produced them
+        torch.cuda.current_stream(u.device).synchronize()
+        L.check("pf_step_plan_create", _lib.pf_step_plan_create(
+            ctypes.byref(self.grid), pr, 1 if rk4 else 0, *(ops._p(t) for t in self.fields),
+            float(mu), float(rho), float(dt), float(min_res), int(max_it),
+            ops._p(self.ws), self.ws.numel(), ops._p(self.stats_dev),
+            ctypes.byref(self._h)))
+
+    def launch(self, nsteps=1, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream(self.ws.device)
+        L.check("pf_step_plan_launch", _lib.pf_step_plan_launch(
+            self._h, int(nsteps), ctypes.c_void_p(s.cuda_stream)))
+
+    def stats(self):
+        return dict(zip(STAT_NAMES, self.stats_dev.cpu().tolist()))
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.pf_step_plan_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

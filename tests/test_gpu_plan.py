@@ -1,0 +1,74 @@
+"""Graph-captured steps (device-side convergence loops) reproduce the
+host-driven pf_forward_step: bit for bit in FP64, and to the mixed-precision
+tolerance in the mixed form; the per-step statistics match the stats kernel."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prec,shape", [("fp64", (32, 32, 32)), ("fp64", (24, 20, 36)),
+                                        ("mixed", (32, 32, 32))])
+def test_plan_matches_forward_step(prec, shape):
+    import pyflow_b200.initial as ic
+    import pyflow_b200.ops as ops
+    from pyflow_b200.plan import StepPlan
+    sp = tuple(2 * np.pi / n for n in shape)
+    f0 = [torch.tensor(a, device="cuda") for a in ic.spectral_velocity(shape, k0=4.0, seed=5)]
+    nu, dt, steps = 0.01, 0.005, 4
+    a = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    infos = []
+    for _ in range(steps):
+        info = ops.forward_step(*a, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec)
+        infos.append(info.iterations)
+    b = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    plan = StepPlan(*b, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec)
+    plan.launch(steps)
+    torch.cuda.synchronize()
+    st = plan.stats()
+    plan.close()
+    assert st["status"] == 0 and st["max_res"] <= 1e-10
+    if prec == "fp64":
+        for x, y in zip(a[:4], b[:4]):
+            assert torch.equal(x, y)
+        assert int(st["iterations"]) == infos[-1]
+    else:
+        for x, y in zip(a[:3], b[:3]):
+            assert (x - y).abs().max().item() <= 1e-7 * y.abs().max().item()
+    ref = ops.stats(*b[:3], sp).cpu().numpy()
+    np.testing.assert_allclose([st["max_u"], st["max_v"], st["max_w"], st["tke"], st["max_div"]],
+                               ref, rtol=1e-14, atol=1e-18)
+
+
+def test_plans_run_concurrently_on_streams():
+    """Several plans on their own streams give the same results as alone."""
+    import pyflow_b200.initial as ic
+    from pyflow_b200.plan import StepPlan
+    shapes = [(16, 16, 16), (24, 24, 24), (32, 32, 32)]
+    alone, mixed = [], []
+    for rep in range(2):
+        plans, fields = [], []
+        for i, sh in enumerate(shapes):
+            sp = tuple(2 * np.pi / n for n in sh)
+            f = [torch.tensor(a, device="cuda") for a in ic.spectral_velocity(sh, seed=20 + i)]
+            f += [torch.zeros_like(f[0]), torch.zeros_like(f[0])]
+            fields.append(f)
+            plans.append(StepPlan(*f, sp, 0.02, 1.0, 0.004, min_res=1e-10, max_it=5000))
+        torch.cuda.synchronize()
+        if rep == 0:
+            for pl in plans:
+                pl.launch(3)
+                torch.cuda.synchronize()
+            alone = [f[0].clone() for f in fields]
+        else:
+            streams = [torch.cuda.Stream() for _ in plans]
+            for _ in range(3):
+                for pl, s in zip(plans, streams):
+                    pl.launch(1, stream=s)
+            torch.cuda.synchronize()
+            mixed = [f[0].clone() for f in fields]
+        for pl in plans:
+            pl.close()
+    for x, y in zip(alone, mixed):
+        assert torch.equal(x, y)

@@ -1,0 +1,60 @@
+"""Serving loop: host logic on CPU (request stream, percentiles, footprint),
+continuous batching and admission on the GPU."""
+import numpy as np
+import pytest
+import torch
+
+
+def test_percentile_and_stream():
+    import pyflow_b200.serving as S
+    assert S.percentile([1, 2, 3, 4], 50) == 2.5
+    assert S.percentile(list(range(101)), 99) == 99
+    reqs = S.stream_requests(600, rate=10.0)
+    assert {r.n for r in reqs} == {32, 48, 64, 96, 128, 192}
+    arr = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(arr) >= 0) and abs(np.mean(np.diff(arr)) - 0.1) < 0.02
+    assert all(abs(r.nu - 0.02 * 32 / r.n) < 1e-15 and r.seed == 1000 + r.id for r in reqs)
+
+
+def test_footprint_grows_with_grid():
+    import pyflow_b200.serving as S
+    a, b = S.footprint_bytes(32), S.footprint_bytes(64)
+    assert b > 7 * a and a > 5 * 8 * 32 ** 3
+
+
+@pytest.mark.gpu
+def test_results_same_alone_and_in_mix():
+    import pyflow_b200.serving as S
+    reqs = [S.Request(id=i, n=n, seed=1000 + i, nu=0.02 * 32 / n, dt=0.01, steps=5,
+                      arrival=0.002 * i) for i, n in enumerate([16, 24, 32, 16, 24, 20])]
+    alone = {}
+    for r in reqs:
+        srv = S.Server(max_slots=1, prec="mixed", keep_fields=True)
+        res = srv.run([S.Request(**{**r.__dict__, "arrival": 0.0})])
+        assert res[0].status == "ok", res[0]
+        alone[r.id] = res[0]
+    srv = S.Server(max_slots=4, prec="mixed", keep_fields=True)
+    mixed = srv.run(reqs)
+    assert srv.max_active > 1
+    assert len(mixed) == len(reqs)
+    for m in mixed:
+        a = alone[m.id]
+        assert m.status == "ok"
+        for x, y in zip(m.fields, a.fields):
+            assert torch.equal(x, y)
+        assert m.stats["max_res"] <= 1e-10
+
+
+@pytest.mark.gpu
+def test_admission_by_free_memory():
+    import pyflow_b200.serving as S
+    one = S.footprint_bytes(24)
+    reqs = [S.Request(id=i, n=24, seed=1000 + i, nu=0.02, dt=0.01, steps=2) for i in range(4)]
+    reqs.append(S.Request(id=9, n=64, seed=7, nu=0.01, dt=0.01, steps=2))
+    # a fake free-HBM provider with room for exactly one 24^3 request
+    srv = S.Server(max_slots=8, free_hbm=lambda used: int(1.5 * one) - used, prec="fp64")
+    res = srv.run(reqs)
+    by = {r.id: r for r in res}
+    assert srv.max_active == 1
+    assert all(by[i].status == "ok" for i in range(4))
+    assert by[9].status == "rejected"
