@@ -15,7 +15,12 @@
  *    operation order; PF_MIXED keeps the velocity/pressure state in FP64, runs
  *    fluxes, RK4 stages and the Poisson matvec in FP32, and keeps FP64 for the
  *    Poisson residual recomputation, the BiCGStab inner products, the
- *    iterative-refinement outer loop and all global sums.
+ *    iterative-refinement outer loop and all global sums.  PF_MIXED_MG is
+ *    PF_MIXED whose FP32 refinement passes run BiCGStab right-preconditioned
+ *    by a geometric multigrid V-cycle (no counterpart in the reference, whose
+ *    BiCGStab is unpreconditioned); it needs every grid dimension to halve
+ *    down to a coarsest level of at most 4096 cells, and otherwise runs the
+ *    PF_MIXED passes.  Both mixed forms converge to the same FP64 tolerance.
  */
 #ifndef PYFLOW_B200_H
 #define PYFLOW_B200_H
@@ -43,13 +48,13 @@ enum pf_status {
     PF_ERR_TOO_LARGE = 7    /* grid exceeds the fixed scratch of pf_bicgstab_solve_noalloc */
 };
 
-enum pf_prec { PF_FP64 = 0, PF_MIXED = 1 };
+enum pf_prec { PF_FP64 = 0, PF_MIXED = 1, PF_MIXED_MG = 2 };
 
 /* Result of a Poisson solve (host struct, filled by the synchronous calls). */
 typedef struct pf_solve_info {
     double max_res;      /* max|r| / max|r0|, the reference's return value */
-    int iterations;      /* BiCGStab iterations (inner iterations for PF_MIXED) */
-    int outer;           /* refinement passes (PF_MIXED), 1 for PF_FP64 */
+    int iterations;      /* BiCGStab iterations (inner iterations for the mixed forms) */
+    int outer;           /* refinement passes (mixed forms), 1 for PF_FP64 */
     int status;          /* pf_status */
 } pf_solve_info;
 
@@ -195,9 +200,10 @@ int pf_bicgstab_solve_noalloc(const pf_grid* g, double rho, double dt,
  * workspace: predictor, divergence, Poisson solve with device-side
  * convergence loops (conditional WHILE nodes), p += DP, projection and the
  * monitor statistics (src/core/PyFlow.py:379-395).  Each launch advances one
- * step with no host synchronisation; stats (device, 8 doubles) receives
+ * step with no host synchronisation; stats (device, 10 doubles) receives
  * max|u|, max|v|, max|w|, TKE, max|div u|, max_res, iterations, status after
- * every step.  The workspace (pf_step_plan_workspace_bytes, 256-byte aligned)
+ * every step, and accumulates the iterations and the step count in
+ * stats[8], stats[9].  The workspace (pf_step_plan_workspace_bytes, 256-byte aligned)
  * belongs to the plan.  Plans of different fields may run concurrently on
  * different streams. */
 typedef struct pf_step_plan pf_step_plan;

@@ -12,7 +12,7 @@ LIB_PATH = os.path.join(_PKG, "libpyflow_b200.so")
 
 PF_OK, PF_ERR_BAD_ARG, PF_ERR_CUDA, PF_BREAKDOWN, PF_MAXIT, PF_NONFINITE, \
     PF_STAGNATION = range(7)
-PF_FP64, PF_MIXED = 0, 1
+PF_FP64, PF_MIXED, PF_MIXED_MG = 0, 1, 2
 
 
 class Grid(ctypes.Structure):

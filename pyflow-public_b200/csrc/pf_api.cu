@@ -20,7 +20,7 @@ bool grid_ok(const pf_grid* g) {
            (long long)g->nx * g->ny * g->nz < (1LL << 40);
 }
 
-bool prec_ok(int p) { return p == PF_FP64 || p == PF_MIXED; }
+bool prec_ok(int p) { return p == PF_FP64 || p == PF_MIXED || p == PF_MIXED_MG; }
 
 cudaStream_t S(void* s) { return (cudaStream_t)s; }
 

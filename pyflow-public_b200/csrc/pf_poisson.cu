@@ -39,242 +39,12 @@
 
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
+#include "pf_sweep.cuh"
+#include "pf_mg.cuh"
 #include "pf_profile.cuh"
 
 namespace pf {
 
-struct BicgScalars {
-    double rho1, rho2, alpha, omega, gamma, buf1, buf2;
-    double max_res0, max_res, min_res;
-    double scale;      // mixed: max|r| of the current refinement pass
-    double max_b;      // mixed: max|b|
-    double true_res;   // mixed: max|b - A x| of the last refinement pass
-    int outer, total;  // mixed graph mode: refinement passes, inner iterations
-    int k;             // index of the next CA kernel
-    int iter;          // completed iterations
-    int done;          // 0 running, 1 stopped, 2 stop after DP += alpha pp
-    int status, max_it;
-    unsigned int counter;
-    int pad[2];
-};
-
-template <typename T>
-struct LapCoef {
-    T c[3][3];
-};
-
-template <typename T>
-static LapCoef<T> lap_coef(const pf_grid* g) {
-    // metric_uniform.__init__ (metric_staggered.py:84-102) in FP64, then cast
-    const double dxi = 1.0 / g->dx, dyi = 1.0 / g->dy, dzi = 1.0 / g->dz;
-    const double vol = (g->dx * g->dy) * g->dz;
-    const double di[3] = {dxi, dyi, dzi};
-    LapCoef<T> c;
-    for (int q = 0; q < 3; ++q) {
-        c.c[q][0] = T((di[q] * di[q]) * (-1.0 * vol));
-        c.c[q][1] = T(((-2.0 * di[q]) * di[q]) * (-1.0 * vol));
-        c.c[q][2] = T((di[q] * di[q]) * (-1.0 * vol));
-    }
-    return c;
-}
-
-// rows of the tile owned by each thread: 4 for FP32, 2 for FP64
-template <typename T>
-struct Rows {
-    static constexpr int R = sizeof(T) == 4 ? 4 : 2;
-    static constexpr int TY = 8 * R;
-};
-
-struct Tiling {
-    int ntz, nty, ntx, xc;
-    long long ntiles;
-};
-
-static int num_sms() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
-
-static Tiling make_tiling(const Dims& d, int ty) {
-    Tiling t;
-    t.ntz = (d.nz + 31) / 32;
-    t.nty = (d.ny + ty - 1) / ty;
-    const long long yz = (long long)t.ntz * t.nty;
-    const long long want = (long long)num_sms() * 3;  // tiles to fill the GPU
-    long long xc = (yz * d.nx) / want;
-    xc = std::max<long long>(4, std::min<long long>(64, xc));
-    t.xc = (int)std::min<long long>(xc, d.nx);
-    t.ntx = (d.nx + t.xc - 1) / t.xc;
-    t.ntiles = yz * t.ntx;
-    return t;
-}
-
-static int tiled_grid(const Tiling& t) {
-    return (int)std::min<long long>(t.ntiles, std::min(num_sms() * 2, kMaxPartials));
-}
-
-static int pointwise_grid(long long n) {
-    long long b = (n + kBlock * 4 - 1) / (kBlock * 4);
-    return (int)std::max<long long>(1, std::min<long long>(b, std::min(num_sms() * 8, kMaxPartials)));
-}
-
-// --------------------------------------------------------------------------
-// Tiled 7-point sweep with one-plane-ahead prefetch.  The phase object Ph
-// provides
-//   Raw raw(q)  -- loads the operand inputs of cell q,
-//   T   op(raw) -- the stencil operand,
-//   Ext ext(q)  -- loads the epilogue inputs of an owned cell,
-//   epi(q, centre operand, A operand, raw, ext) -- consumes an owned cell.
-// Block: 32 x 8 threads; tile 32 (z) x 8R (y) x xc (x).
-// --------------------------------------------------------------------------
-template <typename T, class Ph>
-__device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
-                                      const LapCoef<T>& cf, Ph& ph) {
-    constexpr int R = Ph::R, TY = 8 * Ph::R;
-    using Raw = typename Ph::Raw;
-    using Ext = typename Ph::Ext;
-    __shared__ T sm[TY + 2][34];
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-    const long long plane = (long long)d.ny * d.nz;
-    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
-        const int tz = (int)(t % tl.ntz);
-        const long long rr = t / tl.ntz;
-        const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
-        const int k0 = tz * 32, j0 = tyy * TY, i0 = txx * tl.xc;
-        const int i1 = min(i0 + tl.xc, d.nx);
-        const int ez = min(32, d.nz - k0), ey = min(TY, d.ny - j0);
-        bool vr[R];
-        long long off[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int jl = ty + 8 * r;
-            vr[r] = (tx < ez) && (jl < ey);
-            off[r] = (long long)(j0 + jl) * d.nz + (k0 + tx);
-        }
-        // this thread's halo cell of each plane (at most 2*32 + 2*TY cells)
-        bool hv = false;
-        int hy = 0, hz = 0;
-        long long hoff = 0;
-        if (tid < 64) {
-            const int h = tid & 31;
-            hv = h < ez;
-            hz = h + 1;
-            if (tid < 32) { hy = 0; hoff = (long long)wrap(j0 - 1, d.ny) * d.nz + k0 + h; }
-            else { hy = ey + 1; hoff = (long long)wrap(j0 + ey, d.ny) * d.nz + k0 + h; }
-        } else if (tid < 64 + 2 * TY) {
-            const int u = tid - 64, h = u % TY;
-            hv = h < ey;
-            hy = h + 1;
-            if (u < TY) { hz = 0; hoff = (long long)(j0 + h) * d.nz + wrap(k0 - 1, d.nz); }
-            else { hz = ez + 1; hoff = (long long)(j0 + h) * d.nz + wrap(k0 + ez, d.nz); }
-        }
-        T opP[R], opC[R], opN[R];
-        Raw rawC[R], rawN[R];
-        Ext extC[R];
-        Raw hraw{};
-        {
-            const long long bm = (long long)wrap(i0 - 1, d.nx) * plane;
-            const long long b0 = (long long)i0 * plane;
-            const long long b1 = (long long)wrap(i0 + 1, d.nx) * plane;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (vr[r]) {
-                    opP[r] = ph.op(ph.raw(bm + off[r]));
-                    rawC[r] = ph.raw(b0 + off[r]);
-                    rawN[r] = ph.raw(b1 + off[r]);
-                    extC[r] = ph.ext(b0 + off[r]);
-                    opC[r] = ph.op(rawC[r]);
-                }
-            }
-            if (hv) hraw = ph.raw(b0 + hoff);
-        }
-        for (int i = i0; i < i1; ++i) {
-            const bool more = i + 1 < i1;
-            const long long bi = (long long)i * plane;
-            const long long bh = (long long)wrap(i + 1, d.nx) * plane;
-            const long long bn = (long long)wrap(i + 2, d.nx) * plane;
-            Raw rawNN[R];
-            Ext extN[R];
-            Raw hrawN{};
-            if (more) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    if (vr[r]) {
-                        rawNN[r] = ph.raw(bn + off[r]);
-                        extN[r] = ph.ext(bh + off[r]);
-                    }
-                }
-                if (hv) hrawN = ph.raw(bh + hoff);
-            }
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                if (vr[r]) sm[ty + 8 * r + 1][tx + 1] = opC[r];
-            if (hv) sm[hy][hz] = ph.op(hraw);
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (!vr[r]) continue;
-                opN[r] = ph.op(rawN[r]);
-                const int yy = ty + 8 * r + 1, zz = tx + 1;
-                T b = T(0);
-                b += opP[r] * cf.c[0][0];
-                b += opC[r] * cf.c[0][1];
-                b += opN[r] * cf.c[0][2];
-                b += sm[yy - 1][zz] * cf.c[1][0];
-                b += opC[r] * cf.c[1][1];
-                b += sm[yy + 1][zz] * cf.c[1][2];
-                b += sm[yy][zz - 1] * cf.c[2][0];
-                b += opC[r] * cf.c[2][1];
-                b += sm[yy][zz + 1] * cf.c[2][2];
-                ph.epi(bi + off[r], opC[r], b, rawC[r], extC[r]);
-            }
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                opP[r] = opC[r];
-                opC[r] = opN[r];
-                rawC[r] = rawN[r];
-                if (more) { rawN[r] = rawNN[r]; extC[r] = extN[r]; }
-            }
-            if (more) hraw = hrawN;
-        }
-    }
-}
-
-// Last-block completion: returns true in every thread of the last block.
-__device__ __forceinline__ bool arrive_last(BicgScalars* sc) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        const unsigned prev = atomicAdd(&sc->counter, 1u);
-        last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
-}
-
-// Sum (or max) of gridDim.x partials in a fixed order, by the calling block.
-template <bool MAX>
-__device__ double finish(const double* part, double* sh) {
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int nt = blockDim.x * blockDim.y;
-    double v = 0.0;
-    for (int b = tid; b < (int)gridDim.x; b += nt) {
-        const double x = ((volatile const double*)part)[b];
-        v = MAX ? nanmax(v, x) : v + x;
-    }
-    return MAX ? block_max<kBlock>(v, sh) : block_sum<kBlock>(v, sh);
-}
-
-__device__ __forceinline__ bool tid0() { return threadIdx.x == 0 && threadIdx.y == 0; }
 
 // Solver vectors.  set 0/1: res, pp, vv written by kernel CA of even/odd k.
 template <typename T>
@@ -542,7 +312,9 @@ mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
 // scale = max|r| of the residual the pass solved for).
 template <typename T>
 __global__ void __launch_bounds__(kBlock)
-fold_correction(Dims d, const BicgScalars* sc, const T* e, double* x) {
+fold_correction(Dims d, const BicgScalars* sc, const T* e, double* x, int guard = 0) {
+    // graph mode: a pass that ended non-finite or in breakdown is discarded
+    if (guard && (sc->status == PF_NONFINITE || sc->status == PF_BREAKDOWN)) return;
     const double s = sc->scale;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += (long long)gridDim.x * blockDim.x)
@@ -591,7 +363,6 @@ add_inplace(long long n, const double* a, double* p) {
 }
 
 // ------------------------------------------------------------ workspace
-static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 static constexpr int kNumPartials = 4;
 
@@ -705,6 +476,13 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
         const LapCoef<double> cfd = lap_coef<double>(g);
         const double kInnerTol = 1e-4;
         const int kMaxOuter = 40;
+        // PF_MIXED_MG: the FP32 passes run the multigrid-preconditioned solver
+        // (its vectors share the same region) when the grid coarsens
+        MgPlan mg;
+        if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
+            const int rc = mg_setup(g, region, &mg);
+            if (rc != PF_OK && rc != PF_ERR_BAD_ARG) return rc;
+        }
         PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b, DP, nullptr));
         if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
         const double max_b = hs.max_b;
@@ -727,16 +505,23 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
             const double* rhs = outer == 0 ? b : r;
             ++outer;
             if (!use64) {
-                PF_LAUNCH("bicg_init_f32", s, bicg_init<float, true><<<gp, kBlock, 0, s>>>(
-                    d, sc, part, rhs, 0.0, 0.0, v32, e32, max_it - total, kInnerTol));
-                const int rc = run_iterations<float>(d, cf, sc, part, v32, e32, s, &hs);
-                if (rc) return rc;
+                float* e = e32;
+                if (mg.L) {
+                    const int rc = mg_inner_solve(mg, sc, part, rhs, kInnerTol, max_it - total, s, &hs);
+                    if (rc) return rc;
+                    e = mg.e;
+                } else {
+                    PF_LAUNCH("bicg_init_f32", s, bicg_init<float, true><<<gp, kBlock, 0, s>>>(
+                        d, sc, part, rhs, 0.0, 0.0, v32, e32, max_it - total, kInnerTol));
+                    const int rc = run_iterations<float>(d, cf, sc, part, v32, e32, s, &hs);
+                    if (rc) return rc;
+                }
                 total += hs.iter;
                 if (hs.status == PF_NONFINITE || hs.status == PF_BREAKDOWN) {
                     use64 = true;  // discard this pass: x is unchanged
                     continue;
                 }
-                PF_LAUNCH("fold_correction", s, fold_correction<float><<<gp, kBlock, 0, s>>>(d, sc, e32, DP));
+                PF_LAUNCH("fold_correction", s, fold_correction<float><<<gp, kBlock, 0, s>>>(d, sc, e, DP));
             } else {
                 // an FP64 pass finishes the solve: its tolerance is the
                 // remaining reduction
@@ -1011,7 +796,9 @@ cudaError_t launch_vel_corr(const pf_grid* g, const double* DP, double scale,
 // the condition when the solve stops (converged, iteration limit, breakdown,
 // non-finite), so a whole step runs without any host synchronisation.  The
 // mixed-precision refinement is an outer WHILE node (inner pass, fold,
-// FP64 residual, control) cleared by the control kernel.  Every kernel that
+// FP64 residual, control) cleared by the control kernel.  A pass that ends
+// non-finite or in breakdown is discarded and ends the solve with that status
+// (the host-driven solve switches to FP64 passes instead).  Every kernel that
 // can find the solve already stopped clears the condition as well, so each
 // loop ends after at most max_it iterations.
 // ============================================================================
@@ -1023,10 +810,13 @@ __global__ void mixed_control(BicgScalars* sc, double min_res, int max_outer,
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     sc->outer += 1;
     sc->total += sc->iter;
-    const double ratio = sc->max_b > 0.0 ? sc->true_res / sc->max_b : 0.0;
+    // max|b| == 0: nothing to solve; a NaN max|b| gives a NaN ratio
+    const double ratio = sc->max_b == 0.0 ? 0.0 : sc->true_res / sc->max_b;
+    const int pass = sc->status;  // status of the inner pass just run
     bool stop = true;
     if (!(ratio == ratio) || isinf(ratio)) sc->status = PF_NONFINITE;
     else if (ratio <= min_res) sc->status = PF_OK;
+    else if (pass == PF_NONFINITE || pass == PF_BREAKDOWN) sc->status = pass;
     else if (sc->outer >= max_outer || sc->total >= max_it) sc->status = PF_MAXIT;
     else stop = false;
     sc->max_res = ratio;
@@ -1034,12 +824,16 @@ __global__ void mixed_control(BicgScalars* sc, double min_res, int max_outer,
 }
 
 // copy the solve's result next to the monitor statistics:
-// info[0] = max_res, info[1] = iterations, info[2] = status
+// info[0] = max_res, info[1] = iterations, info[2] = status,
+// info[3] += iterations and info[4] += 1 (running totals over launches)
 __global__ void step_info(const BicgScalars* sc, int mixed, double* info) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double it = double(mixed ? sc->total : sc->iter);
     info[0] = sc->max_res;
-    info[1] = double(mixed ? sc->total : sc->iter);
+    info[1] = it;
     info[2] = double(sc->status);
+    info[3] += it;
+    info[4] += 1.0;
 }
 
 struct StepPlan {
@@ -1170,12 +964,24 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
             const Tiling tb = make_tiling(d, 8 * PhaseB<float>::R);
             const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
             const double kInnerTol = 1e-4;
+            // PF_MIXED_MG: multigrid-preconditioned inner passes when the grid
+            // coarsens (vectors in the same region)
+            MgPlan mg;
+            if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
+                const int e = mg_setup(g, R, &mg);
+                if (e != PF_OK && e != PF_ERR_BAD_ARG) { rc = e; break; }
+            }
+            float* ecorr = mg.L ? mg.e : e32;
             // outer body: inner set-up, inner WHILE, fold + residual + control
             cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;
             if ((rc = capture_begin(cs, nullptr))) break;
-            bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, rr, 0.0, 0.0, v32, e32,
-                                                         max_it, kInnerTol);
-            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32);
+            if (mg.L) {
+                mg_enqueue_init(mg, sc, part, rr, kInnerTol, max_it, cs);
+            } else {
+                bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, rr, 0.0, 0.0, v32, e32,
+                                                             max_it, kInnerTol);
+                bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32);
+            }
             if ((rc = capture_end(cs, &pre))) break;
             cudaGraphNode_t b0, b1, bw, b3;
             cudaGraphConditionalHandle hi;
@@ -1199,11 +1005,17 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
             cudaGraphDestroy(pre);
             if ((rc = add_while(body, b1, &bw, &inner_body, &hi, false))) break;
             if ((rc = capture_begin(cs, inner_body))) break;
-            bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, v32, 1, hi);
-            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32, 1, hi);
+            if (mg.L) {
+                // two iterations per pass of the body: the p buffers alternate
+                mg_enqueue_iteration(mg, sc, part, 0, cs, 1, hi);
+                mg_enqueue_iteration(mg, sc, part, 1, cs, 1, hi);
+            } else {
+                bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, v32, 1, hi);
+                bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32, 1, hi);
+            }
             if ((rc = capture_end(cs, &inner_body))) break;
             if ((rc = capture_begin(cs, nullptr))) break;
-            fold_correction<float><<<gp, kBlock, 0, cs>>>(d, sc, e32, DP);
+            fold_correction<float><<<gp, kBlock, 0, cs>>>(d, sc, ecorr, DP, 1);
             mixed_residual<<<tiled_grid(tld), blk2, 0, cs>>>(d, tld, cfd, sc, part, bb, DP, rr);
             mixed_control<<<1, 32, 0, cs>>>(sc, min_res, 40, max_it, h);
             if ((rc = capture_end(cs, &post))) break;
@@ -1214,7 +1026,7 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
         cudaGraph_t seg3 = nullptr;
         cudaGraphNode_t n3;
         if ((rc = capture_begin(cs, nullptr))) break;
-        step_info<<<1, 32, 0, cs>>>(sc, prec == PF_MIXED ? 1 : 0, stats + 5);
+        step_info<<<1, 32, 0, cs>>>(sc, prec != PF_FP64 ? 1 : 0, stats + 5);
         add_inplace<<<gp, kBlock, 0, cs>>>(d.n, DP, p);
         launch_vel_corr(g, DP, dt / rho, u, v, w, cs);
         launch_stats(g, u, v, w, stats, R, cs);

@@ -1,0 +1,246 @@
+// pf_sweep.cuh -- solver building blocks shared by the Krylov and multigrid
+// kernels: the device scalar block, Laplacian coefficients, the tiled 7-point
+// sweep with one-plane-ahead prefetch, and last-block reductions.
+#pragma once
+#include <algorithm>
+
+#include "pf_common.cuh"
+
+namespace pf {
+
+struct BicgScalars {
+    double rho1, rho2, alpha, omega, gamma, buf1, buf2;
+    double max_res0, max_res, min_res;
+    double scale;      // mixed: max|r| of the current refinement pass
+    double max_b;      // mixed: max|b|
+    double true_res;   // mixed: max|b - A x| of the last refinement pass
+    int outer, total;  // mixed graph mode: refinement passes, inner iterations
+    int k;             // index of the next CA kernel
+    int iter;          // completed iterations
+    int done;          // 0 running, 1 stopped, 2 stop after DP += alpha pp
+    int status, max_it;
+    unsigned int counter;
+    int pad[2];
+};
+
+template <typename T>
+struct LapCoef {
+    T c[3][3];
+};
+
+template <typename T>
+static inline LapCoef<T> lap_coef(const pf_grid* g) {
+    // metric_uniform.__init__ (metric_staggered.py:84-102) in FP64, then cast
+    const double dxi = 1.0 / g->dx, dyi = 1.0 / g->dy, dzi = 1.0 / g->dz;
+    const double vol = (g->dx * g->dy) * g->dz;
+    const double di[3] = {dxi, dyi, dzi};
+    LapCoef<T> c;
+    for (int q = 0; q < 3; ++q) {
+        c.c[q][0] = T((di[q] * di[q]) * (-1.0 * vol));
+        c.c[q][1] = T(((-2.0 * di[q]) * di[q]) * (-1.0 * vol));
+        c.c[q][2] = T((di[q] * di[q]) * (-1.0 * vol));
+    }
+    return c;
+}
+
+// rows of the tile owned by each thread: 4 for FP32, 2 for FP64
+template <typename T>
+struct Rows {
+    static constexpr int R = sizeof(T) == 4 ? 4 : 2;
+    static constexpr int TY = 8 * R;
+};
+
+struct Tiling {
+    int ntz, nty, ntx, xc;
+    long long ntiles;
+};
+
+static inline int num_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+static inline Tiling make_tiling(const Dims& d, int ty) {
+    Tiling t;
+    t.ntz = (d.nz + 31) / 32;
+    t.nty = (d.ny + ty - 1) / ty;
+    const long long yz = (long long)t.ntz * t.nty;
+    const long long want = (long long)num_sms() * 3;  // tiles to fill the GPU
+    long long xc = (yz * d.nx) / want;
+    xc = std::max<long long>(4, std::min<long long>(64, xc));
+    t.xc = (int)std::min<long long>(xc, d.nx);
+    t.ntx = (d.nx + t.xc - 1) / t.xc;
+    t.ntiles = yz * t.ntx;
+    return t;
+}
+
+static inline int tiled_grid(const Tiling& t) {
+    return (int)std::min<long long>(t.ntiles, std::min(num_sms() * 2, kMaxPartials));
+}
+
+static inline int pointwise_grid(long long n) {
+    long long b = (n + kBlock * 4 - 1) / (kBlock * 4);
+    return (int)std::max<long long>(1, std::min<long long>(b, std::min(num_sms() * 8, kMaxPartials)));
+}
+
+// --------------------------------------------------------------------------
+// Tiled 7-point sweep with one-plane-ahead prefetch.  The phase object Ph
+// provides
+//   Raw raw(q)  -- loads the operand inputs of cell q,
+//   T   op(raw) -- the stencil operand,
+//   Ext ext(q)  -- loads the epilogue inputs of an owned cell,
+//   epi(q, centre operand, A operand, raw, ext) -- consumes an owned cell.
+// Block: 32 x 8 threads; tile 32 (z) x 8R (y) x xc (x).
+// --------------------------------------------------------------------------
+template <typename T, class Ph>
+__device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
+                                      const LapCoef<T>& cf, Ph& ph) {
+    constexpr int R = Ph::R, TY = 8 * Ph::R;
+    using Raw = typename Ph::Raw;
+    using Ext = typename Ph::Ext;
+    __shared__ T sm[TY + 2][34];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const long long plane = (long long)d.ny * d.nz;
+    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+        const int tz = (int)(t % tl.ntz);
+        const long long rr = t / tl.ntz;
+        const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
+        const int k0 = tz * 32, j0 = tyy * TY, i0 = txx * tl.xc;
+        const int i1 = min(i0 + tl.xc, d.nx);
+        const int ez = min(32, d.nz - k0), ey = min(TY, d.ny - j0);
+        bool vr[R];
+        long long off[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int jl = ty + 8 * r;
+            vr[r] = (tx < ez) && (jl < ey);
+            off[r] = (long long)(j0 + jl) * d.nz + (k0 + tx);
+        }
+        // this thread's halo cell of each plane (at most 2*32 + 2*TY cells)
+        bool hv = false;
+        int hy = 0, hz = 0;
+        long long hoff = 0;
+        if (tid < 64) {
+            const int h = tid & 31;
+            hv = h < ez;
+            hz = h + 1;
+            if (tid < 32) { hy = 0; hoff = (long long)wrap(j0 - 1, d.ny) * d.nz + k0 + h; }
+            else { hy = ey + 1; hoff = (long long)wrap(j0 + ey, d.ny) * d.nz + k0 + h; }
+        } else if (tid < 64 + 2 * TY) {
+            const int u = tid - 64, h = u % TY;
+            hv = h < ey;
+            hy = h + 1;
+            if (u < TY) { hz = 0; hoff = (long long)(j0 + h) * d.nz + wrap(k0 - 1, d.nz); }
+            else { hz = ez + 1; hoff = (long long)(j0 + h) * d.nz + wrap(k0 + ez, d.nz); }
+        }
+        T opP[R], opC[R], opN[R];
+        Raw rawC[R], rawN[R];
+        Ext extC[R];
+        Raw hraw{};
+        {
+            const long long bm = (long long)wrap(i0 - 1, d.nx) * plane;
+            const long long b0 = (long long)i0 * plane;
+            const long long b1 = (long long)wrap(i0 + 1, d.nx) * plane;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (vr[r]) {
+                    opP[r] = ph.op(ph.raw(bm + off[r]));
+                    rawC[r] = ph.raw(b0 + off[r]);
+                    rawN[r] = ph.raw(b1 + off[r]);
+                    extC[r] = ph.ext(b0 + off[r]);
+                    opC[r] = ph.op(rawC[r]);
+                }
+            }
+            if (hv) hraw = ph.raw(b0 + hoff);
+        }
+        for (int i = i0; i < i1; ++i) {
+            const bool more = i + 1 < i1;
+            const long long bi = (long long)i * plane;
+            const long long bh = (long long)wrap(i + 1, d.nx) * plane;
+            const long long bn = (long long)wrap(i + 2, d.nx) * plane;
+            Raw rawNN[R];
+            Ext extN[R];
+            Raw hrawN{};
+            if (more) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (vr[r]) {
+                        rawNN[r] = ph.raw(bn + off[r]);
+                        extN[r] = ph.ext(bh + off[r]);
+                    }
+                }
+                if (hv) hrawN = ph.raw(bh + hoff);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (vr[r]) sm[ty + 8 * r + 1][tx + 1] = opC[r];
+            if (hv) sm[hy][hz] = ph.op(hraw);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (!vr[r]) continue;
+                opN[r] = ph.op(rawN[r]);
+                const int yy = ty + 8 * r + 1, zz = tx + 1;
+                T b = T(0);
+                b += opP[r] * cf.c[0][0];
+                b += opC[r] * cf.c[0][1];
+                b += opN[r] * cf.c[0][2];
+                b += sm[yy - 1][zz] * cf.c[1][0];
+                b += opC[r] * cf.c[1][1];
+                b += sm[yy + 1][zz] * cf.c[1][2];
+                b += sm[yy][zz - 1] * cf.c[2][0];
+                b += opC[r] * cf.c[2][1];
+                b += sm[yy][zz + 1] * cf.c[2][2];
+                ph.epi(bi + off[r], opC[r], b, rawC[r], extC[r]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                opP[r] = opC[r];
+                opC[r] = opN[r];
+                rawC[r] = rawN[r];
+                if (more) { rawN[r] = rawNN[r]; extC[r] = extN[r]; }
+            }
+            if (more) hraw = hrawN;
+        }
+    }
+}
+
+// Last-block completion: returns true in every thread of the last block.
+__device__ __forceinline__ bool arrive_last(BicgScalars* sc) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const unsigned prev = atomicAdd(&sc->counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// Sum (or max) of gridDim.x partials in a fixed order, by the calling block.
+template <bool MAX>
+__device__ double finish(const double* part, double* sh) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nt = blockDim.x * blockDim.y;
+    double v = 0.0;
+    for (int b = tid; b < (int)gridDim.x; b += nt) {
+        const double x = ((volatile const double*)part)[b];
+        v = MAX ? nanmax(v, x) : v + x;
+    }
+    return MAX ? block_max<kBlock>(v, sh) : block_sum<kBlock>(v, sh);
+}
+
+__device__ __forceinline__ bool tid0() { return threadIdx.x == 0 && threadIdx.y == 0; }
+
+static inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace pf

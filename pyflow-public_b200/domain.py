@@ -7,9 +7,10 @@ step after the predictor (:361-367).  Without an SFS model, or with the
 'tensor' models, the whole step is one C-ABI call (pf_forward_step).
 
 Optional configuration keys beyond the reference's:
-  precisionMode  'fp64' (default) or 'mixed' (FP32 fluxes, stages and inner
+  precisionMode  'fp64' (default), 'mixed' (FP32 fluxes, stages and inner
                  Poisson solve; FP64 state, residuals, inner products and
-                 refinement to the same tolerance);
+                 refinement to the same tolerance) or 'mixed_mg' ('mixed' with
+                 the FP32 passes preconditioned by a multigrid V-cycle);
   SFSmodel       also 'MLP' (the 9 -> 128 -> 128 -> 6 BF16 closure in the
                  'tensor' slot, pyflow_b200.sfsmodel_mlp).
 """

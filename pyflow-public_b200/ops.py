@@ -12,7 +12,7 @@ import torch
 
 from . import _lib as L
 
-PREC = {"fp64": L.PF_FP64, "mixed": L.PF_MIXED}
+PREC = {"fp64": L.PF_FP64, "mixed": L.PF_MIXED, "mixed_mg": L.PF_MIXED_MG}
 _ws_cache = {}
 
 

@@ -28,7 +28,7 @@ _lib.pf_step_plan_destroy.argtypes = [ctypes.c_void_p]
 _lib.pf_step_plan_destroy.restype = ctypes.c_int
 
 STAT_NAMES = ("max_u", "max_v", "max_w", "tke", "max_div", "max_res",
-              "iterations", "status")
+              "iterations", "status", "total_iterations", "steps")
 
 
 class StepPlan:
@@ -41,7 +41,7 @@ class StepPlan:
         pr = ops.PREC[prec]
         need = _lib.pf_step_plan_workspace_bytes(ctypes.byref(self.grid), pr)
         self.ws = torch.empty(need, dtype=torch.uint8, device=u.device)
-        self.stats_dev = torch.zeros(8, dtype=torch.float64, device=u.device)
+        self.stats_dev = torch.zeros(10, dtype=torch.float64, device=u.device)
         self.cells = u.numel()
         self._h = ctypes.c_void_p(0)
         # the fields must be ready: wait for the stream that produced them
@@ -56,6 +56,9 @@ class StepPlan:
         s = stream if stream is not None else torch.cuda.current_stream(self.ws.device)
         L.check("pf_step_plan_launch", _lib.pf_step_plan_launch(
             self._h, int(nsteps), ctypes.c_void_p(s.cuda_stream)))
+
+    def reset_counters(self):
+        self.stats_dev[8:].zero_()
 
     def stats(self):
         return dict(zip(STAT_NAMES, self.stats_dev.cpu().tolist()))

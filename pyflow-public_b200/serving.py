@@ -185,6 +185,30 @@ class Server:
         return results
 
 
+def assign_requests(requests, free_bytes, prec="mixed"):
+    """Shard a request stream over GPUs (one rank each): every request goes,
+    in arrival order, to the rank with the least work assigned so far
+    (cell-steps), among the ranks whose free HBM can hold it; ties go to the
+    rank with more free HBM, then the lower rank.  Requests that fit no rank
+    are returned separately.  The assignment is deterministic, so every rank
+    computes the same one without communicating.  Returns (per-rank lists,
+    unplaceable list)."""
+    world = len(free_bytes)
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    rejected = []
+    for req in sorted(requests, key=lambda r: (r.arrival, r.id)):
+        need = footprint_bytes(req.n, prec)
+        cands = [r for r in range(world) if need <= free_bytes[r]]
+        if not cands:
+            rejected.append(req)
+            continue
+        r = min(cands, key=lambda k: (load[k], -free_bytes[k], k))
+        out[r].append(req)
+        load[r] += req.n ** 3 * req.steps
+    return out, rejected
+
+
 def percentile(xs, q):
     xs = sorted(xs)
     if not xs:

@@ -150,11 +150,12 @@ def test_forward_run_fp64_vs_reference(ops, golden):
     assert np.abs(host(p) - g["p"]).max() <= 1e-8 * np.abs(g["p"]).max()
 
 
-def test_forward_run_mixed_vs_reference(ops, golden):
+@pytest.mark.parametrize("prec", ["mixed", "mixed_mg"])
+def test_forward_run_mixed_vs_reference(ops, golden, prec):
     """Mixed precision: FP32 fluxes/stages/matvec, FP64 state, residual and
     refinement to the same 1e-10 tolerance.  Velocity within 1e-6 relative."""
     g = golden("run_32.npz")
-    u, v, w, p, infos = _run(ops, g, "mixed")
+    u, v, w, p, infos = _run(ops, g, prec)
     assert all(i[2] == 0 for i in infos), infos
     assert all(i[1] <= 1e-10 for i in infos)
     for a, key in ((u, "u"), (v, "v"), (w, "w")):

@@ -9,7 +9,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("prec,shape", [("fp64", (32, 32, 32)), ("fp64", (24, 20, 36)),
-                                        ("mixed", (32, 32, 32))])
+                                        ("mixed", (32, 32, 32)), ("mixed_mg", (32, 32, 32)),
+                                        ("mixed_mg", (24, 20, 36))])
 def test_plan_matches_forward_step(prec, shape):
     import pyflow_b200.initial as ic
     import pyflow_b200.ops as ops

@@ -53,7 +53,7 @@ def _write_inputs(wd, g):
                        ["U", "V", "W", "P"], float(g["dt"]), 0.0)
 
 
-@pytest.mark.parametrize("precision,tol", [(None, 1e-9), ("mixed", 1e-6)])
+@pytest.mark.parametrize("precision,tol", [(None, 1e-9), ("mixed", 1e-6), ("mixed_mg", 1e-6)])
 def test_pyflow_run_matches_reference(golden, tmp_path, monkeypatch, precision, tol):
     import pyflow_b200.PyFlow as PyFlow
     import pyflow_b200.dataReader as dr

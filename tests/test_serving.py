@@ -58,3 +58,62 @@ def test_admission_by_free_memory():
     assert srv.max_active == 1
     assert all(by[i].status == "ok" for i in range(4))
     assert by[9].status == "rejected"
+
+
+def test_assign_requests_balances_and_rejects():
+    import pyflow_b200.serving as S
+    reqs = S.stream_requests(64, rate=20.0)
+    big = S.footprint_bytes(192)
+    shards, rej = S.assign_requests(reqs, [10 * big, 10 * big, S.footprint_bytes(64)])
+    ids = sorted(r.id for sh in shards for r in sh)
+    assert ids == sorted(r.id for r in reqs) and not rej
+    # the small rank only ever gets grids that fit it
+    assert all(r.n <= 64 for r in shards[2])
+    work = [sum(r.n ** 3 * r.steps for r in sh) for sh in shards[:2]]
+    assert max(work) <= 1.5 * min(work)
+    _, rej = S.assign_requests(reqs, [S.footprint_bytes(48)])
+    assert {r.n for r in rej} == {64, 96, 128, 192}
+
+
+def _shard_worker(rank, world, port, q):
+    import torch.distributed as dist
+    import pyflow_b200.serving as S
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank,
+                            world_size=world)
+    try:
+        reqs = S.stream_requests(40, rate=10.0)
+        free = [8 * S.footprint_bytes(192)] * world
+        shards, _ = S.assign_requests(reqs, free)
+        mine = [r.id for r in shards[rank]]
+        allv = [None] * world
+        dist.all_gather_object(allv, mine)
+        work = torch.tensor([float(sum(r.n ** 3 * r.steps for r in shards[rank]))],
+                            dtype=torch.float64)
+        dist.all_reduce(work)
+        q.put((rank, allv, float(work.item()),
+               float(sum(r.n ** 3 * r.steps for r in reqs))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_request_sharding_two_ranks_gloo():
+    """Two ranks compute the same assignment independently: their shards are
+    disjoint, cover the stream, and the aggregate work sums to the total."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, allv, work, total in out:
+        a, b = allv
+        assert not set(a) & set(b) and sorted(a + b) == list(range(40))
+        assert work == total
