@@ -18,9 +18,10 @@
  *    iterative-refinement outer loop and all global sums.  PF_MIXED_MG is
  *    PF_MIXED whose FP32 refinement passes run BiCGStab right-preconditioned
  *    by a geometric multigrid V-cycle (no counterpart in the reference, whose
- *    BiCGStab is unpreconditioned); it needs every grid dimension to halve
- *    down to a coarsest level of at most 4096 cells, and otherwise runs the
- *    PF_MIXED passes.  Both mixed forms converge to the same FP64 tolerance.
+ *    BiCGStab is unpreconditioned); it needs the grid to halve in every
+ *    dimension (while all are even) down to at most 4096 cells, and otherwise
+ *    runs the PF_MIXED passes.  Both mixed forms converge to the same FP64
+ *    tolerance.
  */
 #ifndef PYFLOW_B200_H
 #define PYFLOW_B200_H
@@ -70,7 +71,8 @@ size_t pf_workspace_bytes(const pf_grid* g, int prec);
  * (src/data/domain.py:130-131) or a cell-centred viscosity field; sfs: NULL or
  * six consecutive cell-centred fields FXX,FYY,FZZ,FXY,FXZ,FYZ of a 'tensor'
  * SFS model (src/solver/velocity.py:262-267,286-291,310-315).  Fields are
- * double for PF_FP64, float for PF_MIXED (u,v,w,visc,sfs,rhs all float). */
+ * double for PF_FP64, float for the mixed forms (u,v,w,visc,sfs,rhs all
+ * float). */
 int pf_rhs_ns(const pf_grid* g, int prec, const void* u, const void* v,
               const void* w, const void* visc, double mu, double rho,
               const void* sfs, void* ru, void* rv, void* rw, void* stream);

@@ -126,6 +126,8 @@ class ForwardStep(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, u, v, w, sfs, spacing, mu, rho, dt, rk4, tol, max_it):
+        if sfs is not None:
+            sfs = sfs.contiguous()
         ctx.save_for_backward(u, v, w, sfs if sfs is not None else torch.empty(0))
         ctx.cfg = (spacing, mu, rho, dt, rk4, tol, max_it, sfs is not None)
         uo, vo, wo = u.detach().clone(), v.detach().clone(), w.detach().clone()

@@ -8,7 +8,7 @@
 //   s  = res - alpha v                 sh = M s     t = A sh    omega = (t,s)/(t,t)
 //   e += alpha ph + omega sh           res = s - omega t        rho' = (res,res0)
 // M is one V(2,2) cycle of cell-centred geometric multigrid:
-//   * levels halve every dimension while all are even, down to <= 512 cells;
+//   * levels halve every dimension while all are even, down to <= 64 cells;
 //     level l uses the same 7-point operator with spacing 2^l h (the coarse
 //     right-hand side is the SUM of the 8 fine residuals, because A carries
 //     the cell volume);
@@ -17,11 +17,20 @@
 //     evaluated in one pass as x = w (2 b - w A b), w = omega / diag(A);
 //   * restriction: sum of the 8 children's residuals b - A x, computed from x
 //     in the same kernel; prolongation: trilinear (weights 27, 9, 3, 1 / 64);
-//   * coarsest level: mean removed (the periodic operator is singular), then
-//     48 Jacobi sweeps by one CTA in shared memory.
+//   * coarsest level (<= 64 cells when the grid halves that far): solved
+//     exactly with the pseudo-inverse of its periodic operator (from the
+//     Fourier eigenvalues; the operator is singular), else mean removal and
+//     Jacobi sweeps.
 // M is a fixed linear operator (fixed sweep counts), as BiCGStab requires.
 // At the finest level the p update and s = res - alpha v are fused into the
 // first smoothing pass, which computes them for every cell it loads.
+//
+// Execution by level size: large levels (the finest always) use the tiled
+// sweep of pf_sweep.cuh; mid-size levels one thread per cell (a sweep's
+// plane-by-plane march is latency-bound on small grids); on both, the
+// prolongation is fused into the first post-smoothing pass; every level of at
+// most 4096 cells runs inside ONE CTA in shared memory (mg_bottom), so the
+// bottom of the V-cycle is a single launch.
 //
 // All vectors are FP32; every dot product and max accumulates in FP64 and is
 // finished by the last block (fixed order).  Scalars stay on the device.
@@ -35,7 +44,7 @@
 namespace pf {
 
 constexpr float kMgOmega = 6.0f / 7.0f;
-constexpr int kMgCoarseSweeps = 48;
+constexpr int kMgCoarseSweeps = 32;
 
 // ------------------------------------------------------------ sweep phases
 // Sources of the first (from-zero) smoothing pass.
@@ -43,7 +52,7 @@ struct SrcPlain {  // b of a coarse level
     const float* b;
     struct Raw { float b; };
     __device__ void setup(const BicgScalars*) {}
-    __device__ Raw raw(long long q) const { return Raw{b[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{b[q]}; }
     __device__ float op(const Raw& a) const { return a.b; }
     __device__ void store(long long, float) const {}
 };
@@ -57,7 +66,7 @@ struct SrcP {  // p' = res + beta (p - omega v), stored to p_new
         beta = float((sc->rho1 / sc->rho2) * (sc->alpha / sc->omega));
         omega = float(sc->omega);
     }
-    __device__ Raw raw(long long q) const { return Raw{res[q], p_old[q], v[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{res[q], p_old[q], v[q]}; }
     __device__ float op(const Raw& a) const {
         return fmaf(beta, fmaf(-omega, a.v, a.p), a.r);
     }
@@ -70,7 +79,7 @@ struct SrcS {  // s = res - alpha v, stored to s
     float alpha;
     struct Raw { float r, v; };
     __device__ void setup(const BicgScalars* sc) { alpha = float(sc->alpha); }
-    __device__ Raw raw(long long q) const { return Raw{res[q], v[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{res[q], v[q]}; }
     __device__ float op(const Raw& a) const { return fmaf(-alpha, a.v, a.r); }
     __device__ void store(long long q, float c) const { s[q] = c; }
 };
@@ -84,7 +93,7 @@ struct PhaseSmooth0 {
     float wd;
     using Raw = typename Src::Raw;
     struct Ext {};
-    __device__ Raw raw(long long q) const { return src.raw(q); }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return src.raw(q); }
     __device__ Ext ext(long long) const { return Ext{}; }
     __device__ float op(const Raw& a) const { return src.op(a); }
     __device__ void epi(long long q, float c, float ab, const Raw&, const Ext&) {
@@ -101,7 +110,7 @@ struct PhaseSmooth {
     float wd;
     struct Raw { float x; };
     struct Ext { float b; };
-    __device__ Raw raw(long long q) const { return Raw{x[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{x[q]}; }
     __device__ Ext ext(long long q) const { return Ext{b[q]}; }
     __device__ float op(const Raw& a) const { return a.x; }
     __device__ void epi(long long q, float c, float ax, const Raw&, const Ext& e) {
@@ -117,7 +126,7 @@ struct PhaseAv {
     double dot;
     struct Raw { float x; };
     struct Ext { float r0; };
-    __device__ Raw raw(long long q) const { return Raw{ph[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{ph[q]}; }
     __device__ Ext ext(long long q) const { return Ext{res0[q]}; }
     __device__ float op(const Raw& a) const { return a.x; }
     __device__ void epi(long long q, float, float ax, const Raw&, const Ext& e) {
@@ -134,7 +143,7 @@ struct PhaseAt {
     double ts, tt;
     struct Raw { float x; };
     struct Ext { float s; };
-    __device__ Raw raw(long long q) const { return Raw{sh[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{sh[q]}; }
     __device__ Ext ext(long long q) const { return Ext{s[q]}; }
     __device__ float op(const Raw& a) const { return a.x; }
     __device__ void epi(long long q, float, float ax, const Raw&, const Ext& e) {
@@ -211,14 +220,28 @@ mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
     bc[idx(c, I, J, K)] = sum;
 }
 
-// x += P xc (trilinear, cell-centred)
-__global__ void __launch_bounds__(256)
-mg_prolong(Dims f, Dims c, const float* __restrict__ xc, float* __restrict__ x,
-           const BicgScalars* sc) {
-    if (sc->done) return;
-    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= f.nz || j >= f.ny) return;
+// ------------------------------------------------- one thread per cell
+__device__ __forceinline__ float lap7(const float* __restrict__ x, const Dims& d,
+                                      const LapCoef<float>& cf, int i, int j, int k,
+                                      float xc) {
+    const long long P = (long long)d.ny * d.nz;
+    const long long ci = (long long)i * P, cj = (long long)j * d.nz;
+    float ax = 0.0f;
+    ax += __ldg(x + (long long)wrap(i - 1, d.nx) * P + cj + k) * cf.c[0][0];
+    ax += xc * cf.c[0][1];
+    ax += __ldg(x + (long long)wrap(i + 1, d.nx) * P + cj + k) * cf.c[0][2];
+    ax += __ldg(x + ci + (long long)wrap(j - 1, d.ny) * d.nz + k) * cf.c[1][0];
+    ax += xc * cf.c[1][1];
+    ax += __ldg(x + ci + (long long)wrap(j + 1, d.ny) * d.nz + k) * cf.c[1][2];
+    ax += __ldg(x + ci + cj + wrap(k - 1, d.nz)) * cf.c[2][0];
+    ax += xc * cf.c[2][1];
+    ax += __ldg(x + ci + cj + wrap(k + 1, d.nz)) * cf.c[2][2];
+    return ax;
+}
+
+// trilinear prolongation of the coarse level to fine cell (i, j, k)
+__device__ __forceinline__ float prolong_at(const float* __restrict__ xc, const Dims& c,
+                                            int i, int j, int k) {
     const int I = i >> 1, J = j >> 1, K = k >> 1;
     const int I2 = wrap(I + ((i & 1) ? 1 : -1), c.nx);
     const int J2 = wrap(J + ((j & 1) ? 1 : -1), c.ny);
@@ -229,67 +252,324 @@ mg_prolong(Dims f, Dims c, const float* __restrict__ xc, float* __restrict__ x,
     const float v010 = __ldg(xc + a0 + b1 + K), v001 = __ldg(xc + a0 + b0 + K2);
     const float v110 = __ldg(xc + a1 + b1 + K), v101 = __ldg(xc + a1 + b0 + K2);
     const float v011 = __ldg(xc + a0 + b1 + K2), v111 = __ldg(xc + a1 + b1 + K2);
-    const float e = (27.0f * v000 + 9.0f * (v100 + v010 + v001) +
-                     3.0f * (v110 + v101 + v011) + v111) * (1.0f / 64.0f);
-    const long long q = idx(f, i, j, k);
-    x[q] = x[q] + e;
+    return (27.0f * v000 + 9.0f * (v100 + v010 + v001) + 3.0f * (v110 + v101 + v011) + v111) *
+           (1.0f / 64.0f);
 }
 
-// Coarsest level: remove the mean of b, then Jacobi sweeps in shared memory.
-constexpr int kCoarseThreads = 1024;
-__global__ void __launch_bounds__(kCoarseThreads)
-mg_coarse(Dims d, LapCoef<float> cf, float wd, const float* __restrict__ b,
-          float* __restrict__ x, const BicgScalars* sc) {
+#define PF_CELL_IDX(d)                                                       \
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y; \
+    const int i = blockIdx.z;                                                \
+    if (k >= (d).nz || j >= (d).ny) return;                                  \
+    const long long q = idx((d), i, j, k)
+
+// x = w (2 b - w A b)
+__global__ void __launch_bounds__(256)
+mg_smooth0_pw(Dims d, LapCoef<float> cf, float wd, const float* __restrict__ b,
+              float* __restrict__ x, const BicgScalars* sc) {
     if (sc->done) return;
-    extern __shared__ float smem[];
+    PF_CELL_IDX(d);
+    const float bc = b[q];
+    x[q] = wd * (2.0f * bc - wd * lap7(b, d, cf, i, j, k, bc));
+}
+
+// out = x + w (b - A x)
+__global__ void __launch_bounds__(256)
+mg_smooth_pw(Dims d, LapCoef<float> cf, float wd, const float* __restrict__ x,
+             const float* __restrict__ b, float* __restrict__ out, const BicgScalars* sc) {
+    if (sc->done) return;
+    PF_CELL_IDX(d);
+    const float xc = x[q];
+    out[q] = fmaf(wd, b[q] - lap7(x, d, cf, i, j, k, xc), xc);
+}
+
+// y = x + P xc at the cell and its six neighbours; out = y + w (b - A y)
+__global__ void __launch_bounds__(256)
+mg_prolong_smooth_pw(Dims d, Dims c, LapCoef<float> cf, float wd,
+                     const float* __restrict__ xc, const float* __restrict__ x,
+                     const float* __restrict__ b, float* __restrict__ out,
+                     const BicgScalars* sc) {
+    if (sc->done) return;
+    PF_CELL_IDX(d);
+    auto y = [&](int a, int bb, int cc) {
+        return __ldg(x + idx(d, a, bb, cc)) + prolong_at(xc, c, a, bb, cc);
+    };
+    const int im = wrap(i - 1, d.nx), ip = wrap(i + 1, d.nx);
+    const int jm = wrap(j - 1, d.ny), jp = wrap(j + 1, d.ny);
+    const int km = wrap(k - 1, d.nz), kp = wrap(k + 1, d.nz);
+    const float yc = y(i, j, k);
+    float ax = 0.0f;
+    ax += y(im, j, k) * cf.c[0][0];
+    ax += yc * cf.c[0][1];
+    ax += y(ip, j, k) * cf.c[0][2];
+    ax += y(i, jm, k) * cf.c[1][0];
+    ax += yc * cf.c[1][1];
+    ax += y(i, jp, k) * cf.c[1][2];
+    ax += y(i, j, km) * cf.c[2][0];
+    ax += yc * cf.c[2][1];
+    ax += y(i, j, kp) * cf.c[2][2];
+    out[q] = fmaf(wd, b[q] - ax, yc);
+}
+
+// Swept levels: y = x + P xc computed for every cell the sweep loads (the
+// prolongation costs no pass of its own); out = y + w (b - A y)
+struct PhaseProlongSmooth {
+    static constexpr int R = 4;
+    const float *x, *b, *xc;
+    Dims c;
+    float* out;
+    float wd;
+    struct Raw { float y; };
+    struct Ext { float b; };
+    __device__ Raw raw(long long q, int i, int j, int k) const {
+        return Raw{x[q] + prolong_at(xc, c, i, j, k)};
+    }
+    __device__ Ext ext(long long q) const { return Ext{b[q]}; }
+    __device__ float op(const Raw& a) const { return a.y; }
+    __device__ void epi(long long q, float y, float ay, const Raw&, const Ext& e) {
+        out[q] = fmaf(wd, e.b - ay, y);
+    }
+};
+
+__global__ void __launch_bounds__(kBlock, 2)
+mg_prolong_smooth(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc,
+                  PhaseProlongSmooth ph) {
+    if (sc->done) return;
+    sweep<float>(d, tl, cf, ph);
+}
+
+// ------------------------------------------------- bottom of the V-cycle
+// All levels of at most kMgBottomMax cells in one CTA: b, x, t of each level
+// live in shared memory.  Same operations as the global kernels.
+constexpr int kBottomThreads = 1024;
+
+struct MgBottom {
+    int nlev;
+    Dims d[kMgMaxLevels];
+    LapCoef<float> cf[kMgMaxLevels];
+    float wd[kMgMaxLevels];
+    float inv_p[kMgMaxLevels];  // 1 / (ny nz) and 1 / nz, for index decoding
+    float inv_z[kMgMaxLevels];
+    int off[kMgMaxLevels];      // float offset of the level's b; x and t follow
+    const float* pinv;          // coarsest level's pseudo-inverse, or null
+};
+
+constexpr int kMgPinvMax = 64;  // largest coarsest level solved with a pseudo-inverse
+
+// Pseudo-inverse of the periodic coarsest-level operator (singular: constant
+// null space), from its Fourier eigen-decomposition:
+//   A^+[p][r] = (1/N) sum_{k != 0} cos(sum_q 2 pi k_q (p_q - r_q) / n_q) / lambda(k),
+//   lambda(k) = sum_q c_q (2 - 2 cos(2 pi k_q / n_q)),  c_q = vol / h_q^2.
+// Symmetric; applying it also removes the mean of the right-hand side.
+__global__ void __launch_bounds__(256)
+mg_coarse_pinv(Dims d, double cx, double cy, double cz, float* __restrict__ out) {
+    const int N = (int)d.n;
+    const double tp = 6.283185307179586;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N * N; e += gridDim.x * blockDim.x) {
+        const int p = e / N, r = e - p * N;
+        const int pz = p % d.nz, py = (p / d.nz) % d.ny, px = p / (d.ny * d.nz);
+        const int rz = r % d.nz, ry = (r / d.nz) % d.ny, rx = r / (d.ny * d.nz);
+        double acc = 0.0;
+        for (int kx = 0; kx < d.nx; ++kx)
+            for (int ky = 0; ky < d.ny; ++ky)
+                for (int kz = 0; kz < d.nz; ++kz) {
+                    if (kx == 0 && ky == 0 && kz == 0) continue;
+                    const double lam = cx * (2.0 - 2.0 * cos(tp * kx / d.nx)) +
+                                       cy * (2.0 - 2.0 * cos(tp * ky / d.ny)) +
+                                       cz * (2.0 - 2.0 * cos(tp * kz / d.nz));
+                    const double ph = tp * (double(kx * (px - rx)) / d.nx +
+                                            double(ky * (py - ry)) / d.ny +
+                                            double(kz * (pz - rz)) / d.nz);
+                    acc += cos(ph) / lam;
+                }
+        out[e] = float(acc / double(N));
+    }
+}
+
+__device__ __forceinline__ float lap7_s(const float* x, const Dims& d,
+                                        const LapCoef<float>& cf, int i, int j, int k,
+                                        float xc) {
+    const int P = d.ny * d.nz, ci = i * P, cj = j * d.nz;
+    float ax = 0.0f;
+    ax += x[wrap(i - 1, d.nx) * P + cj + k] * cf.c[0][0];
+    ax += xc * cf.c[0][1];
+    ax += x[wrap(i + 1, d.nx) * P + cj + k] * cf.c[0][2];
+    ax += x[ci + wrap(j - 1, d.ny) * d.nz + k] * cf.c[1][0];
+    ax += xc * cf.c[1][1];
+    ax += x[ci + wrap(j + 1, d.ny) * d.nz + k] * cf.c[1][2];
+    ax += x[ci + cj + wrap(k - 1, d.nz)] * cf.c[2][0];
+    ax += xc * cf.c[2][1];
+    ax += x[ci + cj + wrap(k + 1, d.nz)] * cf.c[2][2];
+    return ax;
+}
+
+// q -> (i, j, k) by float reciprocals: exact for q < 2^16 (the quotients are
+// at least 0.5 / 4096 away from an integer, far above the rounding error)
+__device__ __forceinline__ void decode(int q, const Dims& d, float inv_p, float inv_z,
+                                       int& i, int& j, int& k) {
+    const int P = d.ny * d.nz;
+    i = int((float(q) + 0.5f) * inv_p);
+    const int r = q - i * P;
+    j = int((float(r) + 0.5f) * inv_z);
+    k = r - j * d.nz;
+}
+
+__global__ void __launch_bounds__(kBottomThreads)
+mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
+          const BicgScalars* sc) {
+    if (sc->done) return;
+    extern __shared__ float sm[];
     __shared__ double shd[32];
     __shared__ float mean_s;
-    const int n = (int)d.n;
-    float* sb = smem;
-    float* s0 = smem + n;
-    float* s1 = s0 + n;
-    const int tid = threadIdx.x;
-    double acc = 0.0;
-    for (int q = tid; q < n; q += blockDim.x) {
-        const float v = b[q];
-        sb[q] = v;
-        acc += double(v);
-    }
-    const double tot = block_sum<kCoarseThreads>(acc, shd);
-    if (tid == 0) mean_s = float(tot / double(n));
-    __syncthreads();
-    const float mean = mean_s;
-    for (int q = tid; q < n; q += blockDim.x) {
-        const float v = sb[q] - mean;
-        sb[q] = v;
-        s0[q] = wd * v;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    {
+        const int n = (int)P.d[0].n;
+        float* b = sm + P.off[0];
+        for (int q = tid; q < n; q += nt) b[q] = gb[q];
     }
     __syncthreads();
-    const int nyz = d.ny * d.nz;
-    for (int it = 1; it < kMgCoarseSweeps; ++it) {
-        for (int q = tid; q < n; q += blockDim.x) {
-            const int i = q / nyz, r = q - i * nyz, j = r / d.nz, k = r - j * d.nz;
-            const int im = wrap(i - 1, d.nx) * nyz, ip = wrap(i + 1, d.nx) * nyz;
-            const int jm = wrap(j - 1, d.ny) * d.nz, jp = wrap(j + 1, d.ny) * d.nz;
-            const int km = wrap(k - 1, d.nz), kp = wrap(k + 1, d.nz);
-            const int ic = i * nyz, jc = j * d.nz;
-            const float xc = s0[q];
-            float ax = 0.0f;
-            ax += s0[im + jc + k] * cf.c[0][0];
-            ax += xc * cf.c[0][1];
-            ax += s0[ip + jc + k] * cf.c[0][2];
-            ax += s0[ic + jm + k] * cf.c[1][0];
-            ax += xc * cf.c[1][1];
-            ax += s0[ic + jp + k] * cf.c[1][2];
-            ax += s0[ic + jc + km] * cf.c[2][0];
-            ax += xc * cf.c[2][1];
-            ax += s0[ic + jc + kp] * cf.c[2][2];
-            s1[q] = fmaf(wd, sb[q] - ax, xc);
+    const int last = P.nlev - 1;
+    // down: pre-smooth from zero, restrict
+    for (int l = 0; l < last; ++l) {
+        const Dims d = P.d[l], c = P.d[l + 1];
+        const int n = (int)d.n;
+        float* b = sm + P.off[l];
+        float* x = b + n;
+        const float wd = P.wd[l];
+        for (int q = tid; q < n; q += nt) {
+            int i, j, k;
+            decode(q, d, P.inv_p[l], P.inv_z[l], i, j, k);
+            x[q] = wd * (2.0f * b[q] - wd * lap7_s(b, d, P.cf[l], i, j, k, b[q]));
         }
         __syncthreads();
-        float* tmp = s0; s0 = s1; s1 = tmp;
+        float* bc = sm + P.off[l + 1];
+        for (int Q = tid; Q < (int)c.n; Q += nt) {
+            int I, J, K;
+            decode(Q, c, P.inv_p[l + 1], P.inv_z[l + 1], I, J, K);
+            float sum = 0.0f;
+            for (int a = 0; a < 2; ++a)
+                for (int bb = 0; bb < 2; ++bb)
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const int i = 2 * I + a, j = 2 * J + bb, k = 2 * K + cc;
+                        const int qq = (i * d.ny + j) * d.nz + k;
+                        sum += b[qq] - lap7_s(x, d, P.cf[l], i, j, k, x[qq]);
+                    }
+            bc[Q] = sum;
+        }
+        __syncthreads();
     }
-    for (int q = tid; q < n; q += blockDim.x) x[q] = s0[q];
+    // coarsest: x = A^+ b, or mean removal then Jacobi sweeps (x <-> t)
+    if (P.pinv) {
+        const int n = (int)P.d[last].n;
+        const float* b = sm + P.off[last];
+        float* x = sm + P.off[last] + n;
+        for (int p = tid; p < n; p += nt) {
+            float acc = 0.0f;
+            for (int r = 0; r < n; ++r) acc = fmaf(__ldg(P.pinv + (long long)r * n + p), b[r], acc);
+            x[p] = acc;
+        }
+        __syncthreads();
+    } else {
+        const Dims d = P.d[last];
+        const int n = (int)d.n;
+        float* b = sm + P.off[last];
+        float* x = b + n;
+        float* t = x + n;
+        const float wd = P.wd[last];
+        double acc = 0.0;
+        for (int q = tid; q < n; q += nt) acc += double(b[q]);
+        const double tot = block_sum<kBottomThreads>(acc, shd);
+        if (tid == 0) mean_s = float(tot / double(n));
+        __syncthreads();
+        const float mean = mean_s;
+        for (int q = tid; q < n; q += nt) {
+            const float v = b[q] - mean;
+            b[q] = v;
+            x[q] = wd * v;
+        }
+        __syncthreads();
+        for (int it = 1; it < kMgCoarseSweeps; ++it) {
+            for (int q = tid; q < n; q += nt) {
+                int i, j, k;
+                decode(q, d, P.inv_p[last], P.inv_z[last], i, j, k);
+                const float xc = x[q];
+                t[q] = fmaf(wd, b[q] - lap7_s(x, d, P.cf[last], i, j, k, xc), xc);
+            }
+            __syncthreads();
+            float* tmp = x; x = t; t = tmp;
+        }
+        // the result must sit in the level's x slot
+        if (x != b + n) {
+            for (int q = tid; q < n; q += nt) b[n + q] = x[q];
+            __syncthreads();
+        }
+    }
+    // up: prolong, two post-smoothing sweeps
+    for (int l = last - 1; l >= 0; --l) {
+        const Dims d = P.d[l], c = P.d[l + 1];
+        const int n = (int)d.n;
+        float* b = sm + P.off[l];
+        float* x = b + n;
+        float* t = x + n;
+        const float* xc = sm + P.off[l + 1] + c.n;
+        const float wd = P.wd[l];
+        for (int q = tid; q < n; q += nt) {
+            int i, j, k;
+            decode(q, d, P.inv_p[l], P.inv_z[l], i, j, k);
+            const int I = i >> 1, J = j >> 1, K = k >> 1;
+            const int I2 = wrap(I + ((i & 1) ? 1 : -1), c.nx);
+            const int J2 = wrap(J + ((j & 1) ? 1 : -1), c.ny);
+            const int K2 = wrap(K + ((k & 1) ? 1 : -1), c.nz);
+            auto C = [&](int a, int bb, int cc) { return xc[(a * c.ny + bb) * c.nz + cc]; };
+            const float e = (27.0f * C(I, J, K) + 9.0f * (C(I2, J, K) + C(I, J2, K) + C(I, J, K2)) +
+                             3.0f * (C(I2, J2, K) + C(I2, J, K2) + C(I, J2, K2)) + C(I2, J2, K2)) *
+                            (1.0f / 64.0f);
+            x[q] = x[q] + e;
+        }
+        __syncthreads();
+        for (int q = tid; q < n; q += nt) {
+            int i, j, k;
+            decode(q, d, P.inv_p[l], P.inv_z[l], i, j, k);
+            const float v = x[q];
+            t[q] = fmaf(wd, b[q] - lap7_s(x, d, P.cf[l], i, j, k, v), v);
+        }
+        __syncthreads();
+        for (int q = tid; q < n; q += nt) {
+            int i, j, k;
+            decode(q, d, P.inv_p[l], P.inv_z[l], i, j, k);
+            const float v = t[q];
+            x[q] = fmaf(wd, b[q] - lap7_s(t, d, P.cf[l], i, j, k, v), v);
+        }
+        __syncthreads();
+    }
+    {
+        const int n = (int)P.d[0].n;
+        const float* x = sm + P.off[0] + n;
+        for (int q = tid; q < n; q += nt) gx[q] = x[q];
+    }
+}
+
+static size_t bottom_smem_floats(const MgPlan& P) {
+    size_t f = 0;
+    for (int l = P.B; l < P.L; ++l) f += 3 * (size_t)P.lv[l].d.n;
+    return f;
+}
+
+static MgBottom bottom_params(const MgPlan& P) {
+    MgBottom m{};
+    m.nlev = P.L - P.B;
+    int off = 0;
+    for (int l = P.B; l < P.L; ++l) {
+        const int r = l - P.B;
+        m.d[r] = P.lv[l].d;
+        m.cf[r] = P.lv[l].cf;
+        m.wd[r] = P.lv[l].wd;
+        m.inv_p[r] = 1.0f / float(P.lv[l].d.ny * P.lv[l].d.nz);
+        m.inv_z[r] = 1.0f / float(P.lv[l].d.nz);
+        m.off[r] = off;
+        off += 3 * (int)P.lv[l].d.n;
+    }
+    m.pinv = P.pinv;
+    return m;
 }
 
 // v = A ph, gamma = (v, res0), alpha = rho / gamma
@@ -426,7 +706,7 @@ mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
 }
 
 // ------------------------------------------------------------------- host
-int mg_levels(const pf_grid* g, MgLevel* lv) {
+int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom) {
     pf_grid cur = *g;
     int L = 0;
     for (;;) {
@@ -436,8 +716,11 @@ int mg_levels(const pf_grid* g, MgLevel* lv) {
         const LapCoef<double> c64 = lap_coef<double>(&cur);
         const double diag = c64.c[0][1] + c64.c[1][1] + c64.c[2][1];
         l.wd = float(double(kMgOmega) / diag);
+        for (int q = 0; q < 3; ++q) l.cq[q] = -c64.c[q][2];
         l.b = l.x = l.t = nullptr;
         l.tl = make_tiling(l.d, 32);
+        l.kind = (L == 0 || l.d.n >= kMgSweepMin) ? kMgSwept
+                 : (l.d.n > kMgBottomMax ? kMgPointwise : kMgBottom);
         ++L;
         if (l.d.n <= kMgCoarseTarget || L == kMgMaxLevels) break;
         if ((cur.nx | cur.ny | cur.nz) & 1) break;
@@ -445,7 +728,10 @@ int mg_levels(const pf_grid* g, MgLevel* lv) {
         cur.nx /= 2; cur.ny /= 2; cur.nz /= 2;
         cur.dx *= 2.0; cur.dy *= 2.0; cur.dz *= 2.0;
     }
-    if (L < 2 || lv[L - 1].d.n > kMgCoarseMax) return 0;
+    int B = 0;
+    while (B < L && lv[B].kind != kMgBottom) ++B;
+    if (L < 2 || B == 0 || B == L) return 0;
+    *bottom = B;
     return L;
 }
 
@@ -453,23 +739,28 @@ static constexpr int kMgFineVecs = 11;  // res res0 p0 p1 v s t ph sh e tmp
 
 size_t mg_region_bytes(const pf_grid* g) {
     MgLevel lv[kMgMaxLevels];
-    const int L = mg_levels(g, lv);
+    int B = 0;
+    const int L = mg_levels(g, lv, &B);
     if (!L) return 0;
     size_t b = kMgFineVecs * align256(lv[0].d.n * sizeof(float));
     for (int l = 1; l < L; ++l) b += 3 * align256(lv[l].d.n * sizeof(float));
+    const long long nc = lv[L - 1].d.n;
+    if (nc <= kMgPinvMax) b += align256((size_t)(nc * nc) * sizeof(float));
     return b;
 }
 
 int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
-    P->L = mg_levels(g, P->lv);
+    P->L = mg_levels(g, P->lv, &P->B);
     if (!P->L) return PF_ERR_BAD_ARG;
     static int dev_done[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !dev_done[dev]) {
-        // the coarsest level may need up to 48 KiB of dynamic shared memory
-        if (cudaFuncSetAttribute(mg_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(3 * kMgCoarseMax * sizeof(float))) != cudaSuccess)
+        // the bottom levels (at most 4096 + 512 + 64 + ... cells, 3 arrays
+        // each) need more than the default 48 KiB of shared memory
+        const int bytes = int(3 * sizeof(float) * (kMgBottomMax + kMgBottomMax / 7 + 64));
+        if (cudaFuncSetAttribute(mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes) != cudaSuccess)
             return PF_ERR_CUDA;
         dev_done[dev] = 1;
     }
@@ -484,50 +775,73 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
         P->lv[l].x = (float*)ptr; ptr += lb;
         P->lv[l].t = (float*)ptr; ptr += lb;
     }
+    const long long nc = P->lv[P->L - 1].d.n;
+    P->pinv = nc <= kMgPinvMax ? (float*)ptr : nullptr;
     return PF_OK;
 }
 
 static dim3 cgrid3(const Dims& d) { return dim3((d.nz + 31) / 32, (d.ny + 7) / 8, d.nx); }
 
-// Restriction from level 0 (whose x and b are set), the coarse levels, and
-// the up-sweep back to level 0's x.
+// Restriction from level 0 (whose x and b are set), the levels down to the
+// bottom kernel, and the up-sweep back to level 0's x.
 static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars* sc,
                         cudaStream_t s) {
     const dim3 blk(32, 8);
-    const int L = P.L;
-    for (int l = 0; l + 1 < L; ++l) {
+    for (int l = 0; l < P.B; ++l) {
         const MgLevel& f = P.lv[l];
         const MgLevel& c = P.lv[l + 1];
         const float* bl = l == 0 ? b0 : f.b;
         float* xl = l == 0 ? x0 : f.x;
         if (l > 0) {
-            PhaseSmooth0<SrcPlain> ph{};
-            ph.src.b = f.b; ph.x = f.x; ph.wd = f.wd;
-            PF_LAUNCH("mg_smooth0", s, mg_smooth0<SrcPlain><<<tiled_grid(f.tl), blk, 0, s>>>(
-                f.d, f.tl, f.cf, sc, ph));
+            if (f.kind == kMgSwept) {
+                PhaseSmooth0<SrcPlain> ph{};
+                ph.src.b = f.b; ph.x = f.x; ph.wd = f.wd;
+                PF_LAUNCH("mg_smooth0", s, mg_smooth0<SrcPlain><<<tiled_grid(f.tl), blk, 0, s>>>(
+                    f.d, f.tl, f.cf, sc, ph));
+            } else {
+                PF_LAUNCH("mg_smooth0_pw", s, mg_smooth0_pw<<<cgrid3(f.d), blk, 0, s>>>(
+                    f.d, f.cf, f.wd, f.b, f.x, sc));
+            }
         }
         PF_LAUNCH(l == 0 ? "mg_restrict_l0" : "mg_restrict", s, mg_restrict<<<cgrid3(c.d), blk, 0, s>>>(
             f.d, f.cf, bl, xl, c.d, c.b, sc));
     }
     {
-        const MgLevel& c = P.lv[L - 1];
-        const size_t smem = 3 * (size_t)c.d.n * sizeof(float);
-        PF_LAUNCH("mg_coarse", s, mg_coarse<<<1, kCoarseThreads, smem, s>>>(
-            c.d, c.cf, c.wd, c.b, c.x, sc));
+        const MgBottom m = bottom_params(P);
+        const size_t smem = bottom_smem_floats(P) * sizeof(float);
+        PF_LAUNCH("mg_bottom", s, mg_bottom<<<1, kBottomThreads, smem, s>>>(
+            m, P.lv[P.B].b, P.lv[P.B].x, sc));
     }
-    for (int l = L - 2; l >= 0; --l) {
+    for (int l = P.B - 1; l >= 0; --l) {
         const MgLevel& f = P.lv[l];
         const MgLevel& c = P.lv[l + 1];
         const float* bl = l == 0 ? b0 : f.b;
         float* xl = l == 0 ? x0 : f.x;
-        const char* np = l == 0 ? "mg_prolong_l0" : "mg_prolong";
-        const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
-        PF_LAUNCH(np, s, mg_prolong<<<cgrid3(f.d), blk, 0, s>>>(f.d, c.d, c.x, xl, sc));
-        PhaseSmooth a{xl, bl, f.t, f.wd};
-        PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, a));
-        PhaseSmooth b{f.t, bl, xl, f.wd};
-        PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, b));
+        if (f.kind == kMgSwept) {
+            const char* np = l == 0 ? "mg_psmooth_l0" : "mg_psmooth";
+            const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
+            PhaseProlongSmooth a{xl, bl, c.x, c.d, f.t, f.wd};
+            PF_LAUNCH(np, s, mg_prolong_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(
+                f.d, f.tl, f.cf, sc, a));
+            PhaseSmooth b{f.t, bl, xl, f.wd};
+            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, b));
+        } else {
+            PF_LAUNCH("mg_prolong_smooth_pw", s, mg_prolong_smooth_pw<<<cgrid3(f.d), blk, 0, s>>>(
+                f.d, c.d, f.cf, f.wd, c.x, xl, bl, f.t, sc));
+            PF_LAUNCH("mg_smooth_pw", s, mg_smooth_pw<<<cgrid3(f.d), blk, 0, s>>>(
+                f.d, f.cf, f.wd, f.t, bl, xl, sc));
+        }
     }
+}
+
+int mg_enqueue_setup(const MgPlan& P, cudaStream_t s) {
+    if (P.pinv) {
+        const MgLevel& c = P.lv[P.L - 1];
+        const int ne = (int)(c.d.n * c.d.n);
+        PF_LAUNCH("mg_coarse_pinv", s, mg_coarse_pinv<<<(ne + 255) / 256, 256, 0, s>>>(
+            c.d, c.cq[0], c.cq[1], c.cq[2], P.pinv));
+    }
+    return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;
 }
 
 int mg_enqueue_init(const MgPlan& P, BicgScalars* sc, double* part, const double* rhs,

@@ -6,8 +6,14 @@
 namespace pf {
 
 constexpr int kMgMaxLevels = 16;
-constexpr long long kMgCoarseTarget = 512;  // stop coarsening at or below this
-constexpr long long kMgCoarseMax = 4096;    // largest coarsest level (one CTA)
+constexpr long long kMgCoarseTarget = 64;     // coarsen down to at most this many cells
+constexpr long long kMgBottomMax = 4096;      // levels this small run inside one CTA
+constexpr long long kMgSweepMin = 1LL << 20;  // levels this large use the tiled sweep
+
+// How a level's kernels run: the tiled sweep (the finest level always, and
+// every level of at least kMgSweepMin cells), one thread per cell, or inside
+// the single-CTA bottom kernel (every level of at most kMgBottomMax cells).
+enum MgKind { kMgSwept = 0, kMgPointwise = 1, kMgBottom = 2 };
 
 struct MgLevel {
     Dims d;
@@ -15,19 +21,24 @@ struct MgLevel {
     float wd;           // omega / diag(A)
     float *b, *x, *t;   // right-hand side, iterate, smoothing buffer
     Tiling tl;
+    int kind;
+    double cq[3];       // vol / h_q^2: the operator's off-diagonal magnitudes
 };
 
 struct MgPlan {
     int L = 0;  // number of levels; 0 = multigrid does not apply to the grid
+    int B = 0;  // first level handled by the bottom kernel
     MgLevel lv[kMgMaxLevels];
     // Krylov vectors (FP32, finest grid); p is double-buffered
     float *res, *res0, *p[2], *v, *s, *t, *ph, *sh, *e;
+    float* pinv = nullptr;  // coarsest-level pseudo-inverse (small coarsest levels)
 };
 
 // Level hierarchy of grid g (no memory touched).  Returns the number of
-// levels, 0 when the grid cannot be coarsened to a coarsest level of at most
-// kMgCoarseMax cells.
-int mg_levels(const pf_grid* g, MgLevel* lv);
+// levels and sets *bottom; 0 when the finest level is itself at most
+// kMgBottomMax cells or the grid stops coarsening (an odd dimension) above
+// that size.
+int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom);
 // FP32 bytes of the Krylov vectors and the coarse levels (0 if L == 0).
 size_t mg_region_bytes(const pf_grid* g);
 // Carve the vectors from `region` (mg_region_bytes long, 256-byte aligned).
@@ -37,6 +48,9 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P);
 int mg_inner_solve(const MgPlan& P, BicgScalars* sc, double* part,
                    const double* rhs, double tol, int max_it, cudaStream_t s,
                    BicgScalars* hs);
+// Per-solve set-up kernels (the coarsest level's pseudo-inverse); enqueue
+// once before the first inner solve that uses the vectors of `region`.
+int mg_enqueue_setup(const MgPlan& P, cudaStream_t s);
 // Kernels of the inner solve, for graph capture: initialisation and one
 // iteration with parity k & 1 (kernels of a finished solve return at once).
 int mg_enqueue_init(const MgPlan& P, BicgScalars* sc, double* part,

@@ -6,8 +6,9 @@
 // accumulation; its six outputs times out_scale are the stresses FXX, FYY, FZZ,
 // FXY, FXZ, FYZ of the 'tensor' SFS slot (src/solver/velocity.py:262-267,...).
 //
-// One CTA of 128 threads (4 warps) walks tiles of 128 consecutive cells; cell
-// m of a tile is accumulator row / TMEM lane m and belongs to thread m:
+// CTAs of 128 threads (4 warps, two per SM) walk tiles of 128 consecutive
+// cells; cell m of a tile is accumulator row / TMEM lane m and belongs to
+// thread m:
 //   1. each thread computes its cell's gradients and writes 16 BF16 features
 //      (9 + 7 zero pads) into the X tile in shared memory;
 //   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
@@ -209,7 +210,7 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bia
 }  // namespace mlp
 
 // scales[0] = 1/g_rms (input normalisation), scales[1] = output scale
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
 mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restrict__ v,
                    const double* __restrict__ w, double dxi, double dyi, double dzi,
                    const uint8_t* __restrict__ wpack, const float* __restrict__ scales,
@@ -355,19 +356,29 @@ cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
                        double* out, int* err, cudaStream_t s) {
     Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     const size_t smem = mlp_smem_bytes();
-    static bool attr = false;
-    if (!attr) {
+    static bool attr[64] = {false};  // per device
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur < 0 || cur >= 64 || !attr[cur]) {
         cudaError_t e = cudaFuncSetAttribute(mlp_closure_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        attr = true;
+        // the largest shared-memory carveout, so two CTAs fit on an SM
+        e = cudaFuncSetAttribute(mlp_closure_kernel,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        if (cur >= 0 && cur < 64) attr[cur] = true;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long ntiles = (d.n + mlp::kTile - 1) / mlp::kTile;
-    // one CTA per SM: each holds 256 TMEM columns and ~75 KB of shared memory
-    const int grid = (int)std::min<long long>(ntiles, (long long)sms);
+    // two CTAs per SM, so one's tensor-core layer overlaps the other's
+    // epilogue: each holds 256 of the SM's 512 TMEM columns and ~79 KB of
+    // shared memory (a third would not fit in shared memory, so a TMEM
+    // allocation never has to wait for another CTA of this kernel)
+    const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
     PF_LAUNCH("mlp_closure", s, mlp_closure_kernel<<<grid, 128, smem, s>>>(
         d, u, v, w, 1.0 / g->dx, 1.0 / g->dy, 1.0 / g->dz, (const uint8_t*)wpack, scales,
         out, err));

@@ -106,7 +106,7 @@ struct PhaseCA {
     double gam, mx;
     struct Raw { T r, p, v, t; };
     struct Ext { T x, r0; };
-    __device__ Raw raw(long long q) const { return Raw{res_o[q], pp_o[q], vv_o[q], t[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{res_o[q], pp_o[q], vv_o[q], t[q]}; }
     __device__ Ext ext(long long q) const { return Ext{fin ? x[q] : T(0), res0[q]}; }
     __device__ T resid(const Raw& a) const {
         if (!fin) return a.r;
@@ -221,7 +221,7 @@ struct PhaseB {
     double st, tt, sr, tr;
     struct Raw { T r, v; };
     struct Ext { T r0; };
-    __device__ Raw raw(long long q) const { return Raw{res[q], vv[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{res[q], vv[q]}; }
     __device__ Ext ext(long long q) const { return Ext{res0[q]}; }
     __device__ T op(const Raw& a) const { return fma(-alpha, a.v, a.r); }
     __device__ void epi(long long q, T c, T b, const Raw&, const Ext& e) {
@@ -329,7 +329,7 @@ struct PhaseResidual {
     double mx;
     struct Raw { double x; };
     struct Ext { double b; };
-    __device__ Raw raw(long long q) const { return Raw{x[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{x[q]}; }
     __device__ Ext ext(long long q) const { return Ext{b[q]}; }
     __device__ double op(const Raw& a) const { return a.x; }
     __device__ void epi(long long q, double, double ax, const Raw&, const Ext& e) {
@@ -482,6 +482,7 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
         if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
             const int rc = mg_setup(g, region, &mg);
             if (rc != PF_OK && rc != PF_ERR_BAD_ARG) return rc;
+            if (mg.L && mg_enqueue_setup(mg, s) != PF_OK) return PF_ERR_CUDA;
         }
         PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b, DP, nullptr));
         if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
@@ -592,7 +593,7 @@ struct PhaseJacobiRes {
     double dx2, mx;
     struct Raw { double p; };
     struct Ext { double s; };
-    __device__ Raw raw(long long q) const { return Raw{p[q]}; }
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{p[q]}; }
     __device__ Ext ext(long long q) const { return Ext{sdx[q]}; }
     __device__ double op(const Raw& a) const { return a.p; }
     __device__ void epi(long long, double, double ax, const Raw&, const Ext& e) {
@@ -920,6 +921,13 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
     float* e32 = (float*)vp;
     double* bb = (double*)(R + 9 * align256(n * sizeof(double)));
     double* rr = (double*)(R + 10 * align256(n * sizeof(double)));
+    // PF_MIXED_MG: multigrid-preconditioned inner passes when the grid
+    // coarsens (vectors in the region of the FP32 solver vectors)
+    MgPlan mg;
+    if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
+        const int e = mg_setup(g, R, &mg);
+        if (e != PF_OK && e != PF_ERR_BAD_ARG) return e;
+    }
     cudaStream_t cs;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return PF_ERR_CUDA;
     prof_suspend(true);
@@ -941,6 +949,8 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
             bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v64, DP);
         } else {
             mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, div, c1, c2, bb, DP, rr);
+            // after the predictor, whose stage buffers share the region
+            if (mg.L) mg_enqueue_setup(mg, cs);
         }
         if ((rc = capture_end(cs, &seg1))) break;
         cudaGraphNode_t n1, nw;
@@ -964,13 +974,6 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
             const Tiling tb = make_tiling(d, 8 * PhaseB<float>::R);
             const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
             const double kInnerTol = 1e-4;
-            // PF_MIXED_MG: multigrid-preconditioned inner passes when the grid
-            // coarsens (vectors in the same region)
-            MgPlan mg;
-            if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
-                const int e = mg_setup(g, R, &mg);
-                if (e != PF_OK && e != PF_ERR_BAD_ARG) { rc = e; break; }
-            }
             float* ecorr = mg.L ? mg.e : e32;
             // outer body: inner set-up, inner WHILE, fold + residual + control
             cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;

@@ -39,15 +39,29 @@ __device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i,
                                 int j, int k, T& ru_o, T& rv_o, T& rw_o) {
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const T dxi = a.dxi, dyi = a.dyi, dzi = a.dzi, rho = a.rho;
+    // wrapped plane / row / column offsets of the neighbours i-2 .. i+1
+    // (computed once; every load is then two adds)
+    const long long P = (long long)ny * nz;
+    long long xo[4];
+    int yo[4], zo[4];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) {
+        xo[o] = (long long)wrap(i + o - 2, nx) * P;
+        yo[o] = wrap(j + o - 2, ny) * nz;
+        zo[o] = wrap(k + o - 2, nz);
+    }
+    auto off = [&](int di, int dj, int dk) -> long long {
+        return xo[di + 2] + (long long)(yo[dj + 2] + zo[dk + 2]);
+    };
     auto L = [&](const TI* f, int di, int dj, int dk) -> T {
-        return T(__ldg(f + idx(d, wrap(i + di, nx), wrap(j + dj, ny), wrap(k + dk, nz))));
+        return T(__ldg(f + off(di, dj, dk)));
     };
     auto LV = [&](int di, int dj, int dk) -> T {
-        return a.visc ? __ldg(a.visc + idx(d, wrap(i + di, nx), wrap(j + dj, ny), wrap(k + dk, nz))) : a.mu;
+        return a.visc ? __ldg(a.visc + off(di, dj, dk)) : a.mu;
     };
     const long long n = d.n;
     auto LS = [&](int c, int di, int dj, int dk) -> T {
-        return __ldg(a.sfs + (long long)c * n + idx(d, wrap(i + di, nx), wrap(j + dj, ny), wrap(k + dk, nz)));
+        return __ldg(a.sfs + (long long)c * n + off(di, dj, dk));
     };
     // velocity neighbourhood
     const T u_c = L(a.u, 0, 0, 0), u_xp = L(a.u, 1, 0, 0), u_xm = L(a.u, -1, 0, 0);

@@ -71,8 +71,12 @@ static inline Tiling make_tiling(const Dims& d, int ty) {
     t.ntz = (d.nz + 31) / 32;
     t.nty = (d.ny + ty - 1) / ty;
     const long long yz = (long long)t.ntz * t.nty;
-    const long long want = (long long)num_sms() * 3;  // tiles to fill the GPU
-    long long xc = (yz * d.nx) / want;
+    // split x so the tiles fill the resident blocks (2 per SM) in whole
+    // waves: one tile per block when the grid is small, 64-plane tiles when
+    // it is large
+    const long long slots = (long long)num_sms() * 2;
+    const long long chunks = std::max<long long>(1, slots / yz);
+    long long xc = (d.nx + chunks - 1) / chunks;
     xc = std::max<long long>(4, std::min<long long>(64, xc));
     t.xc = (int)std::min<long long>(xc, d.nx);
     t.ntx = (d.nx + t.xc - 1) / t.xc;
@@ -92,7 +96,7 @@ static inline int pointwise_grid(long long n) {
 // --------------------------------------------------------------------------
 // Tiled 7-point sweep with one-plane-ahead prefetch.  The phase object Ph
 // provides
-//   Raw raw(q)  -- loads the operand inputs of cell q,
+//   Raw raw(q, i, j, k) -- loads the operand inputs of cell q = (i, j, k),
 //   T   op(raw) -- the stencil operand,
 //   Ext ext(q)  -- loads the epilogue inputs of an owned cell,
 //   epi(q, centre operand, A operand, raw, ext) -- consumes an owned cell.
@@ -116,54 +120,60 @@ __device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
         const int ez = min(32, d.nz - k0), ey = min(TY, d.ny - j0);
         bool vr[R];
         long long off[R];
+        const int kk = k0 + tx;  // z index of this thread's cells
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int jl = ty + 8 * r;
             vr[r] = (tx < ez) && (jl < ey);
-            off[r] = (long long)(j0 + jl) * d.nz + (k0 + tx);
+            off[r] = (long long)(j0 + jl) * d.nz + kk;
         }
         // this thread's halo cell of each plane (at most 2*32 + 2*TY cells)
         bool hv = false;
-        int hy = 0, hz = 0;
-        long long hoff = 0;
+        int hy = 0, hz = 0, hj = 0, hk = 0;
         if (tid < 64) {
             const int h = tid & 31;
             hv = h < ez;
             hz = h + 1;
-            if (tid < 32) { hy = 0; hoff = (long long)wrap(j0 - 1, d.ny) * d.nz + k0 + h; }
-            else { hy = ey + 1; hoff = (long long)wrap(j0 + ey, d.ny) * d.nz + k0 + h; }
+            hk = k0 + h;
+            if (tid < 32) { hy = 0; hj = wrap(j0 - 1, d.ny); }
+            else { hy = ey + 1; hj = wrap(j0 + ey, d.ny); }
         } else if (tid < 64 + 2 * TY) {
             const int u = tid - 64, h = u % TY;
             hv = h < ey;
             hy = h + 1;
-            if (u < TY) { hz = 0; hoff = (long long)(j0 + h) * d.nz + wrap(k0 - 1, d.nz); }
-            else { hz = ez + 1; hoff = (long long)(j0 + h) * d.nz + wrap(k0 + ez, d.nz); }
+            hj = j0 + h;
+            if (u < TY) { hz = 0; hk = wrap(k0 - 1, d.nz); }
+            else { hz = ez + 1; hk = wrap(k0 + ez, d.nz); }
         }
+        const long long hoff = (long long)hj * d.nz + hk;
         T opP[R], opC[R], opN[R];
         Raw rawC[R], rawN[R];
         Ext extC[R];
         Raw hraw{};
         {
-            const long long bm = (long long)wrap(i0 - 1, d.nx) * plane;
+            const int im = wrap(i0 - 1, d.nx), ip = wrap(i0 + 1, d.nx);
+            const long long bm = (long long)im * plane;
             const long long b0 = (long long)i0 * plane;
-            const long long b1 = (long long)wrap(i0 + 1, d.nx) * plane;
+            const long long b1 = (long long)ip * plane;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (vr[r]) {
-                    opP[r] = ph.op(ph.raw(bm + off[r]));
-                    rawC[r] = ph.raw(b0 + off[r]);
-                    rawN[r] = ph.raw(b1 + off[r]);
+                    const int jj = j0 + ty + 8 * r;
+                    opP[r] = ph.op(ph.raw(bm + off[r], im, jj, kk));
+                    rawC[r] = ph.raw(b0 + off[r], i0, jj, kk);
+                    rawN[r] = ph.raw(b1 + off[r], ip, jj, kk);
                     extC[r] = ph.ext(b0 + off[r]);
                     opC[r] = ph.op(rawC[r]);
                 }
             }
-            if (hv) hraw = ph.raw(b0 + hoff);
+            if (hv) hraw = ph.raw(b0 + hoff, i0, hj, hk);
         }
         for (int i = i0; i < i1; ++i) {
             const bool more = i + 1 < i1;
+            const int ih = wrap(i + 1, d.nx), in2 = wrap(i + 2, d.nx);
             const long long bi = (long long)i * plane;
-            const long long bh = (long long)wrap(i + 1, d.nx) * plane;
-            const long long bn = (long long)wrap(i + 2, d.nx) * plane;
+            const long long bh = (long long)ih * plane;
+            const long long bn = (long long)in2 * plane;
             Raw rawNN[R];
             Ext extN[R];
             Raw hrawN{};
@@ -171,11 +181,11 @@ __device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (vr[r]) {
-                        rawNN[r] = ph.raw(bn + off[r]);
+                        rawNN[r] = ph.raw(bn + off[r], in2, j0 + ty + 8 * r, kk);
                         extN[r] = ph.ext(bh + off[r]);
                     }
                 }
-                if (hv) hrawN = ph.raw(bh + hoff);
+                if (hv) hrawN = ph.raw(bh + hoff, ih, hj, hk);
             }
 #pragma unroll
             for (int r = 0; r < R; ++r)

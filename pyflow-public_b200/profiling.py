@@ -62,12 +62,12 @@ def bytes_per_cell(name):
         # multigrid-preconditioned FP32 BiCGStab (finest-level launches only;
         # coarse levels have their own names and fewer cells)
         "mg_smooth0_p": 20, "mg_smooth0_s": 16, "mg_smooth_l0": 12,
-        "mg_restrict_l0": 8.5, "mg_prolong_l0": 8.5, "mg_av": 12, "mg_at": 12,
+        "mg_restrict_l0": 8.5, "mg_psmooth_l0": 12.5, "mg_av": 12, "mg_at": 12,
         "mg_update": 32, "mg_init": 32, "fold_correction": 20,
         "mixed_b_init": 24, "mixed_update": 20, "mixed_residual": 24,
-             "add_inplace": 24, "div_vel": 32, "vel_corr": 56, "stats": 24,
-             "laplace_apply": 16, "jacobi_sweep": 24, "jacobi_prep": 24,
-             "jacobi_residual": 16}
+        "add_inplace": 24, "div_vel": 32, "vel_corr": 56, "stats": 24,
+        "laplace_apply": 16, "jacobi_sweep": 24, "jacobi_prep": 24,
+        "jacobi_residual": 16}
     return fixed.get(name)
 
 
@@ -118,3 +118,20 @@ def roofline(ktimes, ncells, prec):
             "traffic": None if tr is None else tr * ncells,
             "algorithmic_bytes_per_launch": b * ncells,
             "launch_ms": per_launch_ms, "share_of_device_time": kt["ms"] / total}
+
+
+def step_roofline(ktimes, ncells, steps, step_ms):
+    """Whole-step figure: the algorithmic bytes of every full-grid launch in
+    ``steps`` steps (coarse multigrid levels, about a seventh more, are not
+    counted) over the measured step time."""
+    peak, src = peaks()
+    total = 0.0
+    for name, kt in ktimes.items():
+        b = bytes_per_cell(name)
+        if b is not None:
+            total += b * ncells * kt["launches"]
+    per_step = total / max(1, steps)
+    achieved = per_step / (step_ms * 1e-3) / 1e9
+    return {"bytes_per_step": per_step, "bytes_per_cell": per_step / ncells,
+            "achieved": achieved, "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": achieved / peak}

@@ -83,19 +83,27 @@ def _ste_bf16(x):
     return x + (x.to(torch.bfloat16).to(x.dtype) - x).detach()
 
 
-def closure_torch(u, v, w, spacing, delta, W1, b1, W2, b2, W3, b3):
-    """Torch restatement of the tensor-core closure (BF16 inputs, weights and
-    hidden activations as straight-through roundings, FP32 accumulation)."""
+def closure_torch(u, v, w, spacing, delta, W1, b1, W2, b2, W3, b3, rounding=True):
+    """Torch restatement of the tensor-core closure: BF16 inputs, weights and
+    hidden activations as straight-through roundings, FP32 accumulation.
+    With rounding=False the same map is evaluated in FP64 without roundings
+    (a smooth function of the weights, for finite-difference checks)."""
     g9 = grad9(u, v, w, spacing)
     g2 = torch.mean(g9 * g9)
     g_rms = torch.sqrt(g2)
     shape = u.shape
-    x = _ste_bf16((g9.reshape(9, -1).T / g_rms).to(torch.float32))
-    h1 = _ste_bf16(torch.tanh(x @ _ste_bf16(W1).T + b1))
-    h2 = _ste_bf16(torch.tanh(h1 @ _ste_bf16(W2).T + b2))
-    y = h2 @ _ste_bf16(W3).T + b3
+    x = g9.reshape(9, -1).T / g_rms
+    if rounding:
+        rnd, dt = _ste_bf16, torch.float32
+    else:
+        rnd, dt = (lambda t: t), torch.float64
+    W1, b1, W2, b2, W3, b3 = (t.to(dt) for t in (W1, b1, W2, b2, W3, b3))
+    x = rnd(x.to(dt))
+    h1 = rnd(torch.tanh(x @ rnd(W1).T + b1))
+    h2 = rnd(torch.tanh(h1 @ rnd(W2).T + b2))
+    y = h2 @ rnd(W3).T + b3
     F = y.to(torch.float64) * ((delta * delta) * g2)
-    return F.T.reshape((6,) + tuple(shape))
+    return F.T.reshape((6,) + tuple(shape)).contiguous()
 
 
 class MLPClosure(torch.autograd.Function):
@@ -174,13 +182,18 @@ class Trainer:
     """RMSprop on the closure's FP32 weights; one call to ``step`` runs the
     LES window forward, the adjoint backward and one optimizer update."""
 
-    def __init__(self, cfg, targets, params=None, device="cuda"):
+    def __init__(self, cfg, targets, params=None, device="cuda", closure="kernel",
+                 dtype=torch.float32):
+        """closure: 'kernel' (tensor-core forward) or 'fp64' (the closure's
+        torch restatement in FP64 without BF16 roundings); dtype: type of the
+        master weights."""
         self.cfg = cfg
+        self.closure = closure
         self.targets = targets
         self.spacing = (2 * math.pi / cfg.n,) * 3
         self.delta = self.spacing[0]
         p0 = params if params is not None else M.xavier_init(cfg.mlp_seed)
-        self.params = [torch.tensor(np.asarray(p0[k]), dtype=torch.float32, device=device,
+        self.params = [torch.tensor(np.asarray(p0[k]), dtype=dtype, device=device,
                                     requires_grad=True) for k in PARAM_NAMES]
         self.opt = torch.optim.RMSprop(self.params, lr=cfg.lr)
         self.history = []
@@ -190,7 +203,11 @@ class Trainer:
         u, v, w = (t.clone() for t in self.targets[0])
         total = 0.0
         for n in range(cfg.steps):
-            F = MLPClosure.apply(u, v, w, *self.params, self.spacing, self.delta)
+            if self.closure == "kernel":
+                F = MLPClosure.apply(u, v, w, *self.params, self.spacing, self.delta)
+            else:
+                F = closure_torch(u, v, w, self.spacing, self.delta, *self.params,
+                                  rounding=False)
             u, v, w = A.forward_step(u, v, w, self.spacing, cfg.nu, 1.0, cfg.dt, sfs=F,
                                      rk4=True, tol=cfg.tol)
             total = total + mse((u, v, w), self.targets[n + 1])

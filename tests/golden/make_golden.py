@@ -32,6 +32,10 @@ run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
                    nu = 0.01, dt = 0.005, RK4 + BiCGStab to 1e-10, 5 steps:
                    final u, v, w, p and per-step max residual, iteration count
                    and monitor statistics.
+run_64.npz         PyFlow.run of the 64^3 plain-DNS workload (seed 0, k0 = 4,
+                   nu = 0.01, dt = 0.005, 20 RK4 steps): final u, v, w, p on
+                   every 4th cell of each axis, their sum / sum of squares /
+                   max, and the per-step residuals, iterations and statistics.
 """
 import os
 import sys
@@ -279,7 +283,7 @@ def jacobi_case(out):
     print("jacobi: max_res", r)
 
 
-def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005):
+def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005, stride=1):
     import torch
     ns = H.load_reference()
     import pyflow_b200.initial as ic
@@ -347,6 +351,21 @@ def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005):
         ns.pressure.Pressure_Base.applyOperator = orig_apply
         os.environ.pop("PF_FAKE_RANK", None)
     D = record["dom"]
+    if stride > 1:
+        # large case: the initial field is regenerated from its seed by the
+        # tests; keep the final fields on a strided subset plus their moments
+        fields = {k: getattr(D, "state_%s_P" % k).interior().numpy().copy()
+                  for k in ("u", "v", "w", "p")}
+        sub = {k + "_sub": a[::stride, ::stride, ::stride].copy() for k, a in fields.items()}
+        mom = np.array([[a.sum(), (a * a).sum(), np.abs(a).max()] for a in fields.values()])
+        np.savez_compressed(
+            os.path.join(out, "run_%d.npz" % n), shape=np.array([n, n, n]),
+            spacing=np.array([2 * np.pi / n] * 3), seed=seed, k0=4.0, urms=1.0, nu=nu,
+            rho=1.0, dt=dt, steps=steps, stride=stride, moments=mom,
+            max_res=np.array(record["max_res"]), iters=np.array(record["iters"]),
+            stats=np.array(record["stats"]), **sub)
+        print("run %d: iters" % n, record["iters"], "max_res", record["max_res"])
+        return
     np.savez_compressed(
         os.path.join(out, "run_%d.npz" % n), shape=np.array([n, n, n]),
         spacing=np.array([2 * np.pi / n] * 3), seed=seed, nu=nu, rho=1.0,
@@ -362,7 +381,7 @@ def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005):
 
 if __name__ == "__main__":
     out = HERE
-    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run"]
+    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run", "run64"]
     if "ops" in which:
         ops_case(out)
     if "jacobi" in which:
@@ -373,3 +392,7 @@ if __name__ == "__main__":
         adjoint_case(out)
     if "run" in which:
         run_case(out)
+    if "run64" in which:
+        # the 64^3 plain-DNS workload: seed 0, k0 = 4, nu = 0.01, dt = 0.005,
+        # 20 RK4 steps, BiCGStab to 1e-10
+        run_case(out, n=64, steps=20, stride=4)

@@ -196,3 +196,34 @@ def test_ragged_shapes_vs_oracle(ops, shape):
         assert np.abs(host(a) - b).max() <= 1e-8 * np.abs(b).max()
     st = host(ops.stats(uu, vv, ww, sp))
     assert st[4] <= 1e-8 * st[0] / min(sp)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-9), ("mixed", 1e-6), ("mixed_mg", 1e-6)])
+def test_run_64_twenty_steps_vs_reference(golden, prec, tol):
+    """The 64^3 plain-DNS workload (seed 0, nu = 0.01, dt = 0.005, 20 RK4 steps)
+    through the captured-graph path against the reference's own run."""
+    import pyflow_b200.initial as ic
+    from pyflow_b200.plan import StepPlan
+    g = golden("run_64.npz")
+    n = int(g["shape"][0])
+    f = [cu(a) for a in ic.spectral_velocity((n, n, n), k0=float(g["k0"]),
+                                             urms=float(g["urms"]), seed=int(g["seed"]))]
+    f += [torch.zeros_like(f[0]), torch.zeros_like(f[0])]
+    plan = StepPlan(*f, g["spacing"], float(g["nu"]), float(g["rho"]), float(g["dt"]),
+                    min_res=1e-10, max_it=1000, prec=prec)
+    its = []
+    for s in range(int(g["steps"])):
+        plan.launch(1)
+        st = plan.stats()
+        its.append(st["iterations"])
+        assert st["status"] == 0 and st["max_res"] <= 1e-10
+        np.testing.assert_allclose([st["max_u"], st["max_v"], st["max_w"], st["tke"]],
+                                   g["stats"][s][:4], rtol=max(tol, 1e-10))
+    plan.close()
+    if prec == "fp64":
+        assert np.all(np.abs(np.array(its) - g["iters"]) <= 0.1 * g["iters"])
+    k = int(g["stride"])
+    for a, key in zip(f[:3], ("u", "v", "w")):
+        ref = g[key + "_sub"]
+        got = host(a)[::k, ::k, ::k]
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max()

@@ -89,3 +89,31 @@ def test_forward_run_32(golden):
         ref = g[key]
         assert np.abs(a - ref).max() <= 1e-11 * np.abs(ref).max()
     assert np.abs(p - g["p"]).max() <= 1e-9 * np.abs(g["p"]).max()
+
+
+def test_forward_run_64_twenty_steps(golden):
+    """The 64^3 plain-DNS workload (seed 0, nu = 0.01, dt = 0.005, 20 RK4
+    steps): the oracle follows the reference's own run step by step."""
+    import pyflow_b200.initial as ic
+    g = golden("run_64.npz")
+    n = int(g["shape"][0])
+    u, v, w = ic.spectral_velocity((n, n, n), k0=float(g["k0"]), urms=float(g["urms"]),
+                                   seed=int(g["seed"]))
+    p = np.zeros_like(u)
+    iters = []
+    for s in range(int(g["steps"])):
+        u, v, w, p, DP, r, it = O.forward_step(
+            g["spacing"], u, v, w, p, float(g["nu"]), float(g["rho"]),
+            float(g["dt"]), min_res=1e-10, max_it=1000)
+        iters.append(it)
+        st = O.stats(g["spacing"], u, v, w)
+        np.testing.assert_allclose(st[:4], g["stats"][s][:4], rtol=1e-10)
+    assert np.all(np.abs(np.array(iters) - g["iters"]) <= 0.1 * g["iters"])
+    k = int(g["stride"])
+    for a, key, mi in ((u, "u", 0), (v, "v", 1), (w, "w", 2), (p, "p", 3)):
+        ref = g[key + "_sub"]
+        tol = 1e-10 if key != "p" else 1e-8
+        assert np.abs(a[::k, ::k, ::k] - ref).max() <= tol * np.abs(ref).max()
+        m = g["moments"][mi]
+        np.testing.assert_allclose((a * a).sum(), m[1], rtol=1e-9)
+        np.testing.assert_allclose(np.abs(a).max(), m[2], rtol=tol)
