@@ -58,7 +58,7 @@ MAX_IT = 20000
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="dns128",
@@ -74,7 +74,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-kernel, e2e and MLP measurements")
-    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--cpu-sample-steps", type=int, default=8,
+                    help="oracle steps timed for cpu_baseline (about 10 s at 128^3)")
     ap.add_argument("--requests", type=int, default=64,
                     help="serve workload: number of requests")
     return ap.parse_args()

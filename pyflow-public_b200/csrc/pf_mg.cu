@@ -26,9 +26,10 @@
 // first smoothing pass, which computes them for every cell it loads.
 //
 // Execution by level size: large levels (the finest always) use the tiled
-// sweep of pf_sweep.cuh; mid-size levels one thread per cell (a sweep's
-// plane-by-plane march is latency-bound on small grids); on both, the
-// prolongation is fused into the first post-smoothing pass; every level of at
+// sweep of pf_sweep.cuh (prolongation: one thread per coarse cell updating its
+// 8 children); mid-size levels one thread per cell (a sweep's plane-by-plane
+// march is latency-bound on small grids) with the prolongation fused into the
+// first post-smoothing pass; every level of at
 // most 4096 cells runs inside ONE CTA in shared memory (mg_bottom), so the
 // bottom of the V-cycle is a single launch.
 //
@@ -310,31 +311,47 @@ mg_prolong_smooth_pw(Dims d, Dims c, LapCoef<float> cf, float wd,
     out[q] = fmaf(wd, b[q] - ax, yc);
 }
 
-// Swept levels: y = x + P xc computed for every cell the sweep loads (the
-// prolongation costs no pass of its own); out = y + w (b - A y)
-struct PhaseProlongSmooth {
-    static constexpr int R = 4;
-    const float *x, *b, *xc;
-    Dims c;
-    float* out;
-    float wd;
-    struct Raw { float y; };
-    struct Ext { float b; };
-    __device__ Raw raw(long long q, int i, int j, int k) const {
-        return Raw{x[q] + prolong_at(xc, c, i, j, k)};
-    }
-    __device__ Ext ext(long long q) const { return Ext{b[q]}; }
-    __device__ float op(const Raw& a) const { return a.y; }
-    __device__ void epi(long long q, float y, float ay, const Raw&, const Ext& e) {
-        out[q] = fmaf(wd, e.b - ay, y);
-    }
-};
-
-__global__ void __launch_bounds__(kBlock, 2)
-mg_prolong_smooth(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc,
-                  PhaseProlongSmooth ph) {
+// Swept levels: x += P xc with one thread per coarse cell, which loads its
+// 3x3x3 coarse neighbourhood once and updates its 8 children (z pairs as one
+// 8-byte access).  Needs even fine dimensions (always true below the top).
+__global__ void __launch_bounds__(256)
+mg_prolong_add(Dims f, Dims c, const float* __restrict__ xc, float* __restrict__ x,
+               const BicgScalars* sc) {
     if (sc->done) return;
-    sweep<float>(d, tl, cf, ph);
+    const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y;
+    const int I = blockIdx.z;
+    if (K >= c.nz || J >= c.ny) return;
+    float v[3][3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const long long pa = (long long)wrap(I + a - 1, c.nx) * c.ny * c.nz;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const long long pb = pa + (long long)wrap(J + b - 1, c.ny) * c.nz;
+#pragma unroll
+            for (int e = 0; e < 3; ++e) v[a][b][e] = __ldg(xc + pb + wrap(K + e - 1, c.nz));
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            // child (2I+a, 2J+b, 2K+cc): far neighbours at offset -1 (child 0) or +1 (child 1)
+            const int A2 = a ? 2 : 0, B2 = b ? 2 : 0;
+            float e2[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int C2 = cc ? 2 : 0;
+                e2[cc] = (27.0f * v[1][1][1] + 9.0f * (v[A2][1][1] + v[1][B2][1] + v[1][1][C2]) +
+                          3.0f * (v[A2][B2][1] + v[A2][1][C2] + v[1][B2][C2]) + v[A2][B2][C2]) *
+                         (1.0f / 64.0f);
+            }
+            const long long q = idx(f, 2 * I + a, 2 * J + b, 2 * K);
+            float2 xv = *reinterpret_cast<const float2*>(x + q);
+            xv.x = xv.x + e2[0];
+            xv.y = xv.y + e2[1];
+            *reinterpret_cast<float2*>(x + q) = xv;
+        }
 }
 
 // ------------------------------------------------- bottom of the V-cycle
@@ -818,11 +835,11 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
         const float* bl = l == 0 ? b0 : f.b;
         float* xl = l == 0 ? x0 : f.x;
         if (f.kind == kMgSwept) {
-            const char* np = l == 0 ? "mg_psmooth_l0" : "mg_psmooth";
+            const char* np = l == 0 ? "mg_prolong_l0" : "mg_prolong";
             const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
-            PhaseProlongSmooth a{xl, bl, c.x, c.d, f.t, f.wd};
-            PF_LAUNCH(np, s, mg_prolong_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(
-                f.d, f.tl, f.cf, sc, a));
+            PF_LAUNCH(np, s, mg_prolong_add<<<cgrid3(c.d), blk, 0, s>>>(f.d, c.d, c.x, xl, sc));
+            PhaseSmooth a{xl, bl, f.t, f.wd};
+            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, a));
             PhaseSmooth b{f.t, bl, xl, f.wd};
             PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, b));
         } else {

@@ -141,46 +141,87 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
     return __bfloat16_as_ushort(__float2bfloat16_rn(x));
 }
 
-__device__ inline void cell_gradients(const Dims& d, const double* __restrict__ u,
-                                      const double* __restrict__ v,
-                                      const double* __restrict__ w, long long cell,
-                                      double dxi, double dyi, double dzi, double* g) {
-    const int k = (int)(cell % d.nz);
-    const long long r = cell / d.nz;
-    const int j = (int)(r % d.ny), i = (int)(r / d.ny);
+// The 30 velocity values the nine gradients of one cell need, loaded ahead
+// of their use so the loads of the next tile overlap this tile's layers.
+struct CellNb {
+    double u[10], v[10], w[10];
+};
+
+__device__ inline void load_nb(const Dims& d, const double* __restrict__ u,
+                               const double* __restrict__ v, const double* __restrict__ w,
+                               long long cell, CellNb& nb) {
+    int i, j, k;
+    if (d.n < (1LL << 31)) {
+        const unsigned c = (unsigned)cell, nz = (unsigned)d.nz, ny = (unsigned)d.ny;
+        const unsigned r = c / nz;
+        k = (int)(c - r * nz);
+        i = (int)(r / ny);
+        j = (int)(r - (unsigned)i * ny);
+    } else {
+        k = (int)(cell % d.nz);
+        const long long r = cell / d.nz;
+        j = (int)(r % d.ny);
+        i = (int)(r / d.ny);
+    }
     const int ip = wrap(i + 1, d.nx), im = wrap(i - 1, d.nx);
     const int jp = wrap(j + 1, d.ny), jm = wrap(j - 1, d.ny);
     const int kp = wrap(k + 1, d.nz), km = wrap(k - 1, d.nz);
     auto L = [&](const double* f, int a, int b, int c) { return __ldg(f + idx(d, a, b, c)); };
+    // u: faces i, i+1 at (j,k), (j-1,k), (j+1,k), (j,k-1), (j,k+1)
+    nb.u[0] = L(u, ip, j, k);  nb.u[1] = L(u, i, j, k);
+    nb.u[2] = L(u, ip, jm, k); nb.u[3] = L(u, i, jm, k);
+    nb.u[4] = L(u, ip, jp, k); nb.u[5] = L(u, i, jp, k);
+    nb.u[6] = L(u, ip, j, km); nb.u[7] = L(u, i, j, km);
+    nb.u[8] = L(u, ip, j, kp); nb.u[9] = L(u, i, j, kp);
+    // v: faces j, j+1 at (i,k), (i-1,k), (i+1,k), (i,k-1), (i,k+1)
+    nb.v[0] = L(v, i, jp, k);  nb.v[1] = L(v, i, j, k);
+    nb.v[2] = L(v, im, jp, k); nb.v[3] = L(v, im, j, k);
+    nb.v[4] = L(v, ip, jp, k); nb.v[5] = L(v, ip, j, k);
+    nb.v[6] = L(v, i, jp, km); nb.v[7] = L(v, i, j, km);
+    nb.v[8] = L(v, i, jp, kp); nb.v[9] = L(v, i, j, kp);
+    // w: faces k, k+1 at (i,j), (i-1,j), (i+1,j), (i,j-1), (i,j+1)
+    nb.w[0] = L(w, i, j, kp);  nb.w[1] = L(w, i, j, k);
+    nb.w[2] = L(w, im, j, kp); nb.w[3] = L(w, im, j, k);
+    nb.w[4] = L(w, ip, j, kp); nb.w[5] = L(w, ip, j, k);
+    nb.w[6] = L(w, i, jm, kp); nb.w[7] = L(w, i, jm, k);
+    nb.w[8] = L(w, i, jp, kp); nb.w[9] = L(w, i, jp, k);
+}
+
+// The nine cell-centred gradients (the arithmetic of pf_sgs_closure model 2)
+__device__ inline void nb_gradients(const CellNb& nb, double dxi, double dyi, double dzi,
+                                    double* g) {
     {
-        const double c0 = 0.5 * (L(u, ip, j, k) + L(u, i, j, k));
-        const double cym = 0.5 * (L(u, ip, jm, k) + L(u, i, jm, k));
-        const double cyp = 0.5 * (L(u, ip, jp, k) + L(u, i, jp, k));
-        const double czm = 0.5 * (L(u, ip, j, km) + L(u, i, j, km));
-        const double czp = 0.5 * (L(u, ip, j, kp) + L(u, i, j, kp));
-        g[0] = (L(u, ip, j, k) - L(u, i, j, k)) * dxi;
+        const double* a = nb.u;
+        const double c0 = 0.5 * (a[0] + a[1]);
+        const double cym = 0.5 * (a[2] + a[3]);
+        const double cyp = 0.5 * (a[4] + a[5]);
+        const double czm = 0.5 * (a[6] + a[7]);
+        const double czp = 0.5 * (a[8] + a[9]);
+        g[0] = (a[0] - a[1]) * dxi;
         g[1] = (0.5 * (cyp + c0) - 0.5 * (c0 + cym)) * dyi;
         g[2] = (0.5 * (czp + c0) - 0.5 * (c0 + czm)) * dzi;
     }
     {
-        const double c0 = 0.5 * (L(v, i, jp, k) + L(v, i, j, k));
-        const double cxm = 0.5 * (L(v, im, jp, k) + L(v, im, j, k));
-        const double cxp = 0.5 * (L(v, ip, jp, k) + L(v, ip, j, k));
-        const double czm = 0.5 * (L(v, i, jp, km) + L(v, i, j, km));
-        const double czp = 0.5 * (L(v, i, jp, kp) + L(v, i, j, kp));
+        const double* a = nb.v;
+        const double c0 = 0.5 * (a[0] + a[1]);
+        const double cxm = 0.5 * (a[2] + a[3]);
+        const double cxp = 0.5 * (a[4] + a[5]);
+        const double czm = 0.5 * (a[6] + a[7]);
+        const double czp = 0.5 * (a[8] + a[9]);
         g[3] = (0.5 * (cxp + c0) - 0.5 * (c0 + cxm)) * dxi;
-        g[4] = (L(v, i, jp, k) - L(v, i, j, k)) * dyi;
+        g[4] = (a[0] - a[1]) * dyi;
         g[5] = (0.5 * (czp + c0) - 0.5 * (c0 + czm)) * dzi;
     }
     {
-        const double c0 = 0.5 * (L(w, i, j, kp) + L(w, i, j, k));
-        const double cxm = 0.5 * (L(w, im, j, kp) + L(w, im, j, k));
-        const double cxp = 0.5 * (L(w, ip, j, kp) + L(w, ip, j, k));
-        const double cym = 0.5 * (L(w, i, jm, kp) + L(w, i, jm, k));
-        const double cyp = 0.5 * (L(w, i, jp, kp) + L(w, i, jp, k));
+        const double* a = nb.w;
+        const double c0 = 0.5 * (a[0] + a[1]);
+        const double cxm = 0.5 * (a[2] + a[3]);
+        const double cxp = 0.5 * (a[4] + a[5]);
+        const double cym = 0.5 * (a[6] + a[7]);
+        const double cyp = 0.5 * (a[8] + a[9]);
         g[6] = (0.5 * (cxp + c0) - 0.5 * (c0 + cxm)) * dxi;
         g[7] = (0.5 * (cyp + c0) - 0.5 * (c0 + cym)) * dyi;
-        g[8] = (L(w, i, j, kp) - L(w, i, j, k)) * dzi;
+        g[8] = (a[0] - a[1]) * dzi;
     }
 }
 
@@ -254,13 +295,18 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     uint32_t phase = 0;
     bool ok = true;
     const long long ntiles = (d.n + kTile - 1) / kTile;
+    CellNb nb;
+    {
+        const long long c0 = (long long)blockIdx.x * kTile + tid;
+        if (blockIdx.x < ntiles && c0 < d.n) load_nb(d, u, v, w, c0, nb);
+    }
     for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const long long cell = t * kTile + tid;
         const bool valid = cell < d.n;
         // ---- features -> X (row tid)
         {
             double g[9];
-            if (valid) cell_gradients(d, u, v, w, cell, dxi, dyi, dzi, g);
+            if (valid) nb_gradients(nb, dxi, dyi, dzi, g);
             uint32_t p[8];
 #pragma unroll
             for (int e = 0; e < 8; ++e) {
@@ -280,6 +326,11 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
             tc_fence_after();
             mma_bf16(d1, smem_desc(smem_u32(sX)), smem_desc(smem_u32(sW1)), id128, 0u);
             commit(bar);
+        }
+        // the next tile's neighbourhood loads run under this tile's layers
+        {
+            const long long cn = (t + gridDim.x) * kTile + tid;
+            if (t + gridDim.x < ntiles && cn < d.n) load_nb(d, u, v, w, cn, nb);
         }
         ok = __syncthreads_and(wait_phase(bar, phase));
         phase ^= 1u;

@@ -15,6 +15,7 @@
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
 #include "pf_profile.cuh"
+#include "pf_sweep.cuh"
 
 namespace pf {
 
@@ -33,49 +34,57 @@ __device__ inline T edge4(T a, T b, T c, T d) {
     return T(0.25) * (((a + b) + c) + d);
 }
 
-// Computes (ru, rv, rw) at cell (i, j, k).
+// Neighbourhood of cell (i, j, k) read from global memory (any viscosity /
+// SFS configuration): wrapped plane / row / column offsets of the neighbours
+// i-2 .. i+1 are computed once, every load is then two adds.
 template <typename T, typename TI>
-__device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i,
-                                int j, int k, T& ru_o, T& rv_o, T& rw_o) {
-    const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const T dxi = a.dxi, dyi = a.dyi, dzi = a.dzi, rho = a.rho;
-    // wrapped plane / row / column offsets of the neighbours i-2 .. i+1
-    // (computed once; every load is then two adds)
-    const long long P = (long long)ny * nz;
+struct GatherSrc {
+    const RhsArgs<T, TI>* a;
     long long xo[4];
     int yo[4], zo[4];
+    long long n;
+    __device__ GatherSrc(const Dims& d, const RhsArgs<T, TI>& args, int i, int j, int k) : a(&args) {
+        const long long P = (long long)d.ny * d.nz;
 #pragma unroll
-    for (int o = 0; o < 4; ++o) {
-        xo[o] = (long long)wrap(i + o - 2, nx) * P;
-        yo[o] = wrap(j + o - 2, ny) * nz;
-        zo[o] = wrap(k + o - 2, nz);
+        for (int o = 0; o < 4; ++o) {
+            xo[o] = (long long)wrap(i + o - 2, d.nx) * P;
+            yo[o] = wrap(j + o - 2, d.ny) * d.nz;
+            zo[o] = wrap(k + o - 2, d.nz);
+        }
+        n = d.n;
     }
-    auto off = [&](int di, int dj, int dk) -> long long {
+    __device__ long long off(int di, int dj, int dk) const {
         return xo[di + 2] + (long long)(yo[dj + 2] + zo[dk + 2]);
-    };
-    auto L = [&](const TI* f, int di, int dj, int dk) -> T {
-        return T(__ldg(f + off(di, dj, dk)));
-    };
-    auto LV = [&](int di, int dj, int dk) -> T {
-        return a.visc ? __ldg(a.visc + off(di, dj, dk)) : a.mu;
-    };
-    const long long n = d.n;
-    auto LS = [&](int c, int di, int dj, int dk) -> T {
-        return __ldg(a.sfs + (long long)c * n + off(di, dj, dk));
-    };
+    }
+    __device__ T u(int di, int dj, int dk) const { return T(__ldg(a->u + off(di, dj, dk))); }
+    __device__ T v(int di, int dj, int dk) const { return T(__ldg(a->v + off(di, dj, dk))); }
+    __device__ T w(int di, int dj, int dk) const { return T(__ldg(a->w + off(di, dj, dk))); }
+    __device__ T visc(int di, int dj, int dk) const { return __ldg(a->visc + off(di, dj, dk)); }
+    __device__ T sfs(int c, int di, int dj, int dk) const {
+        return __ldg(a->sfs + (long long)c * n + off(di, dj, dk));
+    }
+};
+
+// Computes (ru, rv, rw) of one cell from its neighbourhood S (velocity at
+// offsets -1..1, viscosity / SFS stresses at offsets -2..0 when present).
+template <typename T, class Src>
+__device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
+                                bool has_visc, bool has_sfs, T& ru_o, T& rv_o, T& rw_o) {
+    auto LV = [&](int di, int dj, int dk) -> T { return has_visc ? S.visc(di, dj, dk) : mu; };
+    auto LS = [&](int c, int di, int dj, int dk) -> T { return S.sfs(c, di, dj, dk); };
     // velocity neighbourhood
-    const T u_c = L(a.u, 0, 0, 0), u_xp = L(a.u, 1, 0, 0), u_xm = L(a.u, -1, 0, 0);
-    const T u_yp = L(a.u, 0, 1, 0), u_ym = L(a.u, 0, -1, 0), u_zp = L(a.u, 0, 0, 1);
-    const T u_zm = L(a.u, 0, 0, -1), u_xm_yp = L(a.u, -1, 1, 0), u_xp_ym = L(a.u, 1, -1, 0);
-    const T u_xm_zp = L(a.u, -1, 0, 1), u_xp_zm = L(a.u, 1, 0, -1);
-    const T v_c = L(a.v, 0, 0, 0), v_xp = L(a.v, 1, 0, 0), v_xm = L(a.v, -1, 0, 0);
-    const T v_yp = L(a.v, 0, 1, 0), v_ym = L(a.v, 0, -1, 0), v_zp = L(a.v, 0, 0, 1);
-    const T v_zm = L(a.v, 0, 0, -1), v_xm_yp = L(a.v, -1, 1, 0), v_xp_ym = L(a.v, 1, -1, 0);
-    const T v_ym_zp = L(a.v, 0, -1, 1), v_yp_zm = L(a.v, 0, 1, -1);
-    const T w_c = L(a.w, 0, 0, 0), w_xp = L(a.w, 1, 0, 0), w_xm = L(a.w, -1, 0, 0);
-    const T w_yp = L(a.w, 0, 1, 0), w_ym = L(a.w, 0, -1, 0), w_zp = L(a.w, 0, 0, 1);
-    const T w_zm = L(a.w, 0, 0, -1), w_xm_zp = L(a.w, -1, 0, 1), w_xp_zm = L(a.w, 1, 0, -1);
-    const T w_ym_zp = L(a.w, 0, -1, 1), w_yp_zm = L(a.w, 0, 1, -1);
+    const T u_c = S.u(0, 0, 0), u_xp = S.u(1, 0, 0), u_xm = S.u(-1, 0, 0);
+    const T u_yp = S.u(0, 1, 0), u_ym = S.u(0, -1, 0), u_zp = S.u(0, 0, 1);
+    const T u_zm = S.u(0, 0, -1), u_xm_yp = S.u(-1, 1, 0), u_xp_ym = S.u(1, -1, 0);
+    const T u_xm_zp = S.u(-1, 0, 1), u_xp_zm = S.u(1, 0, -1);
+    const T v_c = S.v(0, 0, 0), v_xp = S.v(1, 0, 0), v_xm = S.v(-1, 0, 0);
+    const T v_yp = S.v(0, 1, 0), v_ym = S.v(0, -1, 0), v_zp = S.v(0, 0, 1);
+    const T v_zm = S.v(0, 0, -1), v_xm_yp = S.v(-1, 1, 0), v_xp_ym = S.v(1, -1, 0);
+    const T v_ym_zp = S.v(0, -1, 1), v_yp_zm = S.v(0, 1, -1);
+    const T w_c = S.w(0, 0, 0), w_xp = S.w(1, 0, 0), w_xm = S.w(-1, 0, 0);
+    const T w_yp = S.w(0, 1, 0), w_ym = S.w(0, -1, 0), w_zp = S.w(0, 0, 1);
+    const T w_zm = S.w(0, 0, -1), w_xm_zp = S.w(-1, 0, 1), w_xp_zm = S.w(1, 0, -1);
+    const T w_ym_zp = S.w(0, -1, 1), w_yp_zm = S.w(0, 1, -1);
 
     // divergence / 3 at centres (div_vel_over, metric_staggered.py:424-433)
     auto div3 = [&](T ue, T uw, T vn, T vs, T wt, T wb) -> T {
@@ -97,7 +106,7 @@ __device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i,
 
     // edge viscosities (one cell below the flux, as in the reference)
     T vxy_c, vxy_ym, vxy_xm, vxz_c, vxz_zm, vxz_xm, vyz_c, vyz_zm, vyz_ym;
-    if (a.visc) {
+    if (has_visc) {
         vxy_c = edge4(LV(0, 0, 0), LV(-1, 0, 0), LV(0, -1, 0), LV(-1, -1, 0));
         vxy_ym = edge4(LV(0, -1, 0), LV(-1, -1, 0), LV(0, -2, 0), LV(-1, -2, 0));
         vxy_xm = edge4(LV(-1, 0, 0), LV(-2, 0, 0), LV(-1, -1, 0), LV(-2, -1, 0));
@@ -108,7 +117,7 @@ __device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i,
         vyz_zm = edge4(LV(0, 0, -1), LV(0, -1, -1), LV(0, 0, -2), LV(0, -1, -2));
         vyz_ym = edge4(LV(0, -1, 0), LV(0, -2, 0), LV(0, -1, -1), LV(0, -2, -1));
     } else {
-        const T m = a.mu;
+        const T m = mu;
         const T e = edge4(m, m, m, m);
         vxy_c = vxy_ym = vxy_xm = vxz_c = vxz_zm = vxz_xm = vyz_c = vyz_zm = vyz_ym = e;
     }
@@ -126,7 +135,7 @@ __device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i,
     T ux_p = fxx_c, ux_m = fxx_m, uy_p = fxy_c, uy_m = fxy_ym, uz_p = fxz_c, uz_m = fxz_zm;
     T vx_p = fxy_c, vx_m = fxy_xm, vy_p = fyy_c, vy_m = fyy_m, vz_p = fyz_c, vz_m = fyz_zm;
     T wx_p = fxz_c, wx_m = fxz_xm, wy_p = fyz_c, wy_m = fyz_ym, wz_p = fzz_c, wz_m = fzz_m;
-    if (a.sfs) {
+    if (has_sfs) {
         // 'tensor' SFS stresses, off-diagonals edge-averaged (interp_sc_xy/xz/yz)
         const T sxy_c = edge4(LS(3, 0, 0, 0), LS(3, -1, 0, 0), LS(3, 0, -1, 0), LS(3, -1, -1, 0));
         const T sxy_ym = edge4(LS(3, 0, -1, 0), LS(3, -1, -1, 0), LS(3, 0, -2, 0), LS(3, -1, -2, 0));
@@ -194,24 +203,22 @@ __device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i,
     ru_o = ru; rv_o = rv; rw_o = rw;
 }
 
-enum StageMode { kModeRhs = 0, kModeFirst = 1, kModeMid = 2, kModeLast = 3, kModeEuler = 4 };
+template <typename T, typename TI>
+__device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i, int j, int k,
+                                T& ru, T& rv, T& rw) {
+    GatherSrc<T, TI> S(d, a, i, j, k);
+    rhs_core<T>(S, a.mu, a.rho, a.dxi, a.dyi, a.dzi, a.visc != nullptr, a.sfs != nullptr,
+                ru, rv, rw);
+}
 
-// TS: stage-state storage type; TA: k-sum storage type.
-template <typename T, typename TI, typename TS, typename TA, int MODE>
-__global__ void __launch_bounds__(256)
-rhs_stage_kernel(Dims d, RhsArgs<T, TI> a, double* __restrict__ u,
-                 double* __restrict__ v, double* __restrict__ w,
-                 TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
-                 TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
-                 T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw,
-                 double hdt, double c6, double dt) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= d.nz || j >= d.ny) return;
-    T ku, kv, kw;
-    rhs_cell<T, TI>(d, a, i, j, k, ku, kv, kw);
-    const long long q = idx(d, i, j, k);
+enum StageMode { kModeRhs = 0, kModeFirst = 1, kModeMid = 2, kModeLast = 3, kModeK = 4 };
+
+// Stage arithmetic of one cell (the epilogue of every stage kernel).
+template <typename T, typename TS, typename TA, int MODE>
+__device__ __forceinline__ void stage_store(long long q, T ku, T kv, T kw, double* u,
+                                            double* v, double* w, TS* su, TS* sv, TS* sw,
+                                            TA* au, TA* av, TA* aw, T* ru, T* rv, T* rw,
+                                            double hdt, double c6) {
     if (MODE == kModeRhs) {
         ru[q] = ku; rv[q] = kv; rw[q] = kw;
     } else if (MODE == kModeFirst || MODE == kModeMid) {
@@ -230,10 +237,153 @@ rhs_stage_kernel(Dims d, RhsArgs<T, TI> a, double* __restrict__ u,
         u[q] = u[q] + c6 * (double(T(au[q]) + ku));
         v[q] = v[q] + c6 * (double(T(av[q]) + kv));
         w[q] = w[q] + c6 * (double(T(aw[q]) + kw));
-    } else {  // Euler
-        u[q] = u[q] + double(ku) * dt;
-        v[q] = v[q] + double(kv) * dt;
-        w[q] = w[q] + double(kw) * dt;
+    } else {  // kModeK: k alone (Euler applies it in a second pass)
+        au[q] = TA(ku); av[q] = TA(kv); aw[q] = TA(kw);
+    }
+}
+
+// TS: stage-state storage type; TA: k-sum storage type.  Gather form: any
+// viscosity / SFS configuration.
+template <typename T, typename TI, typename TS, typename TA, int MODE>
+__global__ void __launch_bounds__(256)
+rhs_stage_kernel(Dims d, RhsArgs<T, TI> a, double* __restrict__ u,
+                 double* __restrict__ v, double* __restrict__ w,
+                 TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
+                 TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
+                 T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw,
+                 double hdt, double c6) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= d.nz || j >= d.ny) return;
+    T ku, kv, kw;
+    rhs_cell<T, TI>(d, a, i, j, k, ku, kv, kw);
+    stage_store<T, TS, TA, MODE>(idx(d, i, j, k), ku, kv, kw, u, v, w, su, sv, sw, au, av,
+                                 aw, ru, rv, rw, hdt, c6);
+}
+
+// ---------------------------------------------------------------------------
+// Tiled form (constant viscosity, no SFS stresses: the DNS hot path).  A block
+// of 32 x 8 threads owns a 32 (z) x 16 (y) tile and marches along x; the
+// velocity of planes i-1, i, i+1 (with a one-cell y/z halo, corners
+// included) sits in a three-plane ring in shared memory, and plane i+2 is
+// loaded into registers while plane i is computed.  Every global value is
+// read once per tile; the flux arithmetic is rhs_core, unchanged.
+// ---------------------------------------------------------------------------
+constexpr int kRhsTY = 16;
+constexpr int kRhsSY = kRhsTY + 2, kRhsSZ = 34;
+constexpr int kRhsPos = kRhsSY * kRhsSZ;        // halo-extended plane tile
+constexpr int kRhsPPT = (kRhsPos + 255) / 256;  // positions per thread
+
+__host__ __device__ inline int pmod(int a, int n) {
+    const int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+template <typename T, typename TI>
+struct SmemSrc {
+    const TI (*sm)[3][kRhsSY][kRhsSZ];  // [field][slot][y][z]
+    int s0, s1, s2;                      // slots of planes i-1, i, i+1
+    int y, z;                            // the cell in the halo-extended tile
+    __device__ int slot(int di) const { return di < 0 ? s0 : (di == 0 ? s1 : s2); }
+    __device__ T u(int di, int dj, int dk) const { return T(sm[0][slot(di)][y + dj][z + dk]); }
+    __device__ T v(int di, int dj, int dk) const { return T(sm[1][slot(di)][y + dj][z + dk]); }
+    __device__ T w(int di, int dj, int dk) const { return T(sm[2][slot(di)][y + dj][z + dk]); }
+    __device__ T visc(int, int, int) const { return T(0); }
+    __device__ T sfs(int, int, int, int) const { return T(0); }
+};
+
+template <typename T, typename TI, typename TS, typename TA, int MODE>
+__global__ void __launch_bounds__(256, 2)
+rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
+                double* __restrict__ v, double* __restrict__ w,
+                TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
+                TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
+                T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw,
+                double hdt, double c6) {
+    __shared__ TI sm[3][3][kRhsSY][kRhsSZ];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const long long plane = (long long)d.ny * d.nz;
+    const TI* fld[3] = {a.u, a.v, a.w};
+    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+        const int tz = (int)(t % tl.ntz);
+        const long long rr = t / tl.ntz;
+        const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
+        const int k0 = tz * 32, j0 = tyy * kRhsTY, i0 = txx * tl.xc;
+        const int i1 = min(i0 + tl.xc, d.nx);
+        const int ez = min(32, d.nz - k0), ey = min(kRhsTY, d.ny - j0);
+        long long goff[kRhsPPT];
+        int soff[kRhsPPT];
+        bool pv[kRhsPPT];
+#pragma unroll
+        for (int p = 0; p < kRhsPPT; ++p) {
+            const int pos = tid + 256 * p;
+            pv[p] = pos < kRhsPos;
+            const int yy = pv[p] ? pos / kRhsSZ : 0, zz = pv[p] ? pos - yy * kRhsSZ : 0;
+            goff[p] = (long long)pmod(j0 + yy - 1, d.ny) * d.nz + pmod(k0 + zz - 1, d.nz);
+            soff[p] = yy * kRhsSZ + zz;
+        }
+        // prologue: planes i0-1, i0, i0+1 into slots 0, 1, 2
+#pragma unroll
+        for (int sl = 0; sl < 3; ++sl) {
+            const long long base = (long long)pmod(i0 - 1 + sl, d.nx) * plane;
+#pragma unroll
+            for (int f = 0; f < 3; ++f)
+#pragma unroll
+                for (int p = 0; p < kRhsPPT; ++p)
+                    if (pv[p]) (&sm[f][sl][0][0])[soff[p]] = __ldg(fld[f] + base + goff[p]);
+        }
+        __syncthreads();
+        for (int i = i0; i < i1; ++i) {
+            const int c = i - i0;
+            const int s0 = c % 3, s1 = (c + 1) % 3, s2 = (c + 2) % 3;
+            const bool more = i + 1 < i1;
+            TI pre[3][kRhsPPT];
+            if (more) {
+                const long long base = (long long)pmod(i + 2, d.nx) * plane;
+#pragma unroll
+                for (int f = 0; f < 3; ++f)
+#pragma unroll
+                    for (int p = 0; p < kRhsPPT; ++p)
+                        pre[f][p] = pv[p] ? __ldg(fld[f] + base + goff[p]) : TI(0);
+            }
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int jl = ty + 8 * r;
+                if (tx < ez && jl < ey) {
+                    SmemSrc<T, TI> S{sm, s0, s1, s2, jl + 1, tx + 1};
+                    T ku, kv, kw;
+                    rhs_core<T>(S, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false, ku, kv, kw);
+                    const long long q = (long long)i * plane + (long long)(j0 + jl) * d.nz + k0 + tx;
+                    stage_store<T, TS, TA, MODE>(q, ku, kv, kw, u, v, w, su, sv, sw, au, av,
+                                                 aw, ru, rv, rw, hdt, c6);
+                }
+            }
+            __syncthreads();
+            if (more) {
+#pragma unroll
+                for (int f = 0; f < 3; ++f)
+#pragma unroll
+                    for (int p = 0; p < kRhsPPT; ++p)
+                        if (pv[p]) (&sm[f][s0][0][0])[soff[p]] = pre[f][p];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Euler.step's update u += k dt (src/solver/advancer.py:49-57), applied after
+// k is complete so no kernel reads a velocity another block has updated.
+template <typename T>
+__global__ void __launch_bounds__(256)
+euler_apply(long long n, const T* __restrict__ ku, const T* __restrict__ kv,
+            const T* __restrict__ kw, double dt, double* __restrict__ u,
+            double* __restrict__ v, double* __restrict__ w) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        u[q] = u[q] + double(ku[q]) * dt;
+        v[q] = v[q] + double(kv[q]) * dt;
+        w[q] = w[q] + double(kw[q]) * dt;
     }
 }
 
@@ -263,19 +413,43 @@ cudaError_t launch_rhs(const pf_grid* g, int prec, const void* u,
                                            (const double*)visc, (const double*)sfs, mu, rho);
         PF_LAUNCH("rhs_rhs_f64", s, rhs_stage_kernel<double, double, double, double, kModeRhs><<<cell_grid(d), blk, 0, s>>>(
             d, a, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-            (double*)ru, (double*)rv, (double*)rw, 0.0, 0.0, 0.0));
+            (double*)ru, (double*)rv, (double*)rw, 0.0, 0.0));
     } else {
         auto a = make_args<float, float>(g, (const float*)u, (const float*)v, (const float*)w,
                                          (const float*)visc, (const float*)sfs, mu, rho);
         PF_LAUNCH("rhs_rhs_f32", s, rhs_stage_kernel<float, float, float, float, kModeRhs><<<cell_grid(d), blk, 0, s>>>(
             d, a, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-            (float*)ru, (float*)rv, (float*)rw, 0.0, 0.0, 0.0));
+            (float*)ru, (float*)rv, (float*)rw, 0.0, 0.0));
     }
     return cudaGetLastError();
 }
 
+// One stage: the tiled kernel for constant viscosity without SFS stresses,
+// the gather kernel otherwise.
+template <typename T, typename TI, int MODE>
+static void stage(const char* name, const Dims& d, const RhsArgs<T, TI>& a, double* u,
+                  double* v, double* w, T* st, T* acc, double hdt, double c6,
+                  cudaStream_t s) {
+    const long long n = d.n;
+    T* su = st ? st : nullptr;
+    T* sv = st ? st + n : nullptr;
+    T* sw = st ? st + 2 * n : nullptr;
+    dim3 blk(32, 8);
+    if (!a.visc && !a.sfs) {
+        const Tiling tl = make_tiling(d, kRhsTY);
+        PF_LAUNCH(name, s, rhs_stage_tiled<T, TI, T, T, MODE><<<tiled_grid(tl), blk, 0, s>>>(
+            d, tl, a, u, v, w, su, sv, sw, acc, acc + n, acc + 2 * n, nullptr, nullptr,
+            nullptr, hdt, c6));
+    } else {
+        PF_LAUNCH(name, s, rhs_stage_kernel<T, TI, T, T, MODE><<<cell_grid(d), blk, 0, s>>>(
+            d, a, u, v, w, su, sv, sw, acc, acc + n, acc + 2 * n, nullptr, nullptr, nullptr,
+            hdt, c6));
+    }
+}
+
 // Predictor step.  Workspace: stage states (2 ping-pong sets) and the k-sum,
-// each 3 fields of the stage type (double for PF_FP64, float for PF_MIXED).
+// each 3 fields of the stage type (double for PF_FP64, float for the mixed
+// forms).
 template <typename T>
 static cudaError_t predictor_impl(const pf_grid* g, int rk4, double* u,
                                   double* v, double* w, const T* visc,
@@ -283,30 +457,29 @@ static cudaError_t predictor_impl(const pf_grid* g, int rk4, double* u,
                                   double dt, T* ws, cudaStream_t s) {
     Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     const long long n = d.n;
-    dim3 blk(32, 8), grd = cell_grid(d);
     T *sa = ws, *sb = ws + 3 * n, *acc = ws + 6 * n;
     const double hdt = 0.5 * dt, c6 = dt / 6.0;
+    const bool f64 = sizeof(T) == 8;
     auto a0 = make_args<T, double>(g, u, v, w, visc, sfs, mu, rho);
     if (!rk4) {
-        PF_LAUNCH((sizeof(T) == 8 ? "rhs_euler_f64" : "rhs_euler_f32"), s, rhs_stage_kernel<T, double, T, T, kModeEuler><<<grd, blk, 0, s>>>(
-            d, a0, u, v, w, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-            nullptr, nullptr, nullptr, hdt, c6, dt));
+        stage<T, double, kModeK>(f64 ? "rhs_euler_f64" : "rhs_euler_f32", d, a0, u, v, w,
+                                 nullptr, acc, hdt, c6, s);
+        const int gp = (int)std::min<long long>((n + 1023) / 1024, 4096);
+        PF_LAUNCH("euler_apply", s, euler_apply<T><<<gp, 256, 0, s>>>(
+            n, acc, acc + n, acc + 2 * n, dt, u, v, w));
         return cudaGetLastError();
     }
-    PF_LAUNCH((sizeof(T) == 8 ? "rhs_first_f64" : "rhs_first_f32"), s, rhs_stage_kernel<T, double, T, T, kModeFirst><<<grd, blk, 0, s>>>(
-        d, a0, u, v, w, sa, sa + n, sa + 2 * n, acc, acc + n, acc + 2 * n,
-        nullptr, nullptr, nullptr, hdt, c6, dt));
+    stage<T, double, kModeFirst>(f64 ? "rhs_first_f64" : "rhs_first_f32", d, a0, u, v, w, sa,
+                                 acc, hdt, c6, s);
     auto a1 = make_args<T, T>(g, sa, sa + n, sa + 2 * n, visc, sfs, mu, rho);
-    PF_LAUNCH((sizeof(T) == 8 ? "rhs_mid_f64" : "rhs_mid_f32"), s, rhs_stage_kernel<T, T, T, T, kModeMid><<<grd, blk, 0, s>>>(
-        d, a1, u, v, w, sb, sb + n, sb + 2 * n, acc, acc + n, acc + 2 * n,
-        nullptr, nullptr, nullptr, hdt, c6, dt));
+    stage<T, T, kModeMid>(f64 ? "rhs_mid_f64" : "rhs_mid_f32", d, a1, u, v, w, sb, acc, hdt,
+                          c6, s);
     auto a2 = make_args<T, T>(g, sb, sb + n, sb + 2 * n, visc, sfs, mu, rho);
-    PF_LAUNCH((sizeof(T) == 8 ? "rhs_mid_f64" : "rhs_mid_f32"), s, rhs_stage_kernel<T, T, T, T, kModeMid><<<grd, blk, 0, s>>>(
-        d, a2, u, v, w, sa, sa + n, sa + 2 * n, acc, acc + n, acc + 2 * n,
-        nullptr, nullptr, nullptr, hdt, c6, dt));
-    PF_LAUNCH((sizeof(T) == 8 ? "rhs_last_f64" : "rhs_last_f32"), s, rhs_stage_kernel<T, T, T, T, kModeLast><<<grd, blk, 0, s>>>(
-        d, a1, u, v, w, nullptr, nullptr, nullptr, acc, acc + n, acc + 2 * n,
-        nullptr, nullptr, nullptr, hdt, c6, dt));
+    stage<T, T, kModeMid>(f64 ? "rhs_mid_f64" : "rhs_mid_f32", d, a2, u, v, w, sa, acc, hdt,
+                          c6, s);
+    // the reference's stage-4 state is u + dt/2 k3 = sa (Q1)
+    stage<T, T, kModeLast>(f64 ? "rhs_last_f64" : "rhs_last_f32", d, a1, u, v, w, nullptr,
+                           acc, hdt, c6, s);
     return cudaGetLastError();
 }
 
