@@ -12,6 +12,9 @@ cudaError_t launch_rhs(const pf_grid* g, int prec, const void* u,
                        void* rv, void* rw, cudaStream_t s);
 
 size_t predictor_ws_bytes(const pf_grid* g, int prec);
+// One-time per-device kernel attributes of the predictor (call before any
+// stream capture that contains predictor launches).
+cudaError_t predictor_prepare(int prec);
 cudaError_t launch_predictor(const pf_grid* g, int prec, int rk4, double* u,
                              double* v, double* w, const void* visc,
                              double mu, double rho, const void* sfs,

@@ -692,7 +692,7 @@ mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
 __global__ void __launch_bounds__(kBlock)
 mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
         float* res, float* res0, float* e, float* p0, float* p1, float* v,
-        int max_it, double tol) {
+        int max_it, double tol, double outer_tol) {
     __shared__ double sh[32];
     const double inv = sc->scale > 0.0 ? 1.0 / sc->scale : 0.0;
     double s = 0.0, m = 0.0;
@@ -714,7 +714,12 @@ mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
             sc->rho1 = tot; sc->rho2 = 1.0; sc->alpha = 0.0; sc->omega = 1.0;
             sc->buf1 = 0.0; sc->buf2 = 1.0;
             sc->max_res0 = mx; sc->max_res = 1.0; sc->iter = 0; sc->k = 0;
-            sc->max_it = max_it; sc->min_res = tol; sc->status = PF_OK;
+            // a pass only has to close the remaining gap to the refinement's
+            // tolerance (with a 3x margin): the last pass stops early
+            double t = tol;
+            if (outer_tol > 0.0 && sc->true_res > 0.0 && sc->max_b > 0.0)
+                t = fmin(0.5, fmax(tol, 0.3 * outer_tol * sc->max_b / sc->true_res));
+            sc->max_it = max_it; sc->min_res = t; sc->status = PF_OK;
             sc->done = (mx > 0.0 && mx == mx && !isinf(mx)) ? 0 : 1;
             if (!(mx == mx) || isinf(mx)) sc->status = PF_NONFINITE;
             sc->counter = 0u;
@@ -862,10 +867,10 @@ int mg_enqueue_setup(const MgPlan& P, cudaStream_t s) {
 }
 
 int mg_enqueue_init(const MgPlan& P, BicgScalars* sc, double* part, const double* rhs,
-                    double tol, int max_it, cudaStream_t s) {
+                    double tol, int max_it, cudaStream_t s, double outer_tol) {
     const Dims& d = P.lv[0].d;
     PF_LAUNCH("mg_init", s, mg_init<<<pointwise_grid(d.n), kBlock, 0, s>>>(
-        d, sc, part, rhs, P.res, P.res0, P.e, P.p[0], P.p[1], P.v, max_it, tol));
+        d, sc, part, rhs, P.res, P.res0, P.e, P.p[0], P.p[1], P.v, max_it, tol, outer_tol));
     return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;
 }
 
@@ -899,8 +904,8 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
 }
 
 int mg_inner_solve(const MgPlan& P, BicgScalars* sc, double* part, const double* rhs,
-                   double tol, int max_it, cudaStream_t s, BicgScalars* hs) {
-    int rc = mg_enqueue_init(P, sc, part, rhs, tol, std::max(1, max_it), s);
+                   double tol, int max_it, cudaStream_t s, BicgScalars* hs, double outer_tol) {
+    int rc = mg_enqueue_init(P, sc, part, rhs, tol, std::max(1, max_it), s, outer_tol);
     if (rc) return rc;
     int k = 0, chunk = 2;
     for (int guard = 0; guard < (1 << 20); ++guard) {

@@ -43,18 +43,21 @@ int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom);
 size_t mg_region_bytes(const pf_grid* g);
 // Carve the vectors from `region` (mg_region_bytes long, 256-byte aligned).
 int mg_setup(const pf_grid* g, void* region, MgPlan* P);
-// One inner solve: A e = rhs / sc->scale to relative max-norm `tol` (host
-// polls between chunks).  Leaves the iteration count and status in sc.
+// One inner solve: A e = rhs / sc->scale to relative max-norm `tol`, or
+// looser when the refinement (outer tolerance `outer_tol`, current true
+// residual sc->true_res of max|b| sc->max_b) needs less; the host polls
+// between chunks.  Leaves the iteration count and status in sc.
 int mg_inner_solve(const MgPlan& P, BicgScalars* sc, double* part,
                    const double* rhs, double tol, int max_it, cudaStream_t s,
-                   BicgScalars* hs);
+                   BicgScalars* hs, double outer_tol = 0.0);
 // Per-solve set-up kernels (the coarsest level's pseudo-inverse); enqueue
 // once before the first inner solve that uses the vectors of `region`.
 int mg_enqueue_setup(const MgPlan& P, cudaStream_t s);
 // Kernels of the inner solve, for graph capture: initialisation and one
 // iteration with parity k & 1 (kernels of a finished solve return at once).
 int mg_enqueue_init(const MgPlan& P, BicgScalars* sc, double* part,
-                    const double* rhs, double tol, int max_it, cudaStream_t s);
+                    const double* rhs, double tol, int max_it, cudaStream_t s,
+                    double outer_tol = 0.0);
 int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
                          cudaStream_t s, int use_cond = 0,
                          cudaGraphConditionalHandle cond = 0);

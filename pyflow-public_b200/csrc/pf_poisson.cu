@@ -508,7 +508,8 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
             if (!use64) {
                 float* e = e32;
                 if (mg.L) {
-                    const int rc = mg_inner_solve(mg, sc, part, rhs, kInnerTol, max_it - total, s, &hs);
+                    const int rc = mg_inner_solve(mg, sc, part, rhs, kInnerTol, max_it - total, s,
+                                                  &hs, min_res);
                     if (rc) return rc;
                     e = mg.e;
                 } else {
@@ -928,6 +929,7 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
         const int e = mg_setup(g, R, &mg);
         if (e != PF_OK && e != PF_ERR_BAD_ARG) return e;
     }
+    if (predictor_prepare(prec) != cudaSuccess) return PF_ERR_CUDA;
     cudaStream_t cs;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return PF_ERR_CUDA;
     prof_suspend(true);
@@ -979,7 +981,7 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
             cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;
             if ((rc = capture_begin(cs, nullptr))) break;
             if (mg.L) {
-                mg_enqueue_init(mg, sc, part, rr, kInnerTol, max_it, cs);
+                mg_enqueue_init(mg, sc, part, rr, kInnerTol, max_it, cs, min_res);
             } else {
                 bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, rr, 0.0, 0.0, v32, e32,
                                                              max_it, kInnerTol);

@@ -264,31 +264,64 @@ rhs_stage_kernel(Dims d, RhsArgs<T, TI> a, double* __restrict__ u,
 
 // ---------------------------------------------------------------------------
 // Tiled form (constant viscosity, no SFS stresses: the DNS hot path).  A block
-// of 32 x 8 threads owns a 32 (z) x 16 (y) tile and marches along x; the
-// velocity of planes i-1, i, i+1 (with a one-cell y/z halo, corners
-// included) sits in a three-plane ring in shared memory, and plane i+2 is
-// loaded into registers while plane i is computed.  Every global value is
-// read once per tile; the flux arithmetic is rhs_core, unchanged.
+// of 32 x 8 threads owns a 32 (z) x 16 (y) tile and marches along x.  The
+// velocity of planes i-1, i, i+1 (with a one-cell y/z halo, corners included)
+// sits in a four-slot ring in shared memory; while plane i is computed,
+// cp.async copies plane i+2 into the free slot and the per-cell stage inputs
+// of plane i+1 (u, v, w and the k-sum) into a second buffer, so no thread
+// waits on global memory inside the march and no registers hold the
+// prefetch.  Every global value is read once per tile; the flux arithmetic
+// is rhs_core, unchanged.
 // ---------------------------------------------------------------------------
 constexpr int kRhsTY = 16;
 constexpr int kRhsSY = kRhsTY + 2, kRhsSZ = 34;
 constexpr int kRhsPos = kRhsSY * kRhsSZ;        // halo-extended plane tile
 constexpr int kRhsPPT = (kRhsPos + 255) / 256;  // positions per thread
+constexpr int kRhsCells = 32 * kRhsTY;          // owned cells per plane
 
 __host__ __device__ inline int pmod(int a, int n) {
     const int r = a % n;
     return r < 0 ? r + n : r;
 }
 
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if (BYTES == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// dynamic shared memory of the tiled stage kernel
+template <typename TI, typename TA, int MODE>
+struct RhsSmem {
+    static constexpr bool kU = MODE == kModeFirst || MODE == kModeMid || MODE == kModeLast;
+    static constexpr bool kA = MODE == kModeMid || MODE == kModeLast;
+    static constexpr size_t kEu = kU ? 2 * 3 * kRhsCells * sizeof(double) : 0;  // [2][3][cells]
+    static constexpr size_t kRing = 4 * 3 * kRhsPos * sizeof(TI);            // [4][3][pos]
+    static constexpr size_t kEa = kA ? 2 * 3 * kRhsCells * sizeof(TA) : 0;      // [2][3][cells]
+    static constexpr size_t bytes = kEu + kRing + kEa;
+};
+
 template <typename T, typename TI>
 struct SmemSrc {
-    const TI (*sm)[3][kRhsSY][kRhsSZ];  // [field][slot][y][z]
-    int s0, s1, s2;                      // slots of planes i-1, i, i+1
-    int y, z;                            // the cell in the halo-extended tile
-    __device__ int slot(int di) const { return di < 0 ? s0 : (di == 0 ? s1 : s2); }
-    __device__ T u(int di, int dj, int dk) const { return T(sm[0][slot(di)][y + dj][z + dk]); }
-    __device__ T v(int di, int dj, int dk) const { return T(sm[1][slot(di)][y + dj][z + dk]); }
-    __device__ T w(int di, int dj, int dk) const { return T(sm[2][slot(di)][y + dj][z + dk]); }
+    const TI* ring;
+    int s0, s1, s2;  // slots of planes i-1, i, i+1
+    int y, z;        // the cell in the halo-extended tile
+    __device__ const TI* f(int fld, int di) const {
+        const int sl = di < 0 ? s0 : (di == 0 ? s1 : s2);
+        return ring + (sl * 3 + fld) * kRhsPos;
+    }
+    __device__ T u(int di, int dj, int dk) const { return T(f(0, di)[(y + dj) * kRhsSZ + z + dk]); }
+    __device__ T v(int di, int dj, int dk) const { return T(f(1, di)[(y + dj) * kRhsSZ + z + dk]); }
+    __device__ T w(int di, int dj, int dk) const { return T(f(2, di)[(y + dj) * kRhsSZ + z + dk]); }
     __device__ T visc(int, int, int) const { return T(0); }
     __device__ T sfs(int, int, int, int) const { return T(0); }
 };
@@ -299,12 +332,18 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
                 double* __restrict__ v, double* __restrict__ w,
                 TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
                 TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
-                T* __restrict__ ru, T* __restrict__ rv, T* __restrict__ rw,
                 double hdt, double c6) {
-    __shared__ TI sm[3][3][kRhsSY][kRhsSZ];
+    using SM = RhsSmem<TI, TA, MODE>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* eu = reinterpret_cast<double*>(smraw);
+    TI* ring = reinterpret_cast<TI*>(smraw + SM::kEu);
+    TA* ea = reinterpret_cast<TA*>(smraw + SM::kEu + SM::kRing);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const long long plane = (long long)d.ny * d.nz;
     const TI* fld[3] = {a.u, a.v, a.w};
+    double* U[3] = {u, v, w};
+    TA* A[3] = {au, av, aw};
+    TS* S[3] = {su, sv, sw};
     for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int tz = (int)(t % tl.ntz);
         const long long rr = t / tl.ntz;
@@ -323,53 +362,99 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
             goff[p] = (long long)pmod(j0 + yy - 1, d.ny) * d.nz + pmod(k0 + zz - 1, d.nz);
             soff[p] = yy * kRhsSZ + zz;
         }
-        // prologue: planes i0-1, i0, i0+1 into slots 0, 1, 2
+        // this thread's owned cells (rows ty, ty + 8) within the plane
+        bool cv[2];
+        long long coff[2];
 #pragma unroll
-        for (int sl = 0; sl < 3; ++sl) {
-            const long long base = (long long)pmod(i0 - 1 + sl, d.nx) * plane;
+        for (int r = 0; r < 2; ++r) {
+            const int jl = ty + 8 * r;
+            cv[r] = tx < ez && jl < ey;
+            coff[r] = (long long)(j0 + jl) * d.nz + k0 + tx;
+        }
+        auto load_plane = [&](int x, int slot) {
+            const long long base = (long long)pmod(x, d.nx) * plane;
 #pragma unroll
             for (int f = 0; f < 3; ++f)
 #pragma unroll
                 for (int p = 0; p < kRhsPPT; ++p)
-                    if (pv[p]) (&sm[f][sl][0][0])[soff[p]] = __ldg(fld[f] + base + goff[p]);
-        }
+                    if (pv[p])
+                        cp_async<sizeof(TI)>(ring + (slot * 3 + f) * kRhsPos + soff[p],
+                                             fld[f] + base + goff[p]);
+        };
+        auto load_epi = [&](int x, int buf) {
+            const long long base = (long long)x * plane;
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (!cv[r]) continue;
+                const int c = (ty + 8 * r) * 32 + tx;
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    if (SM::kU) cp_async<8>(eu + (buf * 3 + f) * kRhsCells + c, U[f] + base + coff[r]);
+                    if (SM::kA)
+                        cp_async<sizeof(TA)>(ea + (buf * 3 + f) * kRhsCells + c, A[f] + base + coff[r]);
+                }
+            }
+        };
+        // prologue: planes i0-1, i0, i0+1 into slots 0, 1, 2; stage inputs of i0
+        load_plane(i0 - 1, 0);
+        load_plane(i0, 1);
+        load_plane(i0 + 1, 2);
+        load_epi(i0, 0);
+        cp_async_commit();
+        cp_async_wait_all();
         __syncthreads();
         for (int i = i0; i < i1; ++i) {
             const int c = i - i0;
-            const int s0 = c % 3, s1 = (c + 1) % 3, s2 = (c + 2) % 3;
-            const bool more = i + 1 < i1;
-            TI pre[3][kRhsPPT];
-            if (more) {
-                const long long base = (long long)pmod(i + 2, d.nx) * plane;
-#pragma unroll
-                for (int f = 0; f < 3; ++f)
-#pragma unroll
-                    for (int p = 0; p < kRhsPPT; ++p)
-                        pre[f][p] = pv[p] ? __ldg(fld[f] + base + goff[p]) : TI(0);
+            const int s0 = c & 3, s1 = (c + 1) & 3, s2 = (c + 2) & 3;
+            const int buf = c & 1;
+            if (i + 1 < i1) {
+                load_plane(i + 2, (c + 3) & 3);
+                load_epi(i + 1, buf ^ 1);
+                cp_async_commit();
             }
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
+                if (!cv[r]) continue;
                 const int jl = ty + 8 * r;
-                if (tx < ez && jl < ey) {
-                    SmemSrc<T, TI> S{sm, s0, s1, s2, jl + 1, tx + 1};
-                    T ku, kv, kw;
-                    rhs_core<T>(S, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false, ku, kv, kw);
-                    const long long q = (long long)i * plane + (long long)(j0 + jl) * d.nz + k0 + tx;
-                    stage_store<T, TS, TA, MODE>(q, ku, kv, kw, u, v, w, su, sv, sw, au, av,
-                                                 aw, ru, rv, rw, hdt, c6);
+                SmemSrc<T, TI> src{ring, s0, s1, s2, jl + 1, tx + 1};
+                T k3[3];
+                rhs_core<T>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false, k3[0], k3[1], k3[2]);
+                const long long q = (long long)i * plane + coff[r];
+                const int cc = jl * 32 + tx;
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    const T kf = k3[f];
+                    if (MODE == kModeFirst || MODE == kModeMid) {
+                        // ZAXPY(h, k, u) = h*k + u (src/data/state.py:157-165)
+                        S[f][q] = TS(hdt * double(kf) + eu[(buf * 3 + f) * kRhsCells + cc]);
+                        if (MODE == kModeFirst) A[f][q] = TA(kf);
+                        else A[f][q] = TA(T(ea[(buf * 3 + f) * kRhsCells + cc]) + T(2.0) * kf);
+                    } else if (MODE == kModeLast) {
+                        U[f][q] = eu[(buf * 3 + f) * kRhsCells + cc] +
+                                  c6 * (double(T(ea[(buf * 3 + f) * kRhsCells + cc]) + kf));
+                    } else {  // kModeK
+                        A[f][q] = TA(kf);
+                    }
                 }
             }
-            __syncthreads();
-            if (more) {
-#pragma unroll
-                for (int f = 0; f < 3; ++f)
-#pragma unroll
-                    for (int p = 0; p < kRhsPPT; ++p)
-                        if (pv[p]) (&sm[f][s0][0][0])[soff[p]] = pre[f][p];
-            }
+            cp_async_wait_all();
             __syncthreads();
         }
     }
+}
+
+// Sets the dynamic shared-memory limit of one tiled instance once per device.
+template <typename T, typename TI, int MODE>
+static cudaError_t tiled_prepare() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(
+        rhs_stage_tiled<T, TI, T, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)RhsSmem<TI, T, MODE>::bytes);
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+    return e;
 }
 
 // Euler.step's update u += k dt (src/solver/advancer.py:49-57), applied after
@@ -427,7 +512,7 @@ cudaError_t launch_rhs(const pf_grid* g, int prec, const void* u,
 // One stage: the tiled kernel for constant viscosity without SFS stresses,
 // the gather kernel otherwise.
 template <typename T, typename TI, int MODE>
-static void stage(const char* name, const Dims& d, const RhsArgs<T, TI>& a, double* u,
+static cudaError_t stage(const char* name, const Dims& d, const RhsArgs<T, TI>& a, double* u,
                   double* v, double* w, T* st, T* acc, double hdt, double c6,
                   cudaStream_t s) {
     const long long n = d.n;
@@ -437,14 +522,17 @@ static void stage(const char* name, const Dims& d, const RhsArgs<T, TI>& a, doub
     dim3 blk(32, 8);
     if (!a.visc && !a.sfs) {
         const Tiling tl = make_tiling(d, kRhsTY);
-        PF_LAUNCH(name, s, rhs_stage_tiled<T, TI, T, T, MODE><<<tiled_grid(tl), blk, 0, s>>>(
-            d, tl, a, u, v, w, su, sv, sw, acc, acc + n, acc + 2 * n, nullptr, nullptr,
-            nullptr, hdt, c6));
+        const cudaError_t e = tiled_prepare<T, TI, MODE>();
+        if (e != cudaSuccess) return e;
+        PF_LAUNCH(name, s, rhs_stage_tiled<T, TI, T, T, MODE><<<tiled_grid(tl), blk,
+                                                              RhsSmem<TI, T, MODE>::bytes, s>>>(
+            d, tl, a, u, v, w, su, sv, sw, acc, acc + n, acc + 2 * n, hdt, c6));
     } else {
         PF_LAUNCH(name, s, rhs_stage_kernel<T, TI, T, T, MODE><<<cell_grid(d), blk, 0, s>>>(
             d, a, u, v, w, su, sv, sw, acc, acc + n, acc + 2 * n, nullptr, nullptr, nullptr,
             hdt, c6));
     }
+    return cudaGetLastError();
 }
 
 // Predictor step.  Workspace: stage states (2 ping-pong sets) and the k-sum,
@@ -462,25 +550,44 @@ static cudaError_t predictor_impl(const pf_grid* g, int rk4, double* u,
     const bool f64 = sizeof(T) == 8;
     auto a0 = make_args<T, double>(g, u, v, w, visc, sfs, mu, rho);
     if (!rk4) {
-        stage<T, double, kModeK>(f64 ? "rhs_euler_f64" : "rhs_euler_f32", d, a0, u, v, w,
-                                 nullptr, acc, hdt, c6, s);
+        cudaError_t e = stage<T, double, kModeK>(f64 ? "rhs_euler_f64" : "rhs_euler_f32", d,
+                                                 a0, u, v, w, nullptr, acc, hdt, c6, s);
+        if (e != cudaSuccess) return e;
         const int gp = (int)std::min<long long>((n + 1023) / 1024, 4096);
         PF_LAUNCH("euler_apply", s, euler_apply<T><<<gp, 256, 0, s>>>(
             n, acc, acc + n, acc + 2 * n, dt, u, v, w));
         return cudaGetLastError();
     }
-    stage<T, double, kModeFirst>(f64 ? "rhs_first_f64" : "rhs_first_f32", d, a0, u, v, w, sa,
-                                 acc, hdt, c6, s);
+    cudaError_t e = stage<T, double, kModeFirst>(f64 ? "rhs_first_f64" : "rhs_first_f32", d,
+                                                 a0, u, v, w, sa, acc, hdt, c6, s);
+    if (e != cudaSuccess) return e;
     auto a1 = make_args<T, T>(g, sa, sa + n, sa + 2 * n, visc, sfs, mu, rho);
-    stage<T, T, kModeMid>(f64 ? "rhs_mid_f64" : "rhs_mid_f32", d, a1, u, v, w, sb, acc, hdt,
-                          c6, s);
+    e = stage<T, T, kModeMid>(f64 ? "rhs_mid_f64" : "rhs_mid_f32", d, a1, u, v, w, sb, acc,
+                              hdt, c6, s);
+    if (e != cudaSuccess) return e;
     auto a2 = make_args<T, T>(g, sb, sb + n, sb + 2 * n, visc, sfs, mu, rho);
-    stage<T, T, kModeMid>(f64 ? "rhs_mid_f64" : "rhs_mid_f32", d, a2, u, v, w, sa, acc, hdt,
-                          c6, s);
+    e = stage<T, T, kModeMid>(f64 ? "rhs_mid_f64" : "rhs_mid_f32", d, a2, u, v, w, sa, acc,
+                              hdt, c6, s);
+    if (e != cudaSuccess) return e;
     // the reference's stage-4 state is u + dt/2 k3 = sa (Q1)
-    stage<T, T, kModeLast>(f64 ? "rhs_last_f64" : "rhs_last_f32", d, a1, u, v, w, nullptr,
-                           acc, hdt, c6, s);
+    e = stage<T, T, kModeLast>(f64 ? "rhs_last_f64" : "rhs_last_f32", d, a1, u, v, w, nullptr,
+                               acc, hdt, c6, s);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+cudaError_t predictor_prepare(int prec) {
+    cudaError_t e = cudaSuccess;
+    if (prec == PF_FP64) {
+        if ((e = tiled_prepare<double, double, kModeK>())) return e;
+        if ((e = tiled_prepare<double, double, kModeFirst>())) return e;
+        if ((e = tiled_prepare<double, double, kModeMid>())) return e;
+        return tiled_prepare<double, double, kModeLast>();
+    }
+    if ((e = tiled_prepare<float, double, kModeK>())) return e;
+    if ((e = tiled_prepare<float, double, kModeFirst>())) return e;
+    if ((e = tiled_prepare<float, float, kModeMid>())) return e;
+    return tiled_prepare<float, float, kModeLast>();
 }
 
 size_t predictor_ws_bytes(const pf_grid* g, int prec) {
