@@ -50,6 +50,7 @@ constexpr int kMgCoarseSweeps = 32;
 // ------------------------------------------------------------ sweep phases
 // Sources of the first (from-zero) smoothing pass.
 struct SrcPlain {  // b of a coarse level
+    static constexpr int kRows = 8;
     const float* b;
     struct Raw { float b; };
     __device__ void setup(const BicgScalars*) {}
@@ -59,6 +60,7 @@ struct SrcPlain {  // b of a coarse level
 };
 
 struct SrcP {  // p' = res + beta (p - omega v), stored to p_new
+    static constexpr int kRows = 4;
     const float *res, *p_old, *v;
     float* p_new;
     float beta, omega;
@@ -75,6 +77,7 @@ struct SrcP {  // p' = res + beta (p - omega v), stored to p_new
 };
 
 struct SrcS {  // s = res - alpha v, stored to s
+    static constexpr int kRows = 4;
     const float *res, *v;
     float* s;
     float alpha;
@@ -88,7 +91,7 @@ struct SrcS {  // s = res - alpha v, stored to s
 // x = w (2 b - w A b): two weighted-Jacobi sweeps from x = 0
 template <class Src>
 struct PhaseSmooth0 {
-    static constexpr int R = 4;
+    static constexpr int R = Src::kRows;
     Src src;
     float* x;
     float wd;
@@ -105,7 +108,7 @@ struct PhaseSmooth0 {
 
 // out = x + w (b - A x): one weighted-Jacobi sweep
 struct PhaseSmooth {
-    static constexpr int R = 4;
+    static constexpr int R = 8;  // one field in: 8 rows per thread keep more loads in flight
     const float *x, *b;
     float* out;
     float wd;
@@ -121,7 +124,7 @@ struct PhaseSmooth {
 
 // v = A ph and (v, res0)
 struct PhaseAv {
-    static constexpr int R = 4;
+    static constexpr int R = 8;  // one field in: 8 rows per thread keep more loads in flight
     const float *ph, *res0;
     float* v;
     double dot;
@@ -138,7 +141,7 @@ struct PhaseAv {
 
 // t = A sh, (t, s) and (t, t)
 struct PhaseAt {
-    static constexpr int R = 4;
+    static constexpr int R = 8;  // one field in: 8 rows per thread keep more loads in flight
     const float *sh, *s;
     float* t;
     double ts, tt;
@@ -741,6 +744,7 @@ int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom) {
         for (int q = 0; q < 3; ++q) l.cq[q] = -c64.c[q][2];
         l.b = l.x = l.t = nullptr;
         l.tl = make_tiling(l.d, 32);
+        l.tl8 = make_tiling(l.d, 64);
         l.kind = (L == 0 || l.d.n >= kMgSweepMin) ? kMgSwept
                  : (l.d.n > kMgBottomMax ? kMgPointwise : kMgBottom);
         ++L;
@@ -818,8 +822,8 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
             if (f.kind == kMgSwept) {
                 PhaseSmooth0<SrcPlain> ph{};
                 ph.src.b = f.b; ph.x = f.x; ph.wd = f.wd;
-                PF_LAUNCH("mg_smooth0", s, mg_smooth0<SrcPlain><<<tiled_grid(f.tl), blk, 0, s>>>(
-                    f.d, f.tl, f.cf, sc, ph));
+                PF_LAUNCH("mg_smooth0", s, mg_smooth0<SrcPlain><<<tiled_grid(f.tl8), blk, 0, s>>>(
+                    f.d, f.tl8, f.cf, sc, ph));
             } else {
                 PF_LAUNCH("mg_smooth0_pw", s, mg_smooth0_pw<<<cgrid3(f.d), blk, 0, s>>>(
                     f.d, f.cf, f.wd, f.b, f.x, sc));
@@ -844,9 +848,9 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
             const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
             PF_LAUNCH(np, s, mg_prolong_add<<<cgrid3(c.d), blk, 0, s>>>(f.d, c.d, c.x, xl, sc));
             PhaseSmooth a{xl, bl, f.t, f.wd};
-            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, a));
+            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl8), blk, 0, s>>>(f.d, f.tl8, f.cf, sc, a));
             PhaseSmooth b{f.t, bl, xl, f.wd};
-            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl), blk, 0, s>>>(f.d, f.tl, f.cf, sc, b));
+            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl8), blk, 0, s>>>(f.d, f.tl8, f.cf, sc, b));
         } else {
             PF_LAUNCH("mg_prolong_smooth_pw", s, mg_prolong_smooth_pw<<<cgrid3(f.d), blk, 0, s>>>(
                 f.d, c.d, f.cf, f.wd, c.x, xl, bl, f.t, sc));
@@ -878,7 +882,7 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
                          cudaStream_t s, int use_cond, cudaGraphConditionalHandle cond) {
     const MgLevel& f = P.lv[0];
     const dim3 blk(32, 8);
-    const int gt = tiled_grid(f.tl);
+    const int gt = tiled_grid(f.tl), gt8 = tiled_grid(f.tl8);
     float* p_new = P.p[k & 1];
     const float* p_old = P.p[(k & 1) ^ 1];
     {   // p update fused into the first smoothing pass of M p
@@ -888,7 +892,7 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
         PF_LAUNCH("mg_smooth0_p", s, mg_smooth0<SrcP><<<gt, blk, 0, s>>>(f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, p_new, P.ph, sc, s);
-    PF_LAUNCH("mg_av", s, mg_av<<<gt, blk, 0, s>>>(f.d, f.tl, f.cf, sc, part, P.ph, P.res0,
+    PF_LAUNCH("mg_av", s, mg_av<<<gt8, blk, 0, s>>>(f.d, f.tl8, f.cf, sc, part, P.ph, P.res0,
                                                    P.v, use_cond, cond));
     {   // s = res - alpha v fused into the first smoothing pass of M s
         PhaseSmooth0<SrcS> ph{};
@@ -897,7 +901,7 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
         PF_LAUNCH("mg_smooth0_s", s, mg_smooth0<SrcS><<<gt, blk, 0, s>>>(f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, P.s, P.sh, sc, s);
-    PF_LAUNCH("mg_at", s, mg_at<<<gt, blk, 0, s>>>(f.d, f.tl, f.cf, sc, part, P.sh, P.s, P.t));
+    PF_LAUNCH("mg_at", s, mg_at<<<gt8, blk, 0, s>>>(f.d, f.tl8, f.cf, sc, part, P.sh, P.s, P.t));
     PF_LAUNCH("mg_update", s, mg_update<<<pointwise_grid(f.d.n), kBlock, 0, s>>>(
         f.d, sc, part, P.e, P.ph, P.sh, P.s, P.t, P.res, P.res0, use_cond, cond));
     return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;

@@ -20,7 +20,7 @@ struct MgLevel {
     LapCoef<float> cf;  // the scaled operator -vol L with this level's spacing
     float wd;           // omega / diag(A)
     float *b, *x, *t;   // right-hand side, iterate, smoothing buffer
-    Tiling tl;
+    Tiling tl, tl8;  // tilings of the 4- and 8-row sweep phases
     int kind;
     double cq[3];       // vol / h_q^2: the operator's off-diagonal magnitudes
 };

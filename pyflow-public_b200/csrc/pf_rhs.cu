@@ -450,9 +450,14 @@ static cudaError_t tiled_prepare() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(
+    cudaError_t e = cudaFuncSetAttribute(
         rhs_stage_tiled<T, TI, T, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)RhsSmem<TI, T, MODE>::bytes);
+    // the largest shared-memory carveout, so two blocks fit on an SM
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(rhs_stage_tiled<T, TI, T, T, MODE>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }
