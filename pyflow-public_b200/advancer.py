@@ -14,6 +14,8 @@ def _fused_args(rhsClass):
     if not isinstance(rhsClass, ForwardRHS):
         return None
     r = rhsClass.rhs1
+    if getattr(r.sfsmodel, "modelType", None) == "source":
+        return None  # per-stage source closure: compose the stages
     mu, visc = visc_args(r.VISC)
     return dict(spacing=r.metric.spacing, mu=mu, rho=r.rho, visc=visc,
                 sfs=sfs_args(r.sfsmodel))

@@ -12,7 +12,8 @@ Optional configuration keys beyond the reference's:
                  refinement to the same tolerance) or 'mixed_mg' ('mixed' with
                  the FP32 passes preconditioned by a multigrid V-cycle);
   SFSmodel       also 'MLP' (the 9 -> 128 -> 128 -> 6 BF16 closure in the
-                 'tensor' slot, pyflow_b200.sfsmodel_mlp).
+                 'tensor' slot, pyflow_b200.sfsmodel_mlp); 'ML' is the
+                 reference's 'source' network (pyflow_b200.sfsmodel_ML).
 """
 import numpy as np
 import torch
@@ -74,8 +75,8 @@ class Domain:
             from . import sfsmodel_mlp
             self.sfsmodel = sfsmodel_mlp.residual_stress(inputConfig, decomp, geometry)
         elif sfs == "ML":
-            raise ValueError("the reference's 'source'-type ML closure is not "
-                             "supported; use SFSmodel='MLP'")
+            from . import sfsmodel_ML
+            self.sfsmodel = sfsmodel_ML.residual_stress(inputConfig, decomp, geometry)
         else:
             self.use_SFSmodel = False
             self.sfsmodel = sfsmodel_smagorinsky.stress_constCs(inputConfig, geometry)
@@ -139,7 +140,8 @@ class Domain:
                 self.sfsmodel.update(self.state_u_P, self.state_v_P,
                                      self.state_w_P, self.metric)
         fused = (self.doPressure and isinstance(self.forwardRHS, velocity.ForwardRHS)
-                 and (self.precision == "fp64" or not self.use_SFSmodel))
+                 and (self.precision == "fp64" or not self.use_SFSmodel)
+                 and self.sfsmodel.modelType != "source")
         if fused:
             mu, visc = velocity.visc_args(self.VISC_P)
             sfs = velocity.sfs_args(self.sfsmodel) if self.use_SFSmodel else None

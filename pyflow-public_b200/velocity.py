@@ -63,3 +63,11 @@ class rhs_NavierStokes:
                    self.metric.spacing, mu, self.rho, visc=visc,
                    sfs=sfs_args(self.sfsmodel),
                    out=(self.rhs_u, self.rhs_v, self.rhs_w))
+        if getattr(self.sfsmodel, "modelType", None) == "source":
+            # 'source' closures are evaluated at every stage's state and
+            # subtracted on the faces (src/solver/velocity.py:360-383)
+            self.sfsmodel.update(state_u.interior(), state_v.interior(), state_w.interior())
+            fu, fv, fw = self.sfsmodel.face_sources()
+            self.rhs_u.sub_(fu)
+            self.rhs_v.sub_(fv)
+            self.rhs_w.sub_(fw)

@@ -32,6 +32,9 @@ run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
                    nu = 0.01, dt = 0.005, RK4 + BiCGStab to 1e-10, 5 steps:
                    final u, v, w, p and per-step max residual, iteration count
                    and monitor statistics.
+ml_16.npz          rhs_NavierStokes.evaluate with the reference's 'source' ML
+                   closure (sfsmodel_ML, a seeded random network whose
+                   weights are stored in the fixture) on a 16^3 box.
 run_64.npz         PyFlow.run of the 64^3 plain-DNS workload (seed 0, k0 = 4,
                    nu = 0.01, dt = 0.005, 20 RK4 steps): final u, v, w, p on
                    every 4th cell of each axis, their sum / sum of squares /
@@ -283,6 +286,35 @@ def jacobi_case(out):
     print("jacobi: max_res", r)
 
 
+def ml_case(out):
+    """The reference's 'source' ML closure inside rhs_NavierStokes.evaluate
+    (src/solver/velocity.py:360-383) with a seeded random network."""
+    import torch
+    n = 16
+    S = H.make_setup(n, n, n, 2 * np.pi, 2 * np.pi, 2 * np.pi)
+    ns, d = S.ns, S.decomp
+    rng = np.random.default_rng(123)
+    u, v, w = (0.5 * rng.standard_normal((n, n, n)) for _ in range(3))
+    mu, rho = 0.01, 1.0
+
+    class IC:
+        simDt = 0.01
+
+    torch.manual_seed(5)
+    ml = ns.sfsmodel_ML.residual_stress(IC(), d, S.geo)
+    VISC = torch.ones(n + 4, n + 4, n + 4, dtype=torch.float64) * mu
+    rhs = ns.velocity.rhs_NavierStokes(d, S.metric, rho, VISC, ml)
+    su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    rhs.evaluate(su, sv, sw)
+    res = dict(shape=np.array([n, n, n]), spacing=np.array([S.geo.dx] * 3), u=u, v=v,
+               w=w, mu=mu, rho=rho,
+               rhs_ml=np.stack([rhs.rhs_u.numpy(), rhs.rhs_v.numpy(), rhs.rhs_w.numpy()]))
+    for k, t in ml.model.state_dict().items():
+        res["w_" + k] = t.detach().numpy().copy()
+    np.savez_compressed(os.path.join(out, "ml_16.npz"), **res)
+    print("ml: rhs max", np.abs(res["rhs_ml"]).max())
+
+
 def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005, stride=1):
     import torch
     ns = H.load_reference()
@@ -381,7 +413,7 @@ def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005, stride=1):
 
 if __name__ == "__main__":
     out = HERE
-    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run", "run64"]
+    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run", "run64", "ml"]
     if "ops" in which:
         ops_case(out)
     if "jacobi" in which:
@@ -392,6 +424,8 @@ if __name__ == "__main__":
         adjoint_case(out)
     if "run" in which:
         run_case(out)
+    if "ml" in which:
+        ml_case(out)
     if "run64" in which:
         # the 64^3 plain-DNS workload: seed 0, k0 = 4, nu = 0.01, dt = 0.005,
         # 20 RK4 steps, BiCGStab to 1e-10

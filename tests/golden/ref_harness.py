@@ -55,6 +55,7 @@ def load_reference():
     import domain
     import sfsmodel_smagorinsky
     import sfsmodel_gradient
+    import sfsmodel_ML
     import adjoint
     import PyFlow
 
@@ -82,7 +83,7 @@ def load_reference():
         metric_staggered=metric_staggered, state=state, velocity=velocity,
         pressure=pressure, advancer=advancer, domain=domain,
         sfsmodel_smagorinsky=sfsmodel_smagorinsky,
-        sfsmodel_gradient=sfsmodel_gradient, adjoint=adjoint, PyFlow=PyFlow,
+        sfsmodel_gradient=sfsmodel_gradient, sfsmodel_ML=sfsmodel_ML, adjoint=adjoint, PyFlow=PyFlow,
         tmp=tmp)
     _loaded["ns"] = ns
     return ns
