@@ -71,7 +71,49 @@ def project(vel, spacing, rho, dt, tol=1e-12, max_it=20000):
     return info
 
 
-def stage_states(state, spacing, mu, rho, dt, sfs=None, rk4=True):
+def source_fn(sfsmodel):
+    """The face sources of a 'source'-type SFS model as a function of the
+    staggered velocity (differentiable when grad mode is on), or None."""
+    if sfsmodel is None or getattr(sfsmodel, "modelType", None) != "source":
+        return None
+
+    def S(u, v, w):
+        sfsmodel.update(u, v, w, requires_grad=torch.is_grad_enabled())
+        return sfsmodel.face_sources()
+    return S
+
+
+def rhs_total(state, spacing, mu, rho, sfs=None, source=None):
+    """RHS of the velocity: pf_rhs_ns, minus the face sources of a 'source'
+    closure evaluated at this state (src/solver/velocity.py:360-383)."""
+    k = ops.rhs_ns(*state, spacing, mu, rho, sfs=sfs)
+    if source is not None:
+        with torch.no_grad():
+            fs = source(*state)
+        k = tuple(a - b for a, b in zip(k, fs))
+    return k
+
+
+def predictor(state, spacing, mu, rho, dt, sfs=None, source=None, rk4=True):
+    """RK4.step / Euler.step composed from RHS evaluations (the reference's
+    stage sequence with its stage-4 state u + dt/2 k3), for RHS terms the
+    fused predictor kernels do not have."""
+    u = tuple(state)
+    if not rk4:
+        k = rhs_total(u, spacing, mu, rho, sfs, source)
+        return tuple(a + b * dt for a, b in zip(u, k))
+    h = 0.5 * dt
+    ks, cur = [], u
+    for s in range(4):
+        k = rhs_total(cur, spacing, mu, rho, sfs, source)
+        ks.append(k)
+        if s < 3:
+            cur = tuple((h * kc + uc).contiguous() for kc, uc in zip(k, u))
+    return tuple(uc + dt / 6.0 * (((k1 + 2.0 * k2) + 2.0 * k3) + k4)
+                 for uc, k1, k2, k3, k4 in zip(u, *ks))
+
+
+def stage_states(state, spacing, mu, rho, dt, sfs=None, rk4=True, source=None):
     """The predictor's stage states (RK4: u1 = u, u_s = h k_{s-1} + u with
     h = dt/2 for s = 2, 3, 4; Euler: u1 only), recomputed from the step
     input."""
@@ -81,24 +123,37 @@ def stage_states(state, spacing, mu, rho, dt, sfs=None, rk4=True):
     h = 0.5 * dt
     cur = tuple(state)
     for _ in range(3):
-        k = ops.rhs_ns(*cur, spacing, mu, rho, sfs=sfs)
-        cur = tuple(h * kc + uc for kc, uc in zip(k, state))
+        k = rhs_total(cur, spacing, mu, rho, sfs, source)
+        cur = tuple((h * kc + uc).contiguous() for kc, uc in zip(k, state))
         stages.append(cur)
     return stages
 
 
+def _source_vjp(source, stage, kbar):
+    """-(dS/du)^T kbar at a stage state; accumulates -(dS/dtheta)^T kbar into
+    the closure's parameter gradients (the RHS carries -S)."""
+    with torch.enable_grad():
+        x = [t.detach().requires_grad_(True) for t in stage]
+        fs = source(*x)
+        torch.autograd.backward(fs, [-k for k in kbar])
+    return tuple(t.grad if t.grad is not None else torch.zeros_like(t) for t in x)
+
+
 def step_vjp(state, lam_out, spacing, mu, rho, dt, sfs=None, rk4=True,
-             tol=1e-12, max_it=20000):
-    """dL/du_n given dL/du_{n+1} (and dL/dF of the SFS stresses if sfs)."""
+             tol=1e-12, max_it=20000, source=None):
+    """dL/du_n given dL/du_{n+1} (and dL/dF of the SFS stresses if sfs; a
+    'source' closure's parameter gradients accumulate in its parameters)."""
     lam = tuple(t.clone() for t in lam_out)
     project(lam, spacing, rho, dt, tol, max_it)            # lam* = P lam
-    stages = stage_states(state, spacing, mu, rho, dt, sfs, rk4)
+    stages = stage_states(state, spacing, mu, rho, dt, sfs, rk4, source)
     lamF = torch.zeros((6,) + tuple(state[0].shape), dtype=torch.float64,
                        device=state[0].device) if sfs is not None else None
     total = [t.clone() for t in lam]
     if not rk4:
         kbar = tuple(dt * t for t in lam)
         m = rhs_adjoint(stages[0], kbar, spacing, mu, rho)
+        if source is not None:
+            m = tuple(a + b for a, b in zip(m, _source_vjp(source, stages[0], kbar)))
         if lamF is not None:
             sfs_adjoint_accumulate(kbar, spacing, 1.0, lamF)
         return tuple(a + b for a, b in zip(total, m)), lamF
@@ -110,6 +165,8 @@ def step_vjp(state, lam_out, spacing, mu, rho, dt, sfs=None, rk4=True,
         if m_next is not None:
             kbar = tuple(a + h * b for a, b in zip(kbar, m_next))
         m = rhs_adjoint(stages[s], kbar, spacing, mu, rho)
+        if source is not None:
+            m = tuple(a + b for a, b in zip(m, _source_vjp(source, stages[s], kbar)))
         if lamF is not None:
             sfs_adjoint_accumulate(kbar, spacing, 1.0, lamF)
         total = [a + b for a, b in zip(total, m)]
@@ -125,17 +182,25 @@ class ForwardStep(torch.autograd.Function):
     input.  ``sfs`` (6, nx, ny, nz) stresses, if given, are an input too."""
 
     @staticmethod
-    def forward(ctx, u, v, w, sfs, spacing, mu, rho, dt, rk4, tol, max_it):
+    def forward(ctx, u, v, w, sfs, spacing, mu, rho, dt, rk4, tol, max_it, source=None):
         if sfs is not None:
             sfs = sfs.contiguous()
         ctx.save_for_backward(u, v, w, sfs if sfs is not None else torch.empty(0))
         ctx.cfg = (spacing, mu, rho, dt, rk4, tol, max_it, sfs is not None)
+        ctx.source = source
+        sd = sfs.detach().contiguous() if sfs is not None else None
+        if source is not None:
+            # per-stage source closure: composed stages, then the projection
+            uo, vo, wo = predictor((u.detach(), v.detach(), w.detach()), spacing, mu, rho,
+                                   dt, sd, source, rk4)
+            uo, vo, wo = uo.contiguous(), vo.contiguous(), wo.contiguous()
+            project((uo, vo, wo), spacing, rho, dt, tol, max_it)
+            return uo, vo, wo
         uo, vo, wo = u.detach().clone(), v.detach().clone(), w.detach().clone()
         p = torch.zeros_like(uo)
         DP = torch.zeros_like(uo)
         ops.forward_step(uo, vo, wo, p, DP, spacing, mu, rho, dt, rk4=rk4,
-                         min_res=tol, max_it=max_it,
-                         sfs=sfs.detach().contiguous() if sfs is not None else None)
+                         min_res=tol, max_it=max_it, sfs=sd)
         return uo, vo, wo
 
     @staticmethod
@@ -147,23 +212,99 @@ class ForwardStep(torch.autograd.Function):
         (lu, lv, lw), lamF = step_vjp((u.detach(), v.detach(), w.detach()), lam,
                                       spacing, mu, rho, dt,
                                       sfs=sfs.detach() if has_sfs else None,
-                                      rk4=rk4, tol=tol, max_it=max_it)
-        return lu, lv, lw, lamF, None, None, None, None, None, None, None
+                                      rk4=rk4, tol=tol, max_it=max_it, source=ctx.source)
+        return lu, lv, lw, lamF, None, None, None, None, None, None, None, None
 
 
 def forward_step(u, v, w, spacing, mu, rho, dt, sfs=None, rk4=True, tol=1e-12,
-                 max_it=20000):
+                 max_it=20000, source=None):
+    """One differentiable step; ``source`` is a 'source'-closure function
+    (source_fn), whose parameter gradients accumulate during backward."""
     return ForwardStep.apply(u, v, w, sfs, tuple(spacing), float(mu), float(rho),
-                             float(dt), bool(rk4), float(tol), int(max_it))
+                             float(dt), bool(rk4), float(tol), int(max_it), source)
+
+
+def _stats_row(it, t, dt, u, v, w, spacing, mu, rho):
+    n = u.numel()
+    mx = [float(a.abs().max()) for a in (u, v, w)]
+    cfl = max(mx[0] / spacing[0], mx[1] / spacing[1], mx[2] / spacing[2]) * dt
+    nu = mu / rho
+    cfl = max(cfl, max(nu / h ** 2 for h in spacing) * dt)
+    tke = float((u * u + v * v + w * w).sum()) / n * 0.5
+    div = float(ops.div_vel(u, v, w, spacing).abs().max())
+    return (it, t, cfl, mx[0], mx[1], mx[2], tke, div)
 
 
 def run_training(inputConfig, comms, decomp, geometry, metric, D, startTime):
-    """adjointTraining mode of PyFlow.run (src/core/PyFlow.py:312-607):
-    numIt steps in windows of numCheckpointIt, each window's objective the
-    mean absolute error of the velocity against a target restart file (or
-    mean(u^2) in adjointVerification mode), differentiated through the
-    hand-written adjoint; returns (objective, gradient at the perturbed cell)
-    in verification mode like the reference (src/core/PyFlow.py:660-663)."""
-    raise NotImplementedError(
-        "adjointTraining through PyFlow.run: use pyflow_b200.adjoint.forward_step "
-        "windows (see tests/test_gpu_adjoint.py)")
+    """adjointTraining mode of PyFlow.run (src/core/PyFlow.py:312-607).
+
+    numIt steps in windows of numCheckpointIt.  Each window runs forward with
+    one checkpoint per step (differentiable steps: pf_forward_step, or the
+    composed stages when a 'source' closure is active), then its objective is
+    differentiated through the hand-written adjoint:
+      * adjointVerification: objective mean(u^2) after the window, with
+        ``perturbation`` added to u at the centre cell before the run; returns
+        (objective, dL/du at that cell) like the reference (:475-483, 660-663);
+      * otherwise: the mean absolute error of u, v, w against the target
+        restart file inputConfig.getTargetFileName(startFileIt + itCount)
+        (adjoint initial condition sign(u - u_T) / numPoints, :486-533),
+        optionally after projecting the target (targetDataVelCorr,
+        src/data/domain.py:445-468); the 'source' closure's parameter
+        gradients then go to its finalize (gradient averaging, RMSprop,
+        learning-rate schedule) and save.
+    Constant viscosity; the SFS model, if any, must be 'source'-type or
+    none.  Returns None outside verification mode, like the reference."""
+    from . import dataReader as dr
+    simDt = float(inputConfig.simDt)
+    win = int(getattr(inputConfig, "numCheckpointIt", 0) or 0)
+    if win <= 0:
+        raise Exception("Adjoint training requires specification of numCheckpointIt")
+    verification = bool(getattr(inputConfig, "adjointVerification", False))
+    sp, mu, rho = tuple(D.spacing), float(D.mu), float(D.rho)
+    if D.use_SFSmodel and D.sfsmodel.modelType != "source":
+        raise ValueError("adjoint training supports the 'source' ML closure or no SFS model")
+    model = D.sfsmodel if D.use_SFSmodel else None
+    source = source_fn(model)
+    rk4 = D.advancerName == "RK4"
+    tol = float(getattr(inputConfig, "min_pressure_residual", 1e-12))
+    max_it = int(getattr(inputConfig, "max_pressure_iterations", 20000))
+    state = [s.interior() for s in (D.state_u_P, D.state_v_P, D.state_w_P)]
+    n = state[0].numel()
+    nn = state[0].shape[0] // 2
+    if verification:
+        state[0][nn, nn, nn] += float(inputConfig.perturbation)
+    history, result = [], None
+    it, t = 0, float(startTime)
+    for _ in range(int(inputConfig.numIt) // win):
+        # the velocity carries the graph (the closure's parameters enter
+        # through the steps' backward)
+        u0 = [x.detach().clone().requires_grad_(True) for x in state]
+        cur = tuple(u0)
+        for _ in range(win):
+            cur = forward_step(*cur, sp, mu, rho, simDt, rk4=rk4, tol=tol, max_it=max_it,
+                               source=source)
+            it += 1
+            t += simDt
+            history.append(_stats_row(it, t, simDt, *(c.detach() for c in cur), sp, mu, rho))
+        if verification:
+            L = torch.mean(cur[0] ** 2)
+            L.backward()
+            result = (float(L.detach()), float(u0[0].grad[nn, nn, nn]))
+        else:
+            fname = inputConfig.getTargetFileName(inputConfig.startFileIt + it)
+            _, _, data = dr.readNGArestart(fname, headerOnly=False)
+            tgt = [torch.tensor(data[..., c], dtype=torch.float64, device=state[0].device)
+                   for c in range(3)]
+            if getattr(inputConfig, "targetDataVelCorr", False):
+                project(tgt, sp, rho, simDt, tol, max_it)
+            L = sum(torch.sum(torch.abs(c - g)) for c, g in zip(cur, tgt)) / n
+            L.backward()
+            if model is not None:
+                model.finalize(comms)
+                if getattr(model, "saveModel", False):
+                    model.save()
+            history[-1] = history[-1] + (float(L.detach()),)
+        for x, c in zip(state, cur):
+            x.copy_(c.detach())
+    run_training.last_history = history
+    return result

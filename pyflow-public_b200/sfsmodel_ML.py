@@ -87,11 +87,11 @@ def _derivatives(a, dx):
     return d1, d2
 
 
-def features(u, v, w, dx):
-    """The 21 cell-centred FP32 features, shape (nx, ny, nz, 21), in the
-    reference's order: u, v, w, u_x, u_y, u_z, v_x, ..., w_z, u_xx, u_yy,
-    u_zz, v_xx, ..., w_zz."""
-    uc, vc, wc = (t.to(torch.float32) for t in _centred(u, v, w))
+def features(u, v, w, dx, dtype=torch.float32):
+    """The 21 cell-centred features (FP32 like the reference), shape
+    (nx, ny, nz, 21), in the reference's order: u, v, w, u_x, u_y, u_z, v_x,
+    ..., w_z, u_xx, u_yy, u_zz, v_xx, ..., w_zz."""
+    uc, vc, wc = (t.to(dtype) for t in _centred(u, v, w))
     first, second = [], []
     for a in (uc, vc, wc):
         d1, d2 = _derivatives(a, dx)
@@ -138,19 +138,40 @@ class residual_stress:
         self.model = (model if model is not None else GatedClosureNet()).to(self.device)
         self.epoch = 0
         self.LR = 0.01
+        self.optimizer = torch.optim.RMSprop(self.model.parameters(), lr=self.LR)
+        self.outParamsList, self.sumParamsList = [], []
         if getattr(inputConfig, "loadModel", False):
             ck = torch.load(inputConfig.modelDictName, map_location=self.device)
             self.epoch = ck.get("epoch", 0)
-            self.LR = ck.get("LR", self.LR)
             self.model.load_state_dict(ck["model_state_dict"])
-        self.norm = torch.tensor(NORM, dtype=torch.float32, device=self.device)
+            if "optimizer_state_dict" in ck:
+                self.optimizer.load_state_dict(ck["optimizer_state_dict"])
+            self.LR = ck.get("LR", self.LR)
+            self.outParamsList = list(ck.get("outParamsList", []))
+            self.sumParamsList = list(ck.get("sumParamsList", []))
+        if hasattr(inputConfig, "LR"):
+            self.LR = inputConfig.LR
+            for g in self.optimizer.param_groups:
+                g["lr"] = self.LR
+        # training settings (src/sfsmodel/sfsmodel_ML.py:219-243)
+        self.saveModel = hasattr(inputConfig, "modelDictSave")
+        self.modelDictSave = getattr(inputConfig, "modelDictSave", None)
+        self.LR_decay = int(getattr(inputConfig, "LR_decay", 2500))
+        self.numSumDistr = int(getattr(inputConfig, "numSumDistr", 8))
+        self.optimizer.zero_grad()
+        # evaluation precision: FP32 like the reference; 'float64' (config key
+        # mlDtype) evaluates features and network in FP64
+        self.dtype = torch.float64 if getattr(inputConfig, "mlDtype", "float32") == "float64" \
+            else torch.float32
+        self.model.to(self.dtype)
+        self.norm = torch.tensor(NORM, dtype=self.dtype, device=self.device)
         self.GX = self.GY = self.GZ = None
 
     def update(self, u, v, w, requires_grad=False):
         """Closure terms at cell centres from the staggered velocity (FP64
         interiors); stored as FP64 like the reference (:370-380)."""
         with torch.set_grad_enabled(requires_grad):
-            F = features(u, v, w, self.dx)
+            F = features(u, v, w, self.dx, self.dtype)
             x = network_input(F, self.norm)
             p = self.model(x)
             gx, gy, gz = closure_terms(p, self.dx)
@@ -165,9 +186,46 @@ class residual_stress:
                 0.5 * (self.GY + torch.roll(self.GY, 1, 1)),
                 0.5 * (self.GZ + torch.roll(self.GZ, 1, 2)))
 
-    def save(self, path):
+    def save(self, path=None):
+        """Checkpoint in the reference's format (src/sfsmodel/sfsmodel_ML.py:280-291)."""
+        path = path or self.modelDictSave
         torch.save({"epoch": self.epoch, "LR": self.LR,
-                    "model_state_dict": self.model.state_dict()}, path)
+                    "model_state_dict": self.model.state_dict(),
+                    "optimizer_state_dict": self.optimizer.state_dict(),
+                    "outParamsList": self.outParamsList,
+                    "sumParamsList": self.sumParamsList}, path)
 
     def finalize(self, comms=None):
-        pass
+        """One training update after an adjoint window, with the reference's
+        schedule (src/sfsmodel/sfsmodel_ML.py:296-349): the parameter
+        gradients are accumulated over numSumDistr windows and their average
+        (summed over ranks) is applied at every window until the next
+        average exists; RMSprop step; the learning rate halves every LR_decay
+        windows once 4/5 of LR_decay have passed.  The gradients held by the
+        parameters are already dL/dtheta (the reference's accumulation needs
+        a factor -dt to become that; the hand-written adjoint here does not)."""
+        params = list(self.model.parameters())
+        grads = [p.grad.detach().clone() if p.grad is not None else torch.zeros_like(p)
+                 for p in params]
+        if self.epoch == 0 or not self.sumParamsList:
+            self.outParamsList = [torch.zeros_like(g) for g in grads]
+            self.sumParamsList = [torch.zeros_like(g) for g in grads]
+        for s, g in zip(self.sumParamsList, grads):
+            s.add_(g)
+        if (self.epoch + 1) % self.numSumDistr == 0:
+            size = getattr(comms, "size", 1) if comms is not None else 1
+            for i, s in enumerate(self.sumParamsList):
+                tot = s
+                if comms is not None and size > 1:
+                    tot = torch.as_tensor(comms.parallel_sum(s.cpu().numpy()), device=s.device)
+                self.outParamsList[i] = tot / float(self.numSumDistr * size)
+                self.sumParamsList[i] = torch.zeros_like(s)
+        for p, a in zip(params, self.outParamsList):
+            p.grad = a.clone().to(p.dtype)
+        self.optimizer.step()
+        self.optimizer.zero_grad()
+        self.epoch += 1
+        if self.epoch >= 4 * self.LR_decay // 5 and self.epoch % self.LR_decay == 0:
+            self.LR *= 0.5
+            for g in self.optimizer.param_groups:
+                g["lr"] = 0.5 * g["lr"]
