@@ -162,6 +162,7 @@ template <class Src>
 __global__ void __launch_bounds__(kBlock, 2)
 mg_smooth0(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc,
            PhaseSmooth0<Src> ph) {
+    pdl_wait();
     if (sc->done) return;
     ph.src.setup(sc);
     sweep<float>(d, tl, cf, ph);
@@ -169,6 +170,7 @@ mg_smooth0(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc,
 
 __global__ void __launch_bounds__(kBlock, 2)
 mg_smooth(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, PhaseSmooth ph) {
+    pdl_wait();
     if (sc->done) return;
     sweep<float>(d, tl, cf, ph);
 }
@@ -178,6 +180,7 @@ __global__ void __launch_bounds__(256)
 mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
             const float* __restrict__ x, Dims c, float* __restrict__ bc,
             const BicgScalars* sc) {
+    pdl_wait();
     if (sc->done) return;
     const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y;
     const int I = blockIdx.z;
@@ -270,6 +273,7 @@ __device__ __forceinline__ float prolong_at(const float* __restrict__ xc, const 
 __global__ void __launch_bounds__(256)
 mg_smooth0_pw(Dims d, LapCoef<float> cf, float wd, const float* __restrict__ b,
               float* __restrict__ x, const BicgScalars* sc) {
+    pdl_wait();
     if (sc->done) return;
     PF_CELL_IDX(d);
     const float bc = b[q];
@@ -280,6 +284,7 @@ mg_smooth0_pw(Dims d, LapCoef<float> cf, float wd, const float* __restrict__ b,
 __global__ void __launch_bounds__(256)
 mg_smooth_pw(Dims d, LapCoef<float> cf, float wd, const float* __restrict__ x,
              const float* __restrict__ b, float* __restrict__ out, const BicgScalars* sc) {
+    pdl_wait();
     if (sc->done) return;
     PF_CELL_IDX(d);
     const float xc = x[q];
@@ -292,6 +297,7 @@ mg_prolong_smooth_pw(Dims d, Dims c, LapCoef<float> cf, float wd,
                      const float* __restrict__ xc, const float* __restrict__ x,
                      const float* __restrict__ b, float* __restrict__ out,
                      const BicgScalars* sc) {
+    pdl_wait();
     if (sc->done) return;
     PF_CELL_IDX(d);
     auto y = [&](int a, int bb, int cc) {
@@ -320,6 +326,7 @@ mg_prolong_smooth_pw(Dims d, Dims c, LapCoef<float> cf, float wd,
 __global__ void __launch_bounds__(256)
 mg_prolong_add(Dims f, Dims c, const float* __restrict__ xc, float* __restrict__ x,
                const BicgScalars* sc) {
+    pdl_wait();
     if (sc->done) return;
     const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y;
     const int I = blockIdx.z;
@@ -382,26 +389,48 @@ constexpr int kMgPinvMax = 64;  // largest coarsest level solved with a pseudo-i
 // Symmetric; applying it also removes the mean of the right-hand side.
 __global__ void __launch_bounds__(256)
 mg_coarse_pinv(Dims d, double cx, double cy, double cz, float* __restrict__ out) {
+    pdl_wait();
+    // A^+ is circulant: A^+[p][r] depends on (p - r) mod n only.  The block
+    // tabulates 1/lambda(k), then 4 threads per difference vector sum its
+    // Fourier series over interleaved k (fixed order), and the matrix is
+    // filled from the N values.
+    __shared__ double ilam[kMgPinvMax];
+    __shared__ double part[kMgPinvMax][4];
+    __shared__ double tab[kMgPinvMax];
     const int N = (int)d.n;
     const double tp = 6.283185307179586;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N * N; e += gridDim.x * blockDim.x) {
-        const int p = e / N, r = e - p * N;
-        const int pz = p % d.nz, py = (p / d.nz) % d.ny, px = p / (d.ny * d.nz);
-        const int rz = r % d.nz, ry = (r / d.nz) % d.ny, rx = r / (d.ny * d.nz);
+    const int nyz = d.ny * d.nz;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        const int kz = k % d.nz, ky = (k / d.nz) % d.ny, kx = k / nyz;
+        const double lam = cx * (2.0 - 2.0 * cos(tp * kx / d.nx)) +
+                           cy * (2.0 - 2.0 * cos(tp * ky / d.ny)) +
+                           cz * (2.0 - 2.0 * cos(tp * kz / d.nz));
+        ilam[k] = k == 0 ? 0.0 : 1.0 / lam;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 4 * N; t += blockDim.x) {
+        const int q = t >> 2, lane = t & 3;
+        const int dz = q % d.nz, dy = (q / d.nz) % d.ny, dx = q / nyz;
         double acc = 0.0;
-        for (int kx = 0; kx < d.nx; ++kx)
-            for (int ky = 0; ky < d.ny; ++ky)
-                for (int kz = 0; kz < d.nz; ++kz) {
-                    if (kx == 0 && ky == 0 && kz == 0) continue;
-                    const double lam = cx * (2.0 - 2.0 * cos(tp * kx / d.nx)) +
-                                       cy * (2.0 - 2.0 * cos(tp * ky / d.ny)) +
-                                       cz * (2.0 - 2.0 * cos(tp * kz / d.nz));
-                    const double ph = tp * (double(kx * (px - rx)) / d.nx +
-                                            double(ky * (py - ry)) / d.ny +
-                                            double(kz * (pz - rz)) / d.nz);
-                    acc += cos(ph) / lam;
-                }
-        out[e] = float(acc / double(N));
+        for (int k = 1 + lane; k < N; k += 4) {
+            const int kz = k % d.nz, ky = (k / d.nz) % d.ny, kx = k / nyz;
+            const double ph = tp * (double(kx * dx) / d.nx + double(ky * dy) / d.ny +
+                                    double(kz * dz) / d.nz);
+            acc += cos(ph) * ilam[k];
+        }
+        part[q][lane] = acc;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < N; q += blockDim.x)
+        tab[q] = (((part[q][0] + part[q][1]) + part[q][2]) + part[q][3]) / double(N);
+    __syncthreads();
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+        const int p = e / N, r = e - p * N;
+        const int pz = p % d.nz, py = (p / d.nz) % d.ny, px = p / nyz;
+        const int rz = r % d.nz, ry = (r / d.nz) % d.ny, rx = r / nyz;
+        const int q = ((px - rx + d.nx) % d.nx * d.ny + (py - ry + d.ny) % d.ny) * d.nz +
+                      (pz - rz + d.nz) % d.nz;
+        out[e] = float(tab[q]);
     }
 }
 
@@ -436,6 +465,7 @@ __device__ __forceinline__ void decode(int q, const Dims& d, float inv_p, float 
 __global__ void __launch_bounds__(kBottomThreads)
 mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
           const BicgScalars* sc) {
+    pdl_wait();
     if (sc->done) return;
     extern __shared__ float sm[];
     __shared__ double shd[32];
@@ -597,6 +627,7 @@ __global__ void __launch_bounds__(kBlock, 2)
 mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
       const float* ph, const float* res0, float* v, int use_cond,
       cudaGraphConditionalHandle cond) {
+    pdl_wait();
     __shared__ double sh[32];
     if (sc->done) return;
     PhaseAv p{ph, res0, v, 0.0};
@@ -624,6 +655,7 @@ mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
 __global__ void __launch_bounds__(kBlock, 2)
 mg_at(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
       const float* shv, const float* s, float* t) {
+    pdl_wait();
     __shared__ double sh[32];
     if (sc->done) return;
     PhaseAt p{shv, s, t, 0.0, 0.0};
@@ -648,6 +680,7 @@ __global__ void __launch_bounds__(kBlock)
 mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
           const float* shv, const float* s, const float* t, float* res,
           const float* res0, int use_cond, cudaGraphConditionalHandle cond) {
+    pdl_wait();
     __shared__ double sh[32];
     if (sc->done) {
         if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0);
@@ -655,14 +688,38 @@ mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
     }
     const float alpha = float(sc->alpha), omega = float(sc->omega);
     double dot = 0.0, mx = 0.0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
-         q += (long long)gridDim.x * blockDim.x) {
-        float x = fmaf(alpha, ph[q], e[q]);
-        e[q] = fmaf(omega, shv[q], x);
-        const float r = fmaf(-omega, t[q], s[q]);
-        res[q] = r;
-        dot += double(r) * double(res0[q]);
-        mx = nanmax(mx, fabs(double(r)));
+    auto cell = [&](float& ev, float phv, float shq, float sv, float tv, float r0, float& rv) {
+        const float x = fmaf(alpha, phv, ev);
+        ev = fmaf(omega, shq, x);
+        rv = fmaf(-omega, tv, sv);
+        dot += double(rv) * double(r0);
+        mx = nanmax(mx, fabs(double(rv)));
+    };
+    // four cells per thread with 16-byte accesses (all vectors are 256-byte
+    // aligned), then the tail
+    const long long n4 = d.n >> 2;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+        float4 ev = reinterpret_cast<const float4*>(e)[i];
+        const float4 pv = reinterpret_cast<const float4*>(ph)[i];
+        const float4 hv = reinterpret_cast<const float4*>(shv)[i];
+        const float4 sv = reinterpret_cast<const float4*>(s)[i];
+        const float4 tv = reinterpret_cast<const float4*>(t)[i];
+        const float4 zv = reinterpret_cast<const float4*>(res0)[i];
+        float4 rv;
+        cell(ev.x, pv.x, hv.x, sv.x, tv.x, zv.x, rv.x);
+        cell(ev.y, pv.y, hv.y, sv.y, tv.y, zv.y, rv.y);
+        cell(ev.z, pv.z, hv.z, sv.z, tv.z, zv.z, rv.z);
+        cell(ev.w, pv.w, hv.w, sv.w, tv.w, zv.w, rv.w);
+        reinterpret_cast<float4*>(e)[i] = ev;
+        reinterpret_cast<float4*>(res)[i] = rv;
+    }
+    for (long long q = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
+         q += stride) {
+        float ev = e[q], rv;
+        cell(ev, ph[q], shv[q], s[q], t[q], res0[q], rv);
+        e[q] = ev;
+        res[q] = rv;
     }
     const double bs = block_sum<kBlock>(dot, sh);
     const double bm = block_max<kBlock>(mx, sh);
@@ -696,6 +753,7 @@ __global__ void __launch_bounds__(kBlock)
 mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
         float* res, float* res0, float* e, float* p0, float* p1, float* v,
         int max_it, double tol, double outer_tol) {
+    pdl_wait();
     __shared__ double sh[32];
     const double inv = sc->scale > 0.0 ? 1.0 / sc->scale : 0.0;
     double s = 0.0, m = 0.0;
@@ -822,20 +880,20 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
             if (f.kind == kMgSwept) {
                 PhaseSmooth0<SrcPlain> ph{};
                 ph.src.b = f.b; ph.x = f.x; ph.wd = f.wd;
-                PF_LAUNCH("mg_smooth0", s, mg_smooth0<SrcPlain><<<tiled_grid(f.tl8), blk, 0, s>>>(
+                PF_LAUNCH("mg_smooth0", s, launch_pdl(mg_smooth0<SrcPlain>, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s,
                     f.d, f.tl8, f.cf, sc, ph));
             } else {
-                PF_LAUNCH("mg_smooth0_pw", s, mg_smooth0_pw<<<cgrid3(f.d), blk, 0, s>>>(
+                PF_LAUNCH("mg_smooth0_pw", s, launch_pdl(mg_smooth0_pw, dim3(cgrid3(f.d)), dim3(blk), 0, s,
                     f.d, f.cf, f.wd, f.b, f.x, sc));
             }
         }
-        PF_LAUNCH(l == 0 ? "mg_restrict_l0" : "mg_restrict", s, mg_restrict<<<cgrid3(c.d), blk, 0, s>>>(
+        PF_LAUNCH(l == 0 ? "mg_restrict_l0" : "mg_restrict", s, launch_pdl(mg_restrict, dim3(cgrid3(c.d)), dim3(blk), 0, s,
             f.d, f.cf, bl, xl, c.d, c.b, sc));
     }
     {
         const MgBottom m = bottom_params(P);
         const size_t smem = bottom_smem_floats(P) * sizeof(float);
-        PF_LAUNCH("mg_bottom", s, mg_bottom<<<1, kBottomThreads, smem, s>>>(
+        PF_LAUNCH("mg_bottom", s, launch_pdl(mg_bottom, dim3(1), dim3(kBottomThreads), smem, s,
             m, P.lv[P.B].b, P.lv[P.B].x, sc));
     }
     for (int l = P.B - 1; l >= 0; --l) {
@@ -846,15 +904,15 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
         if (f.kind == kMgSwept) {
             const char* np = l == 0 ? "mg_prolong_l0" : "mg_prolong";
             const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
-            PF_LAUNCH(np, s, mg_prolong_add<<<cgrid3(c.d), blk, 0, s>>>(f.d, c.d, c.x, xl, sc));
+            PF_LAUNCH(np, s, launch_pdl(mg_prolong_add, dim3(cgrid3(c.d)), dim3(blk), 0, s, f.d, c.d, c.x, xl, sc));
             PhaseSmooth a{xl, bl, f.t, f.wd};
-            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl8), blk, 0, s>>>(f.d, f.tl8, f.cf, sc, a));
+            PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, a));
             PhaseSmooth b{f.t, bl, xl, f.wd};
-            PF_LAUNCH(ns, s, mg_smooth<<<tiled_grid(f.tl8), blk, 0, s>>>(f.d, f.tl8, f.cf, sc, b));
+            PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, b));
         } else {
-            PF_LAUNCH("mg_prolong_smooth_pw", s, mg_prolong_smooth_pw<<<cgrid3(f.d), blk, 0, s>>>(
+            PF_LAUNCH("mg_prolong_smooth_pw", s, launch_pdl(mg_prolong_smooth_pw, dim3(cgrid3(f.d)), dim3(blk), 0, s,
                 f.d, c.d, f.cf, f.wd, c.x, xl, bl, f.t, sc));
-            PF_LAUNCH("mg_smooth_pw", s, mg_smooth_pw<<<cgrid3(f.d), blk, 0, s>>>(
+            PF_LAUNCH("mg_smooth_pw", s, launch_pdl(mg_smooth_pw, dim3(cgrid3(f.d)), dim3(blk), 0, s,
                 f.d, f.cf, f.wd, f.t, bl, xl, sc));
         }
     }
@@ -863,8 +921,7 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
 int mg_enqueue_setup(const MgPlan& P, cudaStream_t s) {
     if (P.pinv) {
         const MgLevel& c = P.lv[P.L - 1];
-        const int ne = (int)(c.d.n * c.d.n);
-        PF_LAUNCH("mg_coarse_pinv", s, mg_coarse_pinv<<<(ne + 255) / 256, 256, 0, s>>>(
+        PF_LAUNCH("mg_coarse_pinv", s, launch_pdl(mg_coarse_pinv, dim3(1), dim3(256), 0, s,
             c.d, c.cq[0], c.cq[1], c.cq[2], P.pinv));
     }
     return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;
@@ -873,7 +930,7 @@ int mg_enqueue_setup(const MgPlan& P, cudaStream_t s) {
 int mg_enqueue_init(const MgPlan& P, BicgScalars* sc, double* part, const double* rhs,
                     double tol, int max_it, cudaStream_t s, double outer_tol) {
     const Dims& d = P.lv[0].d;
-    PF_LAUNCH("mg_init", s, mg_init<<<pointwise_grid(d.n), kBlock, 0, s>>>(
+    PF_LAUNCH("mg_init", s, launch_pdl(mg_init, dim3(pointwise_grid(d.n)), dim3(kBlock), 0, s,
         d, sc, part, rhs, P.res, P.res0, P.e, P.p[0], P.p[1], P.v, max_it, tol, outer_tol));
     return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;
 }
@@ -889,20 +946,20 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
         PhaseSmooth0<SrcP> ph{};
         ph.src.res = P.res; ph.src.p_old = p_old; ph.src.v = P.v; ph.src.p_new = p_new;
         ph.x = P.ph; ph.wd = f.wd;
-        PF_LAUNCH("mg_smooth0_p", s, mg_smooth0<SrcP><<<gt, blk, 0, s>>>(f.d, f.tl, f.cf, sc, ph));
+        PF_LAUNCH("mg_smooth0_p", s, launch_pdl(mg_smooth0<SrcP>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, p_new, P.ph, sc, s);
-    PF_LAUNCH("mg_av", s, mg_av<<<gt8, blk, 0, s>>>(f.d, f.tl8, f.cf, sc, part, P.ph, P.res0,
+    PF_LAUNCH("mg_av", s, launch_pdl(mg_av, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, part, P.ph, P.res0,
                                                    P.v, use_cond, cond));
     {   // s = res - alpha v fused into the first smoothing pass of M s
         PhaseSmooth0<SrcS> ph{};
         ph.src.res = P.res; ph.src.v = P.v; ph.src.s = P.s;
         ph.x = P.sh; ph.wd = f.wd;
-        PF_LAUNCH("mg_smooth0_s", s, mg_smooth0<SrcS><<<gt, blk, 0, s>>>(f.d, f.tl, f.cf, sc, ph));
+        PF_LAUNCH("mg_smooth0_s", s, launch_pdl(mg_smooth0<SrcS>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, P.s, P.sh, sc, s);
-    PF_LAUNCH("mg_at", s, mg_at<<<gt8, blk, 0, s>>>(f.d, f.tl8, f.cf, sc, part, P.sh, P.s, P.t));
-    PF_LAUNCH("mg_update", s, mg_update<<<pointwise_grid(f.d.n), kBlock, 0, s>>>(
+    PF_LAUNCH("mg_at", s, launch_pdl(mg_at, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, part, P.sh, P.s, P.t));
+    PF_LAUNCH("mg_update", s, launch_pdl(mg_update, dim3(pointwise_grid(f.d.n)), dim3(kBlock), 0, s,
         f.d, sc, part, P.e, P.ph, P.sh, P.s, P.t, P.res, P.res0, use_cond, cond));
     return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;
 }
@@ -911,7 +968,10 @@ int mg_inner_solve(const MgPlan& P, BicgScalars* sc, double* part, const double*
                    double tol, int max_it, cudaStream_t s, BicgScalars* hs, double outer_tol) {
     int rc = mg_enqueue_init(P, sc, part, rhs, tol, std::max(1, max_it), s, outer_tol);
     if (rc) return rc;
-    int k = 0, chunk = 2;
+    // with per-kernel timing on, poll after every iteration so no launch of
+    // a finished solve (which returns at once) enters the kernel averages
+    const bool exact = prof_on();
+    int k = 0, chunk = exact ? 1 : 2;
     for (int guard = 0; guard < (1 << 20); ++guard) {
         for (int c = 0; c < chunk; ++c, ++k) {
             rc = mg_enqueue_iteration(P, sc, part, k, s);
@@ -921,7 +981,7 @@ int mg_inner_solve(const MgPlan& P, BicgScalars* sc, double* part, const double*
             return PF_ERR_CUDA;
         if (cudaStreamSynchronize(s) != cudaSuccess) return PF_ERR_CUDA;
         if (hs->done) return PF_OK;
-        chunk = std::min(chunk * 2, 8);
+        chunk = exact ? 1 : std::min(chunk * 2, 8);
     }
     return PF_ERR_CUDA;
 }

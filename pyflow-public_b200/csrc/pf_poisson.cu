@@ -413,7 +413,10 @@ static int run_iterations(const Dims& d, const LapCoef<T>& cf,
     const char* nca = sizeof(T) == 8 ? "bicg_ca_f64" : "bicg_ca_f32";
     const char* nb = sizeof(T) == 8 ? "bicg_b_f64" : "bicg_b_f32";
     PF_LAUNCH(nca, s, bicg_ca<T><<<ga, blk2, 0, s>>>(d, ta, cf, sc, part, v, x));
-    int chunk = 4;
+    // with per-kernel timing on, poll after every iteration so no launch of
+    // a finished solve (which returns at once) enters the kernel averages
+    const bool exact = prof_on();
+    int chunk = exact ? 1 : 4;
     for (int guard = 0; guard < (1 << 20); ++guard) {
         for (int c = 0; c < chunk; ++c) {
             PF_LAUNCH(nb, s, bicg_b<T><<<gb, blk2, 0, s>>>(d, tb, cf, sc, part, v));
@@ -423,7 +426,7 @@ static int run_iterations(const Dims& d, const LapCoef<T>& cf,
         const int rc = read_scalars(sc, hs, s);
         if (rc) return rc;
         if (hs->done == 1) return PF_OK;
-        chunk = std::min(chunk * 2, 32);
+        chunk = exact ? 1 : std::min(chunk * 2, 32);
     }
     return PF_ERR_CUDA;
 }

@@ -253,4 +253,29 @@ __device__ __forceinline__ bool tid0() { return threadIdx.x == 0 && threadIdx.y 
 
 static inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Programmatic dependent launch: the kernel may be launched while its
+// predecessor in the stream is still finishing (launch latency and the
+// predecessor's tail overlap); it must call pdl_wait() before touching any
+// memory, which blocks until the predecessor has completed and its writes
+// are visible.  Without the launch attribute pdl_wait() is a no-op.
+__device__ __forceinline__ void pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                                     size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 }  // namespace pf
