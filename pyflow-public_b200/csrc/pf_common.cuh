@@ -33,6 +33,12 @@ __host__ __device__ inline int wrap(int a, int n) {
     return a < 0 ? a + n : (a >= n ? a - n : a);
 }
 
+// full periodic wrap (any distance)
+__host__ __device__ inline int pmod(int a, int n) {
+    const int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
 __host__ __device__ inline long long idx(const Dims& d, int i, int j, int k) {
     return ((long long)i * d.ny + j) * d.nz + k;
 }

@@ -157,6 +157,58 @@ struct PhaseAt {
     }
 };
 
+// The same phases for sweep_async (FP32 grids with nz a multiple of 32).
+struct AsyncSmooth0 {  // x = w (2 b - w A b)
+    static constexpr int NE = 0;
+    const float* rf[1];
+    const float* ef[1];
+    float* x;
+    float wd;
+    __device__ float op(float r) const { return r; }
+    __device__ void epi(long long q, float c, float ab, float, const float*) {
+        x[q] = wd * (2.0f * c - wd * ab);
+    }
+};
+
+struct AsyncSmooth {  // out = x + w (b - A x)
+    static constexpr int NE = 1;
+    const float* rf[1];
+    const float* ef[1];
+    float* out;
+    float wd;
+    __device__ float op(float r) const { return r; }
+    __device__ void epi(long long q, float c, float ax, float, const float* e) {
+        out[q] = fmaf(wd, e[0] - ax, c);
+    }
+};
+
+struct AsyncAv {  // v = A ph, (v, res0)
+    static constexpr int NE = 1;
+    const float* rf[1];
+    const float* ef[1];
+    float* v;
+    double dot;
+    __device__ float op(float r) const { return r; }
+    __device__ void epi(long long q, float, float ax, float, const float* e) {
+        v[q] = ax;
+        dot += double(ax) * double(e[0]);
+    }
+};
+
+struct AsyncAt {  // t = A sh, (t, s), (t, t)
+    static constexpr int NE = 1;
+    const float* rf[1];
+    const float* ef[1];
+    float* t;
+    double ts, tt;
+    __device__ float op(float r) const { return r; }
+    __device__ void epi(long long q, float, float ax, float, const float* e) {
+        t[q] = ax;
+        ts += double(ax) * double(e[0]);
+        tt += double(ax) * double(ax);
+    }
+};
+
 // ------------------------------------------------------------------ kernels
 template <class Src>
 __global__ void __launch_bounds__(kBlock, 2)
@@ -173,6 +225,20 @@ mg_smooth(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, PhaseSmoo
     pdl_wait();
     if (sc->done) return;
     sweep<float>(d, tl, cf, ph);
+}
+
+__global__ void __launch_bounds__(kBlock, 2)
+mg_smooth0_as(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, AsyncSmooth0 ph) {
+    pdl_wait();
+    if (sc->done) return;
+    sweep_async(d, tl, cf, ph);
+}
+
+__global__ void __launch_bounds__(kBlock, 2)
+mg_smooth_as(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, AsyncSmooth ph) {
+    pdl_wait();
+    if (sc->done) return;
+    sweep_async(d, tl, cf, ph);
 }
 
 // bc[I,J,K] = sum over the 8 children of (b - A x) on the fine level
@@ -623,6 +689,7 @@ static MgBottom bottom_params(const MgPlan& P) {
 }
 
 // v = A ph, gamma = (v, res0), alpha = rho / gamma
+template <bool AS>
 __global__ void __launch_bounds__(kBlock, 2)
 mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
       const float* ph, const float* res0, float* v, int use_cond,
@@ -630,9 +697,17 @@ mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
     pdl_wait();
     __shared__ double sh[32];
     if (sc->done) return;
-    PhaseAv p{ph, res0, v, 0.0};
-    sweep<float>(d, tl, cf, p);
-    const double bs = block_sum<kBlock>(p.dot, sh);
+    double dot;
+    if (AS) {
+        AsyncAv p{{ph}, {res0}, v, 0.0};
+        sweep_async(d, tl, cf, p);
+        dot = p.dot;
+    } else {
+        PhaseAv p{ph, res0, v, 0.0};
+        sweep<float>(d, tl, cf, p);
+        dot = p.dot;
+    }
+    const double bs = block_sum<kBlock>(dot, sh);
     if (tid0()) part[blockIdx.x] = bs;
     if (arrive_last(sc)) {
         const double gamma = finish<false>(part, sh);
@@ -652,16 +727,25 @@ mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
 }
 
 // t = A sh, omega = (t, s) / (t, t)
+template <bool AS>
 __global__ void __launch_bounds__(kBlock, 2)
 mg_at(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
       const float* shv, const float* s, float* t) {
     pdl_wait();
     __shared__ double sh[32];
     if (sc->done) return;
-    PhaseAt p{shv, s, t, 0.0, 0.0};
-    sweep<float>(d, tl, cf, p);
-    const double b0 = block_sum<kBlock>(p.ts, sh);
-    const double b1 = block_sum<kBlock>(p.tt, sh);
+    double ts, tt;
+    if (AS) {
+        AsyncAt p{{shv}, {s}, t, 0.0, 0.0};
+        sweep_async(d, tl, cf, p);
+        ts = p.ts; tt = p.tt;
+    } else {
+        PhaseAt p{shv, s, t, 0.0, 0.0};
+        sweep<float>(d, tl, cf, p);
+        ts = p.ts; tt = p.tt;
+    }
+    const double b0 = block_sum<kBlock>(ts, sh);
+    const double b1 = block_sum<kBlock>(tt, sh);
     if (tid0()) { part[blockIdx.x] = b0; part[kMaxPartials + blockIdx.x] = b1; }
     if (arrive_last(sc)) {
         const double ts = finish<false>(part, sh);
@@ -846,6 +930,14 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
         if (cudaFuncSetAttribute(mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess)
             return PF_ERR_CUDA;
+        // the cp.async sweeps' plane rings (~49 KiB with an epilogue field)
+        const int as1 = (int)async_sweep_smem<AsyncSmooth>();
+        if (cudaFuncSetAttribute(mg_smooth_as, cudaFuncAttributeMaxDynamicSharedMemorySize, as1) ||
+            cudaFuncSetAttribute(mg_av<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, as1) ||
+            cudaFuncSetAttribute(mg_at<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, as1) ||
+            cudaFuncSetAttribute(mg_smooth0_as, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)async_sweep_smem<AsyncSmooth0>()))
+            return PF_ERR_CUDA;
         dev_done[dev] = 1;
     }
     char* ptr = (char*)region;
@@ -877,7 +969,11 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
         const float* bl = l == 0 ? b0 : f.b;
         float* xl = l == 0 ? x0 : f.x;
         if (l > 0) {
-            if (f.kind == kMgSwept) {
+            if (f.kind == kMgSwept && f.d.nz % 32 == 0) {
+                AsyncSmooth0 ph{{f.b}, {nullptr}, f.x, f.wd};
+                PF_LAUNCH("mg_smooth0", s, launch_pdl(mg_smooth0_as, dim3(tiled_grid(f.tl)), dim3(blk),
+                    async_sweep_smem<AsyncSmooth0>(), s, f.d, f.tl, f.cf, sc, ph));
+            } else if (f.kind == kMgSwept) {
                 PhaseSmooth0<SrcPlain> ph{};
                 ph.src.b = f.b; ph.x = f.x; ph.wd = f.wd;
                 PF_LAUNCH("mg_smooth0", s, launch_pdl(mg_smooth0<SrcPlain>, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s,
@@ -905,10 +1001,20 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
             const char* np = l == 0 ? "mg_prolong_l0" : "mg_prolong";
             const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
             PF_LAUNCH(np, s, launch_pdl(mg_prolong_add, dim3(cgrid3(c.d)), dim3(blk), 0, s, f.d, c.d, c.x, xl, sc));
-            PhaseSmooth a{xl, bl, f.t, f.wd};
-            PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, a));
-            PhaseSmooth b{f.t, bl, xl, f.wd};
-            PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, b));
+            if (f.d.nz % 32 == 0) {
+                const size_t sm = async_sweep_smem<AsyncSmooth>();
+                AsyncSmooth a{{xl}, {bl}, f.t, f.wd};
+                PF_LAUNCH(ns, s, launch_pdl(mg_smooth_as, dim3(tiled_grid(f.tl)), dim3(blk), sm, s,
+                                            f.d, f.tl, f.cf, sc, a));
+                AsyncSmooth b{{f.t}, {bl}, xl, f.wd};
+                PF_LAUNCH(ns, s, launch_pdl(mg_smooth_as, dim3(tiled_grid(f.tl)), dim3(blk), sm, s,
+                                            f.d, f.tl, f.cf, sc, b));
+            } else {
+                PhaseSmooth a{xl, bl, f.t, f.wd};
+                PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, a));
+                PhaseSmooth b{f.t, bl, xl, f.wd};
+                PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, b));
+            }
         } else {
             PF_LAUNCH("mg_prolong_smooth_pw", s, launch_pdl(mg_prolong_smooth_pw, dim3(cgrid3(f.d)), dim3(blk), 0, s,
                 f.d, c.d, f.cf, f.wd, c.x, xl, bl, f.t, sc));
@@ -949,8 +1055,14 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
         PF_LAUNCH("mg_smooth0_p", s, launch_pdl(mg_smooth0<SrcP>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, p_new, P.ph, sc, s);
-    PF_LAUNCH("mg_av", s, launch_pdl(mg_av, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, part, P.ph, P.res0,
-                                                   P.v, use_cond, cond));
+    const bool as = f.d.nz % 32 == 0;  // cp.async sweep for the single-input phases
+    const size_t sm1 = async_sweep_smem<AsyncAv>();
+    if (as)
+        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<true>, dim3(gt), dim3(blk), sm1, s, f.d, f.tl, f.cf, sc,
+                                         part, P.ph, P.res0, P.v, use_cond, cond));
+    else
+        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<false>, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc,
+                                         part, P.ph, P.res0, P.v, use_cond, cond));
     {   // s = res - alpha v fused into the first smoothing pass of M s
         PhaseSmooth0<SrcS> ph{};
         ph.src.res = P.res; ph.src.v = P.v; ph.src.s = P.s;
@@ -958,7 +1070,12 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
         PF_LAUNCH("mg_smooth0_s", s, launch_pdl(mg_smooth0<SrcS>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, P.s, P.sh, sc, s);
-    PF_LAUNCH("mg_at", s, launch_pdl(mg_at, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, part, P.sh, P.s, P.t));
+    if (as)
+        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<true>, dim3(gt), dim3(blk), sm1, s, f.d, f.tl, f.cf, sc,
+                                         part, P.sh, P.s, P.t));
+    else
+        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<false>, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc,
+                                         part, P.sh, P.s, P.t));
     PF_LAUNCH("mg_update", s, launch_pdl(mg_update, dim3(pointwise_grid(f.d.n)), dim3(kBlock), 0, s,
         f.d, sc, part, P.e, P.ph, P.sh, P.s, P.t, P.res, P.res0, use_cond, cond));
     return cudaGetLastError() == cudaSuccess ? PF_OK : PF_ERR_CUDA;

@@ -279,11 +279,6 @@ constexpr int kRhsPos = kRhsSY * kRhsSZ;        // halo-extended plane tile
 constexpr int kRhsPPT = (kRhsPos + 255) / 256;  // positions per thread
 constexpr int kRhsCells = 32 * kRhsTY;          // owned cells per plane
 
-__host__ __device__ inline int pmod(int a, int n) {
-    const int r = a % n;
-    return r < 0 ? r + n : r;
-}
-
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -453,11 +448,6 @@ static cudaError_t tiled_prepare() {
     cudaError_t e = cudaFuncSetAttribute(
         rhs_stage_tiled<T, TI, T, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)RhsSmem<TI, T, MODE>::bytes);
-    // the largest shared-memory carveout, so two blocks fit on an SM
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(rhs_stage_tiled<T, TI, T, T, MODE>,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }

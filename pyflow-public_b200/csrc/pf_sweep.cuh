@@ -222,6 +222,144 @@ __device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
     }
 }
 
+// --------------------------------------------------------------------------
+// FP32 sweep with a cp.async pipeline (grids whose z extent is a multiple of
+// 32).  Block 32 x 8 threads, tile 32 (z) x 32 (y) x xc (x); the input planes
+// (with a one-cell y/z halo) arrive in shared memory DEP planes ahead of use
+// through 16-byte cp.async copies (4-byte copies for the z-halo columns), so
+// no thread holds prefetched data in registers.  The phase object provides
+//   NR == 1 input field rf[0] and NE (0 or 1) epilogue fields ef[],
+//   float op(float raw)          -- the stencil operand of a cell,
+//   epi(q, op_c, A op, raw_c, e) -- consumes an owned cell (e: NE values).
+// Dynamic shared memory: async_sweep_smem<Ph>() bytes.
+// --------------------------------------------------------------------------
+constexpr int kAsyncTY = 32;         // tile rows
+constexpr int kAsyncSZ = 40;         // smem row stride: halo at 3 and 36, cells at 4..35
+constexpr int kAsyncDep = 2;         // planes in flight ahead of use
+constexpr int kAsyncRS = kAsyncDep + 4;
+constexpr int kAsyncES = kAsyncDep + 2;
+constexpr int kAsyncRPos = (kAsyncTY + 2) * kAsyncSZ;
+constexpr int kAsyncEPos = kAsyncTY * 32;
+
+template <class Ph>
+constexpr size_t async_sweep_smem() {
+    return (size_t)(kAsyncRS * kAsyncRPos + kAsyncES * Ph::NE * kAsyncEPos) * sizeof(float);
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_sm(void* smem, const void* gmem) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    if (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(a), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" :: "r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait_groups() {
+    asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
+}
+
+template <class Ph>
+__device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
+                                            const LapCoef<float>& cf, Ph& ph) {
+    constexpr int TY = kAsyncTY, SZ = kAsyncSZ, RS = kAsyncRS, ES = kAsyncES;
+    extern __shared__ __align__(16) float async_sm[];
+    float* rr = async_sm;                    // [RS][RPos]
+    float* ee = async_sm + RS * kAsyncRPos;  // [ES][NE][EPos]
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const long long plane = (long long)d.ny * d.nz;
+    const float* xr = ph.rf[0];
+    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+        const int tz = (int)(t % tl.ntz);
+        const long long r2 = t / tl.ntz;
+        const int tyy = (int)(r2 % tl.nty), txx = (int)(r2 / tl.nty);
+        const int k0 = tz * 32, j0 = tyy * TY, i0 = txx * tl.xc;
+        const int i1 = min(i0 + tl.xc, d.nx);
+        const int ey = min(TY, d.ny - j0);
+        auto load_raw = [&](int xp, int slot) {
+            const long long base = (long long)pmod(xp, d.nx) * plane;
+            float* dst = rr + slot * kAsyncRPos;
+            for (int p = tid; p < (TY + 2) * 8; p += 256) {
+                const int yy = p >> 3, ch = p & 7;
+                const int jj = pmod(j0 + yy - 1, d.ny);
+                cp_async_sm<16>(dst + yy * SZ + 4 + 4 * ch, xr + base + (long long)jj * d.nz + k0 + 4 * ch);
+            }
+            for (int p = tid; p < (TY + 2) * 2; p += 256) {
+                const int yy = p >> 1, side = p & 1;
+                const int jj = pmod(j0 + yy - 1, d.ny);
+                const int kk = side ? pmod(k0 + 32, d.nz) : pmod(k0 - 1, d.nz);
+                cp_async_sm<4>(dst + yy * SZ + (side ? 36 : 3), xr + base + (long long)jj * d.nz + kk);
+            }
+        };
+        auto load_ext = [&](int xp, int slot) {
+            const long long base = (long long)xp * plane;
+#pragma unroll
+            for (int f = 0; f < Ph::NE; ++f) {
+                float* dst = ee + (slot * Ph::NE + f) * kAsyncEPos;
+                for (int p = tid; p < TY * 8; p += 256) {
+                    const int yy = p >> 3, ch = p & 7;
+                    if (yy < ey)
+                        cp_async_sm<16>(dst + yy * 32 + 4 * ch,
+                                        ph.ef[f] + base + (long long)(j0 + yy) * d.nz + k0 + 4 * ch);
+                }
+            }
+        };
+        auto rslot = [&](int xp) { return (xp - i0 + 1 + 4 * RS) % RS; };
+        auto eslot = [&](int xp) { return (xp - i0 + 4 * ES) % ES; };
+        load_raw(i0 - 1, rslot(i0 - 1));
+        load_raw(i0, rslot(i0));
+        load_raw(i0 + 1, rslot(i0 + 1));
+        load_ext(i0, eslot(i0));
+        cp_async_commit_group();
+#pragma unroll
+        for (int a = 1; a <= kAsyncDep; ++a) {
+            if (i0 + a < i1) { load_raw(i0 + a + 1, rslot(i0 + a + 1)); load_ext(i0 + a, eslot(i0 + a)); }
+            cp_async_commit_group();
+        }
+        for (int i = i0; i < i1; ++i) {
+            cp_async_wait_groups<kAsyncDep>();
+            __syncthreads();
+            if (i + kAsyncDep + 1 < i1) {
+                load_raw(i + kAsyncDep + 2, rslot(i + kAsyncDep + 2));
+                load_ext(i + kAsyncDep + 1, eslot(i + kAsyncDep + 1));
+            }
+            cp_async_commit_group();
+            const float* pm = rr + rslot(i - 1) * kAsyncRPos;
+            const float* pc = rr + rslot(i) * kAsyncRPos;
+            const float* pp = rr + rslot(i + 1) * kAsyncRPos;
+            const float* eb = ee + eslot(i) * Ph::NE * kAsyncEPos;
+            const long long bi = (long long)i * plane;
+#pragma unroll
+            for (int r = 0; r < TY / 8; ++r) {
+                const int yl = ty + 8 * r;
+                if (yl >= ey) continue;
+                const int c = (yl + 1) * SZ + tx + 4;
+                const float rc = pc[c];
+                const float oc = ph.op(rc);
+                float b = 0.0f;
+                b += ph.op(pm[c]) * cf.c[0][0];
+                b += oc * cf.c[0][1];
+                b += ph.op(pp[c]) * cf.c[0][2];
+                b += ph.op(pc[c - SZ]) * cf.c[1][0];
+                b += oc * cf.c[1][1];
+                b += ph.op(pc[c + SZ]) * cf.c[1][2];
+                b += ph.op(pc[c - 1]) * cf.c[2][0];
+                b += oc * cf.c[2][1];
+                b += ph.op(pc[c + 1]) * cf.c[2][2];
+                float e[Ph::NE > 0 ? Ph::NE : 1];
+#pragma unroll
+                for (int f = 0; f < Ph::NE; ++f) e[f] = eb[f * kAsyncEPos + yl * 32 + tx];
+                ph.epi(bi + (long long)(j0 + yl) * d.nz + k0 + tx, oc, b, rc, e);
+            }
+        }
+        cp_async_wait_groups<0>();
+        __syncthreads();
+    }
+}
+
 // Last-block completion: returns true in every thread of the last block.
 __device__ __forceinline__ bool arrive_last(BicgScalars* sc) {
     __shared__ bool last;

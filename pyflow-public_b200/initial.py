@@ -56,13 +56,20 @@ def box_lengths(shape, lengths=None):
 
 
 def spectral_velocity_device(shape, lengths=(2 * np.pi,) * 3, k0=4.0, urms=1.0,
-                             seed=0, device="cuda"):
-    """Same recipe as :func:`spectral_velocity` (same noise from the same
-    seed), with the FFTs done by torch on ``device``; for large grids.
+                             seed=0, device="cuda", noise="host"):
+    """Same recipe as :func:`spectral_velocity`, with the FFTs done by torch
+    on ``device``; for large grids.  noise='host' draws the same noise as
+    spectral_velocity from the same seed (numpy, on the host); noise='device'
+    draws it on the device from a torch generator seeded with ``seed`` (a
+    different field with the same spectrum, without the host cost).
     Returns FP64 torch tensors."""
     import torch
     nx, ny, nz = (int(n) for n in shape)
     rng = np.random.default_rng(seed)
+    gen = None
+    if noise == "device":
+        gen = torch.Generator(device=device)
+        gen.manual_seed(int(seed))
     h = [lengths[d] / shape[d] for d in range(3)]
     kax = [torch.tensor(np.fft.fftfreq(shape[d], d=h[d]) * 2 * np.pi,
                         device=device) for d in range(3)]
@@ -76,9 +83,12 @@ def spectral_velocity_device(shape, lengths=(2 * np.pi,) * 3, k0=4.0, urms=1.0,
     del ek, kmag
     hat = []
     for _ in range(3):
-        noise = torch.from_numpy(rng.standard_normal((nx, ny, nz))).to(device)
-        hat.append(torch.fft.fftn(noise) * amp)
-        del noise
+        if gen is not None:
+            nz_ = torch.randn((nx, ny, nz), generator=gen, dtype=torch.float64, device=device)
+        else:
+            nz_ = torch.from_numpy(rng.standard_normal((nx, ny, nz))).to(device)
+        hat.append(torch.fft.fftn(nz_) * amp)
+        del nz_
     g = [(torch.exp(1j * th[0]) - 1.0)[:, None, None] / h[0],
          (torch.exp(1j * th[1]) - 1.0)[None, :, None] / h[1],
          (torch.exp(1j * th[2]) - 1.0)[None, None, :] / h[2]]

@@ -11,6 +11,10 @@ admitted into free slots, and the steps of all active requests are in flight on
 the device at the same time.  Each step of a request depends only on its own
 buffers, so its result is the same alone and in any mix.
 
+A request's initial field is the seeded k^4 exp(-2 (k/k0)^2) spectrum with
+its noise drawn on the device from the request's seed (no host-side random
+numbers on the admission path).
+
 Reported: per-request latency (arrival to completion), its p50/p99, and the
 aggregate cell-steps/s.
 """
@@ -112,7 +116,8 @@ class Server:
         stream = torch.cuda.Stream(self.device)
         with torch.cuda.stream(stream):
             u, v, w = initial.spectral_velocity_device(
-                (n, n, n), k0=req.k0, urms=req.urms, seed=req.seed, device=self.device)
+                (n, n, n), k0=req.k0, urms=req.urms, seed=req.seed, device=self.device,
+                noise="device")
             u, v, w = u.contiguous(), v.contiguous(), w.contiguous()
             p = torch.zeros_like(u)
             DP = torch.zeros_like(u)
