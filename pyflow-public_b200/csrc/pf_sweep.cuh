@@ -279,19 +279,26 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
         const int k0 = tz * 32, j0 = tyy * TY, i0 = txx * tl.xc;
         const int i1 = min(i0 + tl.xc, d.nx);
         const int ey = min(TY, d.ny - j0);
+        // a single wrap suffices for the halo rows unless the grid is
+        // shorter than a tile in y (nz is a multiple of 32, so z needs one)
+        const bool short_y = d.ny <= TY;
+        auto yrow = [&](int yy) {
+            const int j = j0 + yy - 1;
+            return short_y ? pmod(j, d.ny) : wrap(j, d.ny);
+        };
+        const int kl = wrap(k0 - 1, d.nz), kr = wrap(k0 + 32, d.nz);
         auto load_raw = [&](int xp, int slot) {
             const long long base = (long long)pmod(xp, d.nx) * plane;
             float* dst = rr + slot * kAsyncRPos;
             for (int p = tid; p < (TY + 2) * 8; p += 256) {
                 const int yy = p >> 3, ch = p & 7;
-                const int jj = pmod(j0 + yy - 1, d.ny);
-                cp_async_sm<16>(dst + yy * SZ + 4 + 4 * ch, xr + base + (long long)jj * d.nz + k0 + 4 * ch);
+                cp_async_sm<16>(dst + yy * SZ + 4 + 4 * ch,
+                                xr + base + (long long)yrow(yy) * d.nz + k0 + 4 * ch);
             }
             for (int p = tid; p < (TY + 2) * 2; p += 256) {
                 const int yy = p >> 1, side = p & 1;
-                const int jj = pmod(j0 + yy - 1, d.ny);
-                const int kk = side ? pmod(k0 + 32, d.nz) : pmod(k0 - 1, d.nz);
-                cp_async_sm<4>(dst + yy * SZ + (side ? 36 : 3), xr + base + (long long)jj * d.nz + kk);
+                cp_async_sm<4>(dst + yy * SZ + (side ? 36 : 3),
+                               xr + base + (long long)yrow(yy) * d.nz + (side ? kr : kl));
             }
         };
         auto load_ext = [&](int xp, int slot) {
