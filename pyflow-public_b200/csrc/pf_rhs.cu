@@ -12,6 +12,8 @@
 // The flux expressions keep the reference's operation order (see
 // pf_common.cuh), including the edge-averaged viscosity one cell below the
 // off-diagonal flux (metric_staggered.py:127-144 vs :378-384).
+#include <algorithm>
+
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
 #include "pf_profile.cuh"
@@ -448,6 +450,14 @@ static cudaError_t tiled_prepare() {
     cudaError_t e = cudaFuncSetAttribute(
         rhs_stage_tiled<T, TI, T, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)RhsSmem<TI, T, MODE>::bytes);
+    // a shared-memory carveout just large enough for two blocks per SM (the
+    // rest stays L1): percent of the SM's 228 KiB
+    if (e == cudaSuccess) {
+        const size_t two = 2 * (RhsSmem<TI, T, MODE>::bytes + 1024);
+        const int pct = (int)std::min<size_t>(100, (two * 100 + 228 * 1024 - 1) / (228 * 1024));
+        e = cudaFuncSetAttribute(rhs_stage_tiled<T, TI, T, T, MODE>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }
