@@ -12,8 +12,9 @@
 //   1. each thread computes its cell's gradients and writes 16 BF16 features
 //      (9 + 7 zero pads) into the X tile in shared memory;
 //   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
-//   3. each thread reads its D1 row from TMEM (tcgen05.ld), adds b1, applies
-//      tanh, and writes the BF16 row into the H tile;
+//   3. each thread reads its D1 row from TMEM (tcgen05.ld, 32 columns per
+//      wait), adds b1, applies tanh, and writes the BF16 row (pairs packed
+//      by one conversion) into the H tile;
 //   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
 //   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
 //      its six stresses (FP64) to global memory.
@@ -131,10 +132,34 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float tanh_fast(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
+// 32 consecutive accumulator columns of this thread's lane, one wait
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+          "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+          "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
+          "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+          "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// tanh of two FP32 values (hardware approximation), rounded to BF16 and
+// packed (a in the low half) by one conversion
+__device__ __forceinline__ uint32_t tanh_pack_bf16x2(float a, float b) {
+    float ta, tb;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(ta) : "f"(a));
+    asm("tanh.approx.f32 %0, %1;" : "=f"(tb) : "f"(b));
+    uint32_t out;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(tb), "f"(ta));
+    return out;
 }
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {
@@ -229,18 +254,16 @@ __device__ inline void nb_gradients(const CellNb& nb, double dxi, double dyi, do
 __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bias,
                                                 uint8_t* H, int row) {
 #pragma unroll 1
-    for (int c0 = 0; c0 < kHidden; c0 += 16) {
-        float v[16];
-        tmem_ld16(taddr + c0, v);
+    for (int c0 = 0; c0 < kHidden; c0 += 32) {
+        float v[32];
+        tmem_ld32(taddr + c0, v);
 #pragma unroll
-        for (int q = 0; q < 16; q += 8) {
+        for (int q = 0; q < 32; q += 8) {
             uint32_t packed[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const float a = tanh_fast(v[q + 2 * e] + bias[c0 + q + 2 * e]);
-                const float b = tanh_fast(v[q + 2 * e + 1] + bias[c0 + q + 2 * e + 1]);
-                packed[e] = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
-            }
+            for (int e = 0; e < 4; ++e)
+                packed[e] = tanh_pack_bf16x2(v[q + 2 * e] + bias[c0 + q + 2 * e],
+                                             v[q + 2 * e + 1] + bias[c0 + q + 2 * e + 1]);
             // 8 consecutive k of one row are one 16-byte chunk
             *reinterpret_cast<uint4*>(H + kmajor_off(row, c0 + q, 4096)) =
                 make_uint4(packed[0], packed[1], packed[2], packed[3]);
