@@ -132,9 +132,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 32 consecutive accumulator columns of this thread's lane, one wait
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-    uint32_t r[32];
+// 32 consecutive accumulator columns of this thread's lane (no wait)
+__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
@@ -146,9 +145,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
           "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // tanh of two FP32 values (hardware approximation), rounded to BF16 and
@@ -254,11 +254,17 @@ __device__ inline void nb_gradients(const CellNb& nb, double dxi, double dyi, do
 __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bias,
                                                 uint8_t* H, int row) {
 #pragma unroll 1
-    for (int c0 = 0; c0 < kHidden; c0 += 32) {
-        float v[32];
-        tmem_ld32(taddr + c0, v);
+    for (int c0 = 0; c0 < kHidden; c0 += 64) {
+        // two 32-column loads in flight, one wait
+        uint32_t r[64];
+        tmem_ld32_issue(taddr + c0, r);
+        tmem_ld32_issue(taddr + c0 + 32, r + 32);
+        tmem_wait_ld();
+        float v[64];
 #pragma unroll
-        for (int q = 0; q < 32; q += 8) {
+        for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+#pragma unroll
+        for (int q = 0; q < 64; q += 8) {
             uint32_t packed[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e)
