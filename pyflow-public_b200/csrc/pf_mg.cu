@@ -537,13 +537,19 @@ mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
     __shared__ double shd[32];
     __shared__ float mean_s;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int last = P.nlev - 1;
     {
         const int n = (int)P.d[0].n;
         float* b = sm + P.off[0];
         for (int q = tid; q < n; q += nt) b[q] = gb[q];
+        // the coarsest pseudo-inverse (<= 64 x 64) into shared memory too
+        if (P.pinv) {
+            const int nc = (int)P.d[last].n;
+            float* pv = sm + P.off[last] + 3 * nc;
+            for (int q = tid; q < nc * nc; q += nt) pv[q] = __ldg(P.pinv + q);
+        }
     }
     __syncthreads();
-    const int last = P.nlev - 1;
     // down: pre-smooth from zero, restrict
     for (int l = 0; l < last; ++l) {
         const Dims d = P.d[l], c = P.d[l + 1];
@@ -575,13 +581,22 @@ mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
     }
     // coarsest: x = A^+ b, or mean removal then Jacobi sweeps (x <-> t)
     if (P.pinv) {
+        // x = A^+ b: 16 threads per row, 16-lane shuffle reduction
         const int n = (int)P.d[last].n;
         const float* b = sm + P.off[last];
         float* x = sm + P.off[last] + n;
-        for (int p = tid; p < n; p += nt) {
+        const float* pv = sm + P.off[last] + 3 * n;
+        // whole warps take part in every pass of the loop (the bound is a
+        // multiple of 32, like the block), so the shuffles see all lanes
+        const int tot = ((16 * n + 31) / 32) * 32;
+        for (int t = tid; t < tot; t += nt) {
+            const int p = t >> 4, part = t & 15;
             float acc = 0.0f;
-            for (int r = 0; r < n; ++r) acc = fmaf(__ldg(P.pinv + (long long)r * n + p), b[r], acc);
-            x[p] = acc;
+            if (p < n)
+                for (int r = part; r < n; r += 16) acc = fmaf(pv[r * n + p], b[r], acc);
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, 16);
+            if (part == 0 && p < n) x[p] = acc;
         }
         __syncthreads();
     } else {
@@ -667,6 +682,7 @@ mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
 static size_t bottom_smem_floats(const MgPlan& P) {
     size_t f = 0;
     for (int l = P.B; l < P.L; ++l) f += 3 * (size_t)P.lv[l].d.n;
+    if (P.pinv) f += (size_t)P.lv[P.L - 1].d.n * P.lv[P.L - 1].d.n;  // the pseudo-inverse
     return f;
 }
 
@@ -926,7 +942,8 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
     if (dev >= 0 && dev < 64 && !dev_done[dev]) {
         // the bottom levels (at most 4096 + 512 + 64 + ... cells, 3 arrays
         // each) need more than the default 48 KiB of shared memory
-        const int bytes = int(3 * sizeof(float) * (kMgBottomMax + kMgBottomMax / 7 + 64));
+        const int bytes = int(sizeof(float) * (3 * (kMgBottomMax + kMgBottomMax / 7 + 64) +
+                                                kMgPinvMax * kMgPinvMax));
         if (cudaFuncSetAttribute(mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess)
             return PF_ERR_CUDA;
