@@ -29,9 +29,9 @@
 // sweep of pf_sweep.cuh (prolongation: one thread per coarse cell updating its
 // 8 children); mid-size levels one thread per cell (a sweep's plane-by-plane
 // march is latency-bound on small grids) with the prolongation fused into the
-// first post-smoothing pass; every level of at
-// most 4096 cells runs inside ONE CTA in shared memory (mg_bottom), so the
-// bottom of the V-cycle is a single launch.
+// first post-smoothing pass; every level of at most 512 cells (and the
+// coarsest level, at most 4096 cells) runs inside ONE CTA in shared memory
+// (mg_bottom), so the bottom of the V-cycle is a single launch.
 //
 // All vectors are FP32; every dot product and max accumulates in FP64 and is
 // finished by the last block (fixed order).  Scalars stay on the device.
@@ -904,7 +904,7 @@ int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom) {
         l.tl = make_tiling(l.d, 32);
         l.tl8 = make_tiling(l.d, 64);
         l.kind = (L == 0 || l.d.n >= kMgSweepMin) ? kMgSwept
-                 : (l.d.n > kMgBottomMax ? kMgPointwise : kMgBottom);
+                 : (l.d.n > kMgBottomLevel ? kMgPointwise : kMgBottom);
         ++L;
         if (l.d.n <= kMgCoarseTarget || L == kMgMaxLevels) break;
         if ((cur.nx | cur.ny | cur.nz) & 1) break;
@@ -912,6 +912,9 @@ int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom) {
         cur.nx /= 2; cur.ny /= 2; cur.nz /= 2;
         cur.dx *= 2.0; cur.dy *= 2.0; cur.dz *= 2.0;
     }
+    // the coarsest level always runs in the bottom kernel
+    if (L >= 2 && lv[L - 1].kind == kMgPointwise && lv[L - 1].d.n <= kMgBottomMax)
+        lv[L - 1].kind = kMgBottom;
     int B = 0;
     while (B < L && lv[B].kind != kMgBottom) ++B;
     if (L < 2 || B == 0 || B == L) return 0;

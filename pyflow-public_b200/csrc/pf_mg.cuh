@@ -7,12 +7,14 @@ namespace pf {
 
 constexpr int kMgMaxLevels = 16;
 constexpr long long kMgCoarseTarget = 64;     // coarsen down to at most this many cells
-constexpr long long kMgBottomMax = 4096;      // levels this small run inside one CTA
+constexpr long long kMgBottomMax = 4096;      // largest coarsest level (solved in one CTA)
+constexpr long long kMgBottomLevel = 512;     // levels this small run inside that CTA
 constexpr long long kMgSweepMin = 1LL << 20;  // levels this large use the tiled sweep
 
 // How a level's kernels run: the tiled sweep (the finest level always, and
 // every level of at least kMgSweepMin cells), one thread per cell, or inside
-// the single-CTA bottom kernel (every level of at most kMgBottomMax cells).
+// the single-CTA bottom kernel (every level of at most kMgBottomLevel cells,
+// and the coarsest level, which must have at most kMgBottomMax cells).
 enum MgKind { kMgSwept = 0, kMgPointwise = 1, kMgBottom = 2 };
 
 struct MgLevel {
