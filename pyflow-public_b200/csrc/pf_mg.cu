@@ -158,56 +158,81 @@ struct PhaseAt {
 };
 
 // The same phases for sweep_async (FP32 grids with nz a multiple of 32).
-struct AsyncSmooth0 {  // x = w (2 b - w A b)
-    static constexpr int NE = 0;
-    const float* rf[1];
+// Sources of the first smoothing pass, from their raw input fields:
+struct AsyncPlain {  // b of a coarse level
+    static constexpr int NR = 1;
+    __device__ void setup(const BicgScalars*) {}
+    __device__ float op(const float* r) const { return r[0]; }
+    __device__ void store(long long, float) const {}
+};
+
+struct AsyncS {  // s = res - alpha v from (res, v), stored to s
+    static constexpr int NR = 2;
+    float* s;
+    float alpha;
+    __device__ void setup(const BicgScalars* sc) { alpha = float(sc->alpha); }
+    __device__ float op(const float* r) const { return fmaf(-alpha, r[1], r[0]); }
+    __device__ void store(long long q, float c) const { s[q] = c; }
+};
+
+template <class S>
+struct AsyncSmooth0 {  // x = w (2 b - w A b), b = the source's operand
+    static constexpr int NR = S::NR, NE = 0;
+    S src;
+    const float* rf[NR];
     const float* ef[1];
     float* x;
     float wd;
-    __device__ float op(float r) const { return r; }
-    __device__ void epi(long long q, float c, float ab, float, const float*) {
+    __device__ float op(const float* r) const { return src.op(r); }
+    __device__ void epi(long long q, float c, float ab, const float*) {
+        src.store(q, c);
         x[q] = wd * (2.0f * c - wd * ab);
     }
 };
 
 struct AsyncSmooth {  // out = x + w (b - A x)
-    static constexpr int NE = 1;
+    static constexpr int NR = 1, NE = 1;
     const float* rf[1];
     const float* ef[1];
     float* out;
     float wd;
-    __device__ float op(float r) const { return r; }
-    __device__ void epi(long long q, float c, float ax, float, const float* e) {
+    __device__ float op(const float* r) const { return r[0]; }
+    __device__ void epi(long long q, float c, float ax, const float* e) {
         out[q] = fmaf(wd, e[0] - ax, c);
     }
 };
 
 struct AsyncAv {  // v = A ph, (v, res0)
-    static constexpr int NE = 1;
+    static constexpr int NR = 1, NE = 1;
     const float* rf[1];
     const float* ef[1];
     float* v;
     double dot;
-    __device__ float op(float r) const { return r; }
-    __device__ void epi(long long q, float, float ax, float, const float* e) {
+    __device__ float op(const float* r) const { return r[0]; }
+    __device__ void epi(long long q, float, float ax, const float* e) {
         v[q] = ax;
         dot += double(ax) * double(e[0]);
     }
 };
 
 struct AsyncAt {  // t = A sh, (t, s), (t, t)
-    static constexpr int NE = 1;
+    static constexpr int NR = 1, NE = 1;
     const float* rf[1];
     const float* ef[1];
     float* t;
     double ts, tt;
-    __device__ float op(float r) const { return r; }
-    __device__ void epi(long long q, float, float ax, float, const float* e) {
+    __device__ float op(const float* r) const { return r[0]; }
+    __device__ void epi(long long q, float, float ax, const float* e) {
         t[q] = ax;
         ts += double(ax) * double(e[0]);
         tt += double(ax) * double(ax);
     }
 };
+
+// Tile heights of the cp.async sweeps: 32 rows for one input field, 16 for
+// the two-field first pass of M s (its plane ring stays small enough for two
+// blocks per SM).
+constexpr int kAsTY1 = 32, kAsTYn = 16;
 
 // ------------------------------------------------------------------ kernels
 template <class Src>
@@ -227,21 +252,30 @@ mg_smooth(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, PhaseSmoo
     sweep<float>(d, tl, cf, ph);
 }
 
+template <int TY, int TZ, class S>
 __global__ void __launch_bounds__(kBlock, 2)
-mg_smooth0_as(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, AsyncSmooth0 ph) {
+mg_smooth0_as(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, AsyncSmooth0<S> ph) {
     pdl_wait();
     if (sc->done) return;
-    sweep_async(d, tl, cf, ph);
+    ph.src.setup(sc);
+    sweep_async<TY, TZ>(d, tl, cf, ph);
 }
 
+template <int TZ>
 __global__ void __launch_bounds__(kBlock, 2)
 mg_smooth_as(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, AsyncSmooth ph) {
     pdl_wait();
     if (sc->done) return;
-    sweep_async(d, tl, cf, ph);
+    sweep_async<kAsTY1, TZ>(d, tl, cf, ph);
 }
 
-// bc[I,J,K] = sum over the 8 children of (b - A x) on the fine level
+// bc[I,J,K] = sum over the 8 children of (b - A x) on the fine level.  One
+// thread per coarse (J, K) and TWO coarse planes I0, I0 + 1 (fine x planes
+// 2 I0 - 1 .. 2 I0 + 4 loaded once); each fine row pair 2K, 2K + 1 is one
+// 8-byte load, and the z halos 2K - 1, 2K + 2 come from the neighbouring
+// lanes (loaded only at the warp's edges and the grid's periodic wrap).
+// Lanes past c.nz compute on a clamped K (so every lane takes part in the
+// shuffles) and store nothing.  Needs fine dims = 2 x coarse dims.
 __global__ void __launch_bounds__(256)
 mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
             const float* __restrict__ x, Dims c, float* __restrict__ bc,
@@ -249,48 +283,59 @@ mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
     pdl_wait();
     if (sc->done) return;
     const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y;
-    const int I = blockIdx.z;
-    if (K >= c.nz || J >= c.ny) return;
-    long long ia[4], jb[4];
-    int kc[4];
+    const int I0 = blockIdx.z * 2;
+    if (J >= c.ny) return;  // uniform across the warp (threadIdx.y is)
+    const bool ok = K < c.nz;
+    const int Kc = ok ? K : c.nz - 1;
+    const bool ledge = threadIdx.x == 0, redge = threadIdx.x == 31 || Kc + 1 >= c.nz;
+    long long ia[6], jb[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        ia[a] = (long long)wrap(2 * I - 1 + a, f.nx) * f.ny * f.nz;
-        jb[a] = (long long)wrap(2 * J - 1 + a, f.ny) * f.nz;
-        kc[a] = wrap(2 * K - 1 + a, f.nz);
+    for (int a = 0; a < 6; ++a) ia[a] = (long long)pmod(2 * I0 - 1 + a, f.nx) * f.ny * f.nz;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) jb[a] = (long long)wrap(2 * J - 1 + a, f.ny) * f.nz;
+    const int kl = wrap(2 * Kc - 1, f.nz), kr = wrap(2 * Kc + 2, f.nz);
+    // x pairs (2K, 2K+1) of fine rows (a, bb); the four corner rows are unused
+    float2 xp[6][4];
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            const bool need = (a >= 1 && a <= 4) || bb == 1 || bb == 2;
+            xp[a][bb] = need ? __ldg(reinterpret_cast<const float2*>(x + ia[a] + jb[bb] + 2 * Kc))
+                             : make_float2(0.0f, 0.0f);
+        }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int a = 1 + 2 * h; a < 3 + 2 * h; ++a)
+#pragma unroll
+            for (int bb = 1; bb < 3; ++bb) {
+                float zl = __shfl_up_sync(0xffffffffu, xp[a][bb].y, 1);
+                float zr = __shfl_down_sync(0xffffffffu, xp[a][bb].x, 1);
+                if (ledge) zl = __ldg(x + ia[a] + jb[bb] + kl);
+                if (redge) zr = __ldg(x + ia[a] + jb[bb] + kr);
+                const float2 bv = __ldg(reinterpret_cast<const float2*>(b + ia[a] + jb[bb] + 2 * Kc));
+                const float z[4] = {zl, xp[a][bb].x, xp[a][bb].y, zr};
+#pragma unroll
+                for (int cc = 1; cc < 3; ++cc) {
+                    auto at = [&](int aa, int b2) { return cc == 1 ? xp[aa][b2].x : xp[aa][b2].y; };
+                    const float xc = z[cc];
+                    float ax = 0.0f;
+                    ax += at(a - 1, bb) * cf.c[0][0];
+                    ax += xc * cf.c[0][1];
+                    ax += at(a + 1, bb) * cf.c[0][2];
+                    ax += at(a, bb - 1) * cf.c[1][0];
+                    ax += xc * cf.c[1][1];
+                    ax += at(a, bb + 1) * cf.c[1][2];
+                    ax += z[cc - 1] * cf.c[2][0];
+                    ax += xc * cf.c[2][1];
+                    ax += z[cc + 1] * cf.c[2][2];
+                    sum += (cc == 1 ? bv.x : bv.y) - ax;
+                }
+            }
+        if (ok && I0 + h < c.nx) bc[idx(c, I0 + h, J, K)] = sum;
     }
-    // x on the 2x2x2 block and its 24 face neighbours
-    float xv[4][4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int bb = 0; bb < 4; ++bb)
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                const int core = (a == 1 || a == 2) + (bb == 1 || bb == 2) + (cc == 1 || cc == 2);
-                xv[a][bb][cc] = core >= 2 ? __ldg(x + ia[a] + jb[bb] + kc[cc]) : 0.0f;
-            }
-    float sum = 0.0f;
-#pragma unroll
-    for (int a = 1; a < 3; ++a)
-#pragma unroll
-        for (int bb = 1; bb < 3; ++bb)
-#pragma unroll
-            for (int cc = 1; cc < 3; ++cc) {
-                const float xc = xv[a][bb][cc];
-                float ax = 0.0f;
-                ax += xv[a - 1][bb][cc] * cf.c[0][0];
-                ax += xc * cf.c[0][1];
-                ax += xv[a + 1][bb][cc] * cf.c[0][2];
-                ax += xv[a][bb - 1][cc] * cf.c[1][0];
-                ax += xc * cf.c[1][1];
-                ax += xv[a][bb + 1][cc] * cf.c[1][2];
-                ax += xv[a][bb][cc - 1] * cf.c[2][0];
-                ax += xc * cf.c[2][1];
-                ax += xv[a][bb][cc + 1] * cf.c[2][2];
-                sum += __ldg(b + ia[a] + jb[bb] + kc[cc]) - ax;
-            }
-    bc[idx(c, I, J, K)] = sum;
 }
 
 // ------------------------------------------------- one thread per cell
@@ -704,8 +749,9 @@ static MgBottom bottom_params(const MgPlan& P) {
     return m;
 }
 
-// v = A ph, gamma = (v, res0), alpha = rho / gamma
-template <bool AS>
+// v = A ph, gamma = (v, res0), alpha = rho / gamma (TZ: cp.async tile width,
+// 0 for the register-prefetch sweep)
+template <int TZ>
 __global__ void __launch_bounds__(kBlock, 2)
 mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
       const float* ph, const float* res0, float* v, int use_cond,
@@ -714,9 +760,9 @@ mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
     __shared__ double sh[32];
     if (sc->done) return;
     double dot;
-    if (AS) {
+    if constexpr (TZ > 0) {
         AsyncAv p{{ph}, {res0}, v, 0.0};
-        sweep_async(d, tl, cf, p);
+        sweep_async<kAsTY1, TZ>(d, tl, cf, p);
         dot = p.dot;
     } else {
         PhaseAv p{ph, res0, v, 0.0};
@@ -743,7 +789,7 @@ mg_av(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
 }
 
 // t = A sh, omega = (t, s) / (t, t)
-template <bool AS>
+template <int TZ>
 __global__ void __launch_bounds__(kBlock, 2)
 mg_at(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
       const float* shv, const float* s, float* t) {
@@ -751,9 +797,9 @@ mg_at(Dims d, Tiling tl, LapCoef<float> cf, BicgScalars* sc, double* part,
     __shared__ double sh[32];
     if (sc->done) return;
     double ts, tt;
-    if (AS) {
+    if constexpr (TZ > 0) {
         AsyncAt p{{shv}, {s}, t, 0.0, 0.0};
-        sweep_async(d, tl, cf, p);
+        sweep_async<kAsTY1, TZ>(d, tl, cf, p);
         ts = p.ts; tt = p.tt;
     } else {
         PhaseAt p{shv, s, t, 0.0, 0.0};
@@ -903,6 +949,9 @@ int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom) {
         l.b = l.x = l.t = nullptr;
         l.tl = make_tiling(l.d, 32);
         l.tl8 = make_tiling(l.d, 64);
+        l.az = l.d.nz % 64 == 0 ? 64 : (l.d.nz % 32 == 0 ? 32 : 0);
+        l.ta1 = make_tiling(l.d, kAsTY1, l.az ? l.az : 32);
+        l.tan = make_tiling(l.d, kAsTYn, l.az ? l.az : 32);
         l.kind = (L == 0 || l.d.n >= kMgSweepMin) ? kMgSwept
                  : (l.d.n > kMgBottomLevel ? kMgPointwise : kMgBottom);
         ++L;
@@ -936,6 +985,24 @@ size_t mg_region_bytes(const pf_grid* g) {
     return b;
 }
 
+template <class K>
+static bool smem_attr(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bytes) != cudaSuccess;
+}
+
+// dynamic shared memory limits of the cp.async sweeps of tile width TZ
+template <int TZ>
+static bool async_attrs() {
+    return smem_attr(mg_smooth0_as<kAsTY1, TZ, AsyncPlain>,
+                     async_sweep_smem<kAsTY1, TZ, AsyncSmooth0<AsyncPlain>>()) ||
+           smem_attr(mg_smooth0_as<kAsTYn, TZ, AsyncS>,
+                     async_sweep_smem<kAsTYn, TZ, AsyncSmooth0<AsyncS>>()) ||
+           smem_attr(mg_smooth_as<TZ>, async_sweep_smem<kAsTY1, TZ, AsyncSmooth>()) ||
+           smem_attr(mg_av<TZ>, async_sweep_smem<kAsTY1, TZ, AsyncAv>()) ||
+           smem_attr(mg_at<TZ>, async_sweep_smem<kAsTY1, TZ, AsyncAt>());
+}
+
 int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
     P->L = mg_levels(g, P->lv, &P->B);
     if (!P->L) return PF_ERR_BAD_ARG;
@@ -950,14 +1017,8 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
         if (cudaFuncSetAttribute(mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  bytes) != cudaSuccess)
             return PF_ERR_CUDA;
-        // the cp.async sweeps' plane rings (~49 KiB with an epilogue field)
-        const int as1 = (int)async_sweep_smem<AsyncSmooth>();
-        if (cudaFuncSetAttribute(mg_smooth_as, cudaFuncAttributeMaxDynamicSharedMemorySize, as1) ||
-            cudaFuncSetAttribute(mg_av<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, as1) ||
-            cudaFuncSetAttribute(mg_at<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, as1) ||
-            cudaFuncSetAttribute(mg_smooth0_as, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)async_sweep_smem<AsyncSmooth0>()))
-            return PF_ERR_CUDA;
+        // the cp.async sweeps' plane rings (up to ~93 KiB)
+        if (async_attrs<32>() || async_attrs<64>()) return PF_ERR_CUDA;
         dev_done[dev] = 1;
     }
     char* ptr = (char*)region;
@@ -977,6 +1038,33 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
 }
 
 static dim3 cgrid3(const Dims& d) { return dim3((d.nz + 31) / 32, (d.ny + 7) / 8, d.nx); }
+// restriction / prolongation: two coarse planes per thread
+static dim3 cgrid3h(const Dims& c) { return dim3((c.nz + 31) / 32, (c.ny + 7) / 8, (c.nx + 1) / 2); }
+
+// Launchers of the cp.async sweeps for the level's tile width.
+template <int TY, class S>
+static void smooth0_as(const MgLevel& f, const BicgScalars* sc, const AsyncSmooth0<S>& ph,
+                       const char* name, cudaStream_t s) {
+    const dim3 blk(32, 8);
+    const Tiling& tl = TY == kAsTY1 ? f.ta1 : f.tan;
+    if (f.az == 64)
+        PF_LAUNCH(name, s, launch_pdl(mg_smooth0_as<TY, 64, S>, dim3(tiled_grid(tl)), dim3(blk),
+            async_sweep_smem<TY, 64, AsyncSmooth0<S>>(), s, f.d, tl, f.cf, sc, ph));
+    else
+        PF_LAUNCH(name, s, launch_pdl(mg_smooth0_as<TY, 32, S>, dim3(tiled_grid(tl)), dim3(blk),
+            async_sweep_smem<TY, 32, AsyncSmooth0<S>>(), s, f.d, tl, f.cf, sc, ph));
+}
+
+static void smooth_as(const MgLevel& f, const BicgScalars* sc, const AsyncSmooth& ph,
+                      const char* name, cudaStream_t s) {
+    const dim3 blk(32, 8);
+    if (f.az == 64)
+        PF_LAUNCH(name, s, launch_pdl(mg_smooth_as<64>, dim3(tiled_grid(f.ta1)), dim3(blk),
+            async_sweep_smem<kAsTY1, 64, AsyncSmooth>(), s, f.d, f.ta1, f.cf, sc, ph));
+    else
+        PF_LAUNCH(name, s, launch_pdl(mg_smooth_as<32>, dim3(tiled_grid(f.ta1)), dim3(blk),
+            async_sweep_smem<kAsTY1, 32, AsyncSmooth>(), s, f.d, f.ta1, f.cf, sc, ph));
+}
 
 // Restriction from level 0 (whose x and b are set), the levels down to the
 // bottom kernel, and the up-sweep back to level 0's x.
@@ -989,10 +1077,9 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
         const float* bl = l == 0 ? b0 : f.b;
         float* xl = l == 0 ? x0 : f.x;
         if (l > 0) {
-            if (f.kind == kMgSwept && f.d.nz % 32 == 0) {
-                AsyncSmooth0 ph{{f.b}, {nullptr}, f.x, f.wd};
-                PF_LAUNCH("mg_smooth0", s, launch_pdl(mg_smooth0_as, dim3(tiled_grid(f.tl)), dim3(blk),
-                    async_sweep_smem<AsyncSmooth0>(), s, f.d, f.tl, f.cf, sc, ph));
+            if (f.kind == kMgSwept && f.az) {
+                AsyncSmooth0<AsyncPlain> ph{{}, {f.b}, {nullptr}, f.x, f.wd};
+                smooth0_as<kAsTY1>(f, sc, ph, "mg_smooth0", s);
             } else if (f.kind == kMgSwept) {
                 PhaseSmooth0<SrcPlain> ph{};
                 ph.src.b = f.b; ph.x = f.x; ph.wd = f.wd;
@@ -1003,7 +1090,7 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
                     f.d, f.cf, f.wd, f.b, f.x, sc));
             }
         }
-        PF_LAUNCH(l == 0 ? "mg_restrict_l0" : "mg_restrict", s, launch_pdl(mg_restrict, dim3(cgrid3(c.d)), dim3(blk), 0, s,
+        PF_LAUNCH(l == 0 ? "mg_restrict_l0" : "mg_restrict", s, launch_pdl(mg_restrict, dim3(cgrid3h(c.d)), dim3(blk), 0, s,
             f.d, f.cf, bl, xl, c.d, c.b, sc));
     }
     {
@@ -1021,14 +1108,9 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
             const char* np = l == 0 ? "mg_prolong_l0" : "mg_prolong";
             const char* ns = l == 0 ? "mg_smooth_l0" : "mg_smooth";
             PF_LAUNCH(np, s, launch_pdl(mg_prolong_add, dim3(cgrid3(c.d)), dim3(blk), 0, s, f.d, c.d, c.x, xl, sc));
-            if (f.d.nz % 32 == 0) {
-                const size_t sm = async_sweep_smem<AsyncSmooth>();
-                AsyncSmooth a{{xl}, {bl}, f.t, f.wd};
-                PF_LAUNCH(ns, s, launch_pdl(mg_smooth_as, dim3(tiled_grid(f.tl)), dim3(blk), sm, s,
-                                            f.d, f.tl, f.cf, sc, a));
-                AsyncSmooth b{{f.t}, {bl}, xl, f.wd};
-                PF_LAUNCH(ns, s, launch_pdl(mg_smooth_as, dim3(tiled_grid(f.tl)), dim3(blk), sm, s,
-                                            f.d, f.tl, f.cf, sc, b));
+            if (f.az) {
+                smooth_as(f, sc, AsyncSmooth{{xl}, {bl}, f.t, f.wd}, ns, s);
+                smooth_as(f, sc, AsyncSmooth{{f.t}, {bl}, xl, f.wd}, ns, s);
             } else {
                 PhaseSmooth a{xl, bl, f.t, f.wd};
                 PF_LAUNCH(ns, s, launch_pdl(mg_smooth, dim3(tiled_grid(f.tl8)), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc, a));
@@ -1068,33 +1150,42 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
     const int gt = tiled_grid(f.tl), gt8 = tiled_grid(f.tl8);
     float* p_new = P.p[k & 1];
     const float* p_old = P.p[(k & 1) ^ 1];
-    {   // p update fused into the first smoothing pass of M p
+    {   // p update fused into the first smoothing pass of M p (three input
+        // fields: the register sweep beats the cp.async ring here)
         PhaseSmooth0<SrcP> ph{};
         ph.src.res = P.res; ph.src.p_old = p_old; ph.src.v = P.v; ph.src.p_new = p_new;
         ph.x = P.ph; ph.wd = f.wd;
         PF_LAUNCH("mg_smooth0_p", s, launch_pdl(mg_smooth0<SrcP>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, p_new, P.ph, sc, s);
-    const bool as = f.d.nz % 32 == 0;  // cp.async sweep for the single-input phases
-    const size_t sm1 = async_sweep_smem<AsyncAv>();
-    if (as)
-        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<true>, dim3(gt), dim3(blk), sm1, s, f.d, f.tl, f.cf, sc,
-                                         part, P.ph, P.res0, P.v, use_cond, cond));
+    const int ga = tiled_grid(f.ta1);
+    if (f.az == 64)
+        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<64>, dim3(ga), dim3(blk), async_sweep_smem<kAsTY1, 64, AsyncAv>(),
+                                         s, f.d, f.ta1, f.cf, sc, part, P.ph, P.res0, P.v, use_cond, cond));
+    else if (f.az == 32)
+        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<32>, dim3(ga), dim3(blk), async_sweep_smem<kAsTY1, 32, AsyncAv>(),
+                                         s, f.d, f.ta1, f.cf, sc, part, P.ph, P.res0, P.v, use_cond, cond));
     else
-        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<false>, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc,
+        PF_LAUNCH("mg_av", s, launch_pdl(mg_av<0>, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc,
                                          part, P.ph, P.res0, P.v, use_cond, cond));
-    {   // s = res - alpha v fused into the first smoothing pass of M s
+    if (f.az) {  // s = res - alpha v fused into the first smoothing pass of M s
+        AsyncSmooth0<AsyncS> ph{{P.s, 0.0f}, {P.res, P.v}, {nullptr}, P.sh, f.wd};
+        smooth0_as<kAsTYn>(f, sc, ph, "mg_smooth0_s", s);
+    } else {
         PhaseSmooth0<SrcS> ph{};
         ph.src.res = P.res; ph.src.v = P.v; ph.src.s = P.s;
         ph.x = P.sh; ph.wd = f.wd;
         PF_LAUNCH("mg_smooth0_s", s, launch_pdl(mg_smooth0<SrcS>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, P.s, P.sh, sc, s);
-    if (as)
-        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<true>, dim3(gt), dim3(blk), sm1, s, f.d, f.tl, f.cf, sc,
-                                         part, P.sh, P.s, P.t));
+    if (f.az == 64)
+        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<64>, dim3(ga), dim3(blk), async_sweep_smem<kAsTY1, 64, AsyncAt>(),
+                                         s, f.d, f.ta1, f.cf, sc, part, P.sh, P.s, P.t));
+    else if (f.az == 32)
+        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<32>, dim3(ga), dim3(blk), async_sweep_smem<kAsTY1, 32, AsyncAt>(),
+                                         s, f.d, f.ta1, f.cf, sc, part, P.sh, P.s, P.t));
     else
-        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<false>, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc,
+        PF_LAUNCH("mg_at", s, launch_pdl(mg_at<0>, dim3(gt8), dim3(blk), 0, s, f.d, f.tl8, f.cf, sc,
                                          part, P.sh, P.s, P.t));
     PF_LAUNCH("mg_update", s, launch_pdl(mg_update, dim3(pointwise_grid(f.d.n)), dim3(kBlock), 0, s,
         f.d, sc, part, P.e, P.ph, P.sh, P.s, P.t, P.res, P.res0, use_cond, cond));

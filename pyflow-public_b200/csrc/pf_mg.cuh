@@ -22,7 +22,9 @@ struct MgLevel {
     LapCoef<float> cf;  // the scaled operator -vol L with this level's spacing
     float wd;           // omega / diag(A)
     float *b, *x, *t;   // right-hand side, iterate, smoothing buffer
-    Tiling tl, tl8;  // tilings of the 4- and 8-row sweep phases
+    Tiling tl, tl8;     // tilings of the 4- and 8-row register sweeps
+    int az;             // cp.async sweep tile width (64, 32; 0: none, nz not a multiple of 32)
+    Tiling ta1, tan;    // cp.async tilings: one input field (32 rows), several (16 rows)
     int kind;
     double cq[3];       // vol / h_q^2: the operator's off-diagonal magnitudes
 };

@@ -297,19 +297,23 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // dynamic shared memory of the tiled stage kernel
-template <typename TI, typename TA, int MODE>
+template <typename T, typename TI, typename TA, int MODE>
 struct RhsSmem {
+    // FP64 input planes of an FP32 stage (the state u of the first stage or
+    // of Euler's k) are staged as FP64 and converted to T once per position
+    static constexpr bool kConv = sizeof(TI) > sizeof(T);
     static constexpr bool kU = MODE == kModeFirst || MODE == kModeMid || MODE == kModeLast;
     static constexpr bool kA = MODE == kModeMid || MODE == kModeLast;
-    static constexpr size_t kEu = kU ? 2 * 3 * kRhsCells * sizeof(double) : 0;  // [2][3][cells]
-    static constexpr size_t kRing = 4 * 3 * kRhsPos * sizeof(TI);            // [4][3][pos]
-    static constexpr size_t kEa = kA ? 2 * 3 * kRhsCells * sizeof(TA) : 0;      // [2][3][cells]
-    static constexpr size_t bytes = kEu + kRing + kEa;
+    static constexpr size_t kEu = (kU && !kConv) ? 2 * 3 * kRhsCells * sizeof(double) : 0;  // [2][3][cells]
+    static constexpr size_t kStg = kConv ? 4 * 3 * kRhsPos * sizeof(TI) : 0;             // [4][3][pos]
+    static constexpr size_t kRing = 4 * 3 * kRhsPos * (kConv ? sizeof(T) : sizeof(TI)); // [4][3][pos]
+    static constexpr size_t kEa = kA ? 2 * 3 * kRhsCells * sizeof(TA) : 0;               // [2][3][cells]
+    static constexpr size_t bytes = kEu + kStg + kRing + kEa;
 };
 
 template <typename T, typename TI>
 struct SmemSrc {
-    const TI* ring;
+    const TI* ring;  // [4][3][kRhsPos]
     int s0, s1, s2;  // slots of planes i-1, i, i+1
     int y, z;        // the cell in the halo-extended tile
     __device__ const TI* f(int fld, int di) const {
@@ -323,6 +327,121 @@ struct SmemSrc {
     __device__ T sfs(int, int, int, int) const { return T(0); }
 };
 
+// The tiled stage for an FP64 input of an FP32 stage (first RK4 stage,
+// Euler's k): plane x's FP64 values arrive by cp.async in stg slot
+// (x - i0 + 1) & 3, and the thread that copied a position converts it into
+// the FP32 ring slot of the same number once the copy has landed (a thread's
+// own copies need no barrier).  Plane i + 2 is converted after plane i is
+// computed, so one barrier per plane orders conversion and use; the first
+// stage's FP64 u of the owned cells comes from plane i's stg slot.
+template <typename T, typename TI, typename TS, typename TA, int MODE>
+__device__ __forceinline__ void
+rhs_stage_tiled_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
+                     double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+                     TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
+                     TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
+                     double hdt) {
+    static_assert(MODE == kModeFirst || MODE == kModeK, "FP64 input planes: first stage or k");
+    using SM = RhsSmem<T, TI, TA, MODE>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    TI* stg = reinterpret_cast<TI*>(smraw);
+    T* ring = reinterpret_cast<T*>(smraw + SM::kStg);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const long long plane = (long long)d.ny * d.nz;
+    const TI* fld[3] = {a.u, a.v, a.w};
+    TA* A[3] = {au, av, aw};
+    TS* S[3] = {su, sv, sw};
+    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+        const int tz = (int)(t % tl.ntz);
+        const long long rr = t / tl.ntz;
+        const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
+        const int k0 = tz * 32, j0 = tyy * kRhsTY, i0 = txx * tl.xc;
+        const int i1 = min(i0 + tl.xc, d.nx);
+        const int ez = min(32, d.nz - k0), ey = min(kRhsTY, d.ny - j0);
+        long long goff[kRhsPPT];
+        int soff[kRhsPPT];
+        bool pv[kRhsPPT];
+#pragma unroll
+        for (int p = 0; p < kRhsPPT; ++p) {
+            const int pos = tid + 256 * p;
+            pv[p] = pos < kRhsPos;
+            const int yy = pv[p] ? pos / kRhsSZ : 0, zz = pv[p] ? pos - yy * kRhsSZ : 0;
+            goff[p] = (long long)pmod(j0 + yy - 1, d.ny) * d.nz + pmod(k0 + zz - 1, d.nz);
+            soff[p] = yy * kRhsSZ + zz;
+        }
+        bool cv[2];
+        long long coff[2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int jl = ty + 8 * r;
+            cv[r] = tx < ez && jl < ey;
+            coff[r] = (long long)(j0 + jl) * d.nz + k0 + tx;
+        }
+        auto slot = [&](int x) { return (x - i0 + 1) & 3; };
+        auto load_stg = [&](int x) {
+            const long long base = (long long)pmod(x, d.nx) * plane;
+            TI* dst = stg + slot(x) * 3 * kRhsPos;
+#pragma unroll
+            for (int f = 0; f < 3; ++f)
+#pragma unroll
+                for (int p = 0; p < kRhsPPT; ++p)
+                    if (pv[p]) cp_async<sizeof(TI)>(dst + f * kRhsPos + soff[p], fld[f] + base + goff[p]);
+        };
+        auto convert = [&](int x) {
+            const TI* src = stg + slot(x) * 3 * kRhsPos;
+            T* dst = ring + slot(x) * 3 * kRhsPos;
+#pragma unroll
+            for (int f = 0; f < 3; ++f)
+#pragma unroll
+                for (int p = 0; p < kRhsPPT; ++p)
+                    if (pv[p]) dst[f * kRhsPos + soff[p]] = T(src[f * kRhsPos + soff[p]]);
+        };
+        load_stg(i0 - 1);
+        load_stg(i0);
+        load_stg(i0 + 1);
+        cp_async_commit();
+        if (i0 + 1 < i1) load_stg(i0 + 2);
+        cp_async_commit();
+        cp_async_wait_groups<1>();
+        convert(i0 - 1);
+        convert(i0);
+        convert(i0 + 1);
+        __syncthreads();
+        for (int i = i0; i < i1; ++i) {
+            const int c = i - i0;
+            const int s0 = c & 3, s1 = (c + 1) & 3, s2 = (c + 2) & 3;
+            if (i + 2 < i1) load_stg(i + 3);
+            cp_async_commit();
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (!cv[r]) continue;
+                const int jl = ty + 8 * r;
+                SmemSrc<T, T> src{ring, s0, s1, s2, jl + 1, tx + 1};
+                T k3[3];
+                rhs_core<T>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false, k3[0], k3[1], k3[2]);
+                const long long q = (long long)i * plane + coff[r];
+                const int pc = (jl + 1) * kRhsSZ + tx + 1;
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                    const T kf = k3[f];
+                    if (MODE == kModeFirst) {
+                        // ZAXPY(h, k, u) = h*k + u (src/data/state.py:157-165)
+                        S[f][q] = TS(hdt * double(kf) + double(stg[(s1 * 3 + f) * kRhsPos + pc]));
+                        A[f][q] = TA(kf);
+                    } else {  // kModeK
+                        A[f][q] = TA(kf);
+                    }
+                }
+            }
+            cp_async_wait_groups<1>();
+            if (i + 1 < i1) convert(i + 2);
+            __syncthreads();
+        }
+        cp_async_wait_all();
+        __syncthreads();
+    }
+}
+
 template <typename T, typename TI, typename TS, typename TA, int MODE>
 __global__ void __launch_bounds__(256, 2)
 rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
@@ -330,7 +449,11 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
                 TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
                 TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
                 double hdt, double c6) {
-    using SM = RhsSmem<TI, TA, MODE>;
+    using SM = RhsSmem<T, TI, TA, MODE>;
+    if constexpr (SM::kConv) {
+        rhs_stage_tiled_conv<T, TI, TS, TA, MODE>(d, tl, a, u, v, w, su, sv, sw, au, av, aw, hdt);
+        return;
+    }
     extern __shared__ __align__(16) unsigned char smraw[];
     double* eu = reinterpret_cast<double*>(smraw);
     TI* ring = reinterpret_cast<TI*>(smraw + SM::kEu);
@@ -449,11 +572,11 @@ static cudaError_t tiled_prepare() {
     if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(
         rhs_stage_tiled<T, TI, T, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int)RhsSmem<TI, T, MODE>::bytes);
+        (int)RhsSmem<T, TI, T, MODE>::bytes);
     // a shared-memory carveout just large enough for two blocks per SM (the
     // rest stays L1): percent of the SM's 228 KiB
     if (e == cudaSuccess) {
-        const size_t two = 2 * (RhsSmem<TI, T, MODE>::bytes + 1024);
+        const size_t two = 2 * (RhsSmem<T, TI, T, MODE>::bytes + 1024);
         const int pct = (int)std::min<size_t>(100, (two * 100 + 228 * 1024 - 1) / (228 * 1024));
         e = cudaFuncSetAttribute(rhs_stage_tiled<T, TI, T, T, MODE>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, pct);
@@ -530,7 +653,7 @@ static cudaError_t stage(const char* name, const Dims& d, const RhsArgs<T, TI>& 
         const cudaError_t e = tiled_prepare<T, TI, MODE>();
         if (e != cudaSuccess) return e;
         PF_LAUNCH(name, s, rhs_stage_tiled<T, TI, T, T, MODE><<<tiled_grid(tl), blk,
-                                                              RhsSmem<TI, T, MODE>::bytes, s>>>(
+                                                              RhsSmem<T, TI, T, MODE>::bytes, s>>>(
             d, tl, a, u, v, w, su, sv, sw, acc, acc + n, acc + 2 * n, hdt, c6));
     } else {
         PF_LAUNCH(name, s, rhs_stage_kernel<T, TI, T, T, MODE><<<cell_grid(d), blk, 0, s>>>(

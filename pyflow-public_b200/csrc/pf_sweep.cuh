@@ -66,9 +66,9 @@ static inline int num_sms() {
     return n;
 }
 
-static inline Tiling make_tiling(const Dims& d, int ty) {
+static inline Tiling make_tiling(const Dims& d, int ty, int tz = 32) {
     Tiling t;
-    t.ntz = (d.nz + 31) / 32;
+    t.ntz = (d.nz + tz - 1) / tz;
     t.nty = (d.ny + ty - 1) / ty;
     const long long yz = (long long)t.ntz * t.nty;
     // split x so the tiles fill the resident blocks (2 per SM) in whole
@@ -224,26 +224,37 @@ __device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
 
 // --------------------------------------------------------------------------
 // FP32 sweep with a cp.async pipeline (grids whose z extent is a multiple of
-// 32).  Block 32 x 8 threads, tile 32 (z) x 32 (y) x xc (x); the input planes
-// (with a one-cell y/z halo) arrive in shared memory DEP planes ahead of use
-// through 16-byte cp.async copies (4-byte copies for the z-halo columns), so
-// no thread holds prefetched data in registers.  The phase object provides
-//   NR == 1 input field rf[0] and NE (0 or 1) epilogue fields ef[],
-//   float op(float raw)          -- the stencil operand of a cell,
-//   epi(q, op_c, A op, raw_c, e) -- consumes an owned cell (e: NE values).
-// Dynamic shared memory: async_sweep_smem<Ph>() bytes.
+// TZ).  Block 32 x 8 threads, tile TZ (z, 32 or 64) x TY (y) x xc (x); the
+// input planes (with a one-cell y/z halo) arrive in shared memory kAsyncDep
+// planes ahead of use through 16-byte cp.async copies (the z halos as the
+// 16-byte chunks that end and start next to the tile), so no thread holds
+// prefetched data in registers.  Wider z tiles make every row copy a longer
+// contiguous run of the plane.  The phase object provides
+//   NR input fields rf[] and NE (0 or 1) epilogue fields ef[],
+//   float op(const float* raw)  -- the stencil operand of a cell from its NR
+//                                  raw values,
+//   epi(q, op_c, A op, e)       -- consumes an owned cell (e: NE values).
+// Dynamic shared memory: async_sweep_smem<TY, TZ, Ph>() bytes.
 // --------------------------------------------------------------------------
-constexpr int kAsyncTY = 32;         // tile rows
-constexpr int kAsyncSZ = 40;         // smem row stride: halo at 3 and 36, cells at 4..35
-constexpr int kAsyncDep = 2;         // planes in flight ahead of use
-constexpr int kAsyncRS = kAsyncDep + 4;
-constexpr int kAsyncES = kAsyncDep + 2;
-constexpr int kAsyncRPos = (kAsyncTY + 2) * kAsyncSZ;
-constexpr int kAsyncEPos = kAsyncTY * 32;
+constexpr int kAsyncDep = 2;  // planes in flight ahead of use
 
-template <class Ph>
+template <int TY, int TZ, class Ph>
+struct AsyncGeom {
+    static_assert(TZ == 32 || TZ == 64, "tile width");
+    static_assert(TY % 8 == 0, "tile height");
+    static constexpr int SZ = TZ + 8;          // row stride: halo chunks at 0..3 and TZ+4..TZ+7
+    static constexpr int RS = kAsyncDep + 4;   // raw plane slots (3 in use, DEP + 1 in flight)
+    static constexpr int ES = kAsyncDep + 2;   // epilogue plane slots
+    static constexpr int RPos = (TY + 2) * SZ;
+    static constexpr int EPos = TY * TZ;
+    static constexpr int NCH = TZ / 4 + 2;     // 16-byte chunks per raw row
+    static constexpr size_t bytes =
+        (size_t)(RS * Ph::NR * RPos + ES * Ph::NE * EPos) * sizeof(float);
+};
+
+template <int TY, int TZ, class Ph>
 constexpr size_t async_sweep_smem() {
-    return (size_t)(kAsyncRS * kAsyncRPos + kAsyncES * Ph::NE * kAsyncEPos) * sizeof(float);
+    return AsyncGeom<TY, TZ, Ph>::bytes;
 }
 
 template <int BYTES>
@@ -262,54 +273,55 @@ __device__ __forceinline__ void cp_async_wait_groups() {
     asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
 }
 
-template <class Ph>
+template <int TY, int TZ, class Ph>
 __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
                                             const LapCoef<float>& cf, Ph& ph) {
-    constexpr int TY = kAsyncTY, SZ = kAsyncSZ, RS = kAsyncRS, ES = kAsyncES;
+    using G = AsyncGeom<TY, TZ, Ph>;
+    constexpr int SZ = G::SZ, RS = G::RS, ES = G::ES, RPos = G::RPos, EPos = G::EPos;
+    constexpr int NR = Ph::NR, NE = Ph::NE, NCH = G::NCH;
     extern __shared__ __align__(16) float async_sm[];
-    float* rr = async_sm;                    // [RS][RPos]
-    float* ee = async_sm + RS * kAsyncRPos;  // [ES][NE][EPos]
+    float* rr = async_sm;                    // [RS][NR][RPos]
+    float* ee = async_sm + RS * NR * RPos;   // [ES][NE][EPos]
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const long long plane = (long long)d.ny * d.nz;
-    const float* xr = ph.rf[0];
     for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int tz = (int)(t % tl.ntz);
         const long long r2 = t / tl.ntz;
         const int tyy = (int)(r2 % tl.nty), txx = (int)(r2 / tl.nty);
-        const int k0 = tz * 32, j0 = tyy * TY, i0 = txx * tl.xc;
+        const int k0 = tz * TZ, j0 = tyy * TY, i0 = txx * tl.xc;
         const int i1 = min(i0 + tl.xc, d.nx);
         const int ey = min(TY, d.ny - j0);
         // a single wrap suffices for the halo rows unless the grid is
-        // shorter than a tile in y (nz is a multiple of 32, so z needs one)
+        // shorter than a tile in y; nz is a multiple of TZ >= 32, so the
+        // halo chunks k0 - 4 and k0 + TZ need one
         const bool short_y = d.ny <= TY;
         auto yrow = [&](int yy) {
             const int j = j0 + yy - 1;
             return short_y ? pmod(j, d.ny) : wrap(j, d.ny);
         };
-        const int kl = wrap(k0 - 1, d.nz), kr = wrap(k0 + 32, d.nz);
+        const int kl = wrap(k0 - 4, d.nz), kr = wrap(k0 + TZ, d.nz);
         auto load_raw = [&](int xp, int slot) {
             const long long base = (long long)pmod(xp, d.nx) * plane;
-            float* dst = rr + slot * kAsyncRPos;
-            for (int p = tid; p < (TY + 2) * 8; p += 256) {
-                const int yy = p >> 3, ch = p & 7;
-                cp_async_sm<16>(dst + yy * SZ + 4 + 4 * ch,
-                                xr + base + (long long)yrow(yy) * d.nz + k0 + 4 * ch);
-            }
-            for (int p = tid; p < (TY + 2) * 2; p += 256) {
-                const int yy = p >> 1, side = p & 1;
-                cp_async_sm<4>(dst + yy * SZ + (side ? 36 : 3),
-                               xr + base + (long long)yrow(yy) * d.nz + (side ? kr : kl));
+#pragma unroll
+            for (int f = 0; f < NR; ++f) {
+                float* dst = rr + (slot * NR + f) * RPos;
+                for (int p = tid; p < (TY + 2) * NCH; p += 256) {
+                    const int yy = p / NCH, ch = p - yy * NCH;
+                    const int k = ch == 0 ? kl : (ch == NCH - 1 ? kr : k0 + 4 * (ch - 1));
+                    cp_async_sm<16>(dst + yy * SZ + 4 * ch,
+                                    ph.rf[f] + base + (long long)yrow(yy) * d.nz + k);
+                }
             }
         };
         auto load_ext = [&](int xp, int slot) {
             const long long base = (long long)xp * plane;
 #pragma unroll
-            for (int f = 0; f < Ph::NE; ++f) {
-                float* dst = ee + (slot * Ph::NE + f) * kAsyncEPos;
-                for (int p = tid; p < TY * 8; p += 256) {
-                    const int yy = p >> 3, ch = p & 7;
+            for (int f = 0; f < NE; ++f) {
+                float* dst = ee + (slot * NE + f) * EPos;
+                for (int p = tid; p < TY * (TZ / 4); p += 256) {
+                    const int yy = p / (TZ / 4), ch = p - yy * (TZ / 4);
                     if (yy < ey)
-                        cp_async_sm<16>(dst + yy * 32 + 4 * ch,
+                        cp_async_sm<16>(dst + yy * TZ + 4 * ch,
                                         ph.ef[f] + base + (long long)(j0 + yy) * d.nz + k0 + 4 * ch);
                 }
             }
@@ -334,32 +346,41 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
                 load_ext(i + kAsyncDep + 1, eslot(i + kAsyncDep + 1));
             }
             cp_async_commit_group();
-            const float* pm = rr + rslot(i - 1) * kAsyncRPos;
-            const float* pc = rr + rslot(i) * kAsyncRPos;
-            const float* pp = rr + rslot(i + 1) * kAsyncRPos;
-            const float* eb = ee + eslot(i) * Ph::NE * kAsyncEPos;
+            const float* pm = rr + rslot(i - 1) * NR * RPos;
+            const float* pc = rr + rslot(i) * NR * RPos;
+            const float* pp = rr + rslot(i + 1) * NR * RPos;
+            const float* eb = ee + eslot(i) * NE * EPos;
             const long long bi = (long long)i * plane;
+            auto opat = [&](const float* pl, int c) {
+                float r[NR];
+#pragma unroll
+                for (int f = 0; f < NR; ++f) r[f] = pl[f * RPos + c];
+                return ph.op(r);
+            };
 #pragma unroll
             for (int r = 0; r < TY / 8; ++r) {
                 const int yl = ty + 8 * r;
                 if (yl >= ey) continue;
-                const int c = (yl + 1) * SZ + tx + 4;
-                const float rc = pc[c];
-                const float oc = ph.op(rc);
-                float b = 0.0f;
-                b += ph.op(pm[c]) * cf.c[0][0];
-                b += oc * cf.c[0][1];
-                b += ph.op(pp[c]) * cf.c[0][2];
-                b += ph.op(pc[c - SZ]) * cf.c[1][0];
-                b += oc * cf.c[1][1];
-                b += ph.op(pc[c + SZ]) * cf.c[1][2];
-                b += ph.op(pc[c - 1]) * cf.c[2][0];
-                b += oc * cf.c[2][1];
-                b += ph.op(pc[c + 1]) * cf.c[2][2];
-                float e[Ph::NE > 0 ? Ph::NE : 1];
 #pragma unroll
-                for (int f = 0; f < Ph::NE; ++f) e[f] = eb[f * kAsyncEPos + yl * 32 + tx];
-                ph.epi(bi + (long long)(j0 + yl) * d.nz + k0 + tx, oc, b, rc, e);
+                for (int v = 0; v < TZ / 32; ++v) {
+                    const int zl = tx + 32 * v;
+                    const int c = (yl + 1) * SZ + zl + 4;
+                    const float oc = opat(pc, c);
+                    float b = 0.0f;
+                    b += opat(pm, c) * cf.c[0][0];
+                    b += oc * cf.c[0][1];
+                    b += opat(pp, c) * cf.c[0][2];
+                    b += opat(pc, c - SZ) * cf.c[1][0];
+                    b += oc * cf.c[1][1];
+                    b += opat(pc, c + SZ) * cf.c[1][2];
+                    b += opat(pc, c - 1) * cf.c[2][0];
+                    b += oc * cf.c[2][1];
+                    b += opat(pc, c + 1) * cf.c[2][2];
+                    float e[NE > 0 ? NE : 1];
+#pragma unroll
+                    for (int f = 0; f < NE; ++f) e[f] = eb[f * EPos + yl * TZ + zl];
+                    ph.epi(bi + (long long)(j0 + yl) * d.nz + k0 + zl, oc, b, e);
+                }
             }
         }
         cp_async_wait_groups<0>();
