@@ -275,7 +275,8 @@ mg_smooth_as(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc, AsyncS
 // 8-byte load, and the z halos 2K - 1, 2K + 2 come from the neighbouring
 // lanes (loaded only at the warp's edges and the grid's periodic wrap).
 // Lanes past c.nz compute on a clamped K (so every lane takes part in the
-// shuffles) and store nothing.  Needs fine dims = 2 x coarse dims.
+// shuffles) and store nothing.  A x in fused multiply-adds with one centre
+// coefficient, as the cp.async sweeps.  Needs fine dims = 2 x coarse dims.
 __global__ void __launch_bounds__(256)
 mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
             const float* __restrict__ x, Dims c, float* __restrict__ bc,
@@ -294,6 +295,7 @@ mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
 #pragma unroll
     for (int a = 0; a < 4; ++a) jb[a] = (long long)wrap(2 * J - 1 + a, f.ny) * f.nz;
     const int kl = wrap(2 * Kc - 1, f.nz), kr = wrap(2 * Kc + 2, f.nz);
+    const float cen = (cf.c[0][1] + cf.c[1][1]) + cf.c[2][1];
     // x pairs (2K, 2K+1) of fine rows (a, bb); the four corner rows are unused
     float2 xp[6][4];
 #pragma unroll
@@ -320,17 +322,13 @@ mg_restrict(Dims f, LapCoef<float> cf, const float* __restrict__ b,
 #pragma unroll
                 for (int cc = 1; cc < 3; ++cc) {
                     auto at = [&](int aa, int b2) { return cc == 1 ? xp[aa][b2].x : xp[aa][b2].y; };
-                    const float xc = z[cc];
-                    float ax = 0.0f;
-                    ax += at(a - 1, bb) * cf.c[0][0];
-                    ax += xc * cf.c[0][1];
-                    ax += at(a + 1, bb) * cf.c[0][2];
-                    ax += at(a, bb - 1) * cf.c[1][0];
-                    ax += xc * cf.c[1][1];
-                    ax += at(a, bb + 1) * cf.c[1][2];
-                    ax += z[cc - 1] * cf.c[2][0];
-                    ax += xc * cf.c[2][1];
-                    ax += z[cc + 1] * cf.c[2][2];
+                    float ax = z[cc] * cen;
+                    ax = fmaf(at(a - 1, bb), cf.c[0][0], ax);
+                    ax = fmaf(at(a + 1, bb), cf.c[0][2], ax);
+                    ax = fmaf(at(a, bb - 1), cf.c[1][0], ax);
+                    ax = fmaf(at(a, bb + 1), cf.c[1][2], ax);
+                    ax = fmaf(z[cc - 1], cf.c[2][0], ax);
+                    ax = fmaf(z[cc + 1], cf.c[2][2], ax);
                     sum += (cc == 1 ? bv.x : bv.y) - ax;
                 }
             }

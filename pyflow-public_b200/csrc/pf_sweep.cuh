@@ -229,7 +229,11 @@ __device__ __forceinline__ void sweep(const Dims& d, const Tiling& tl,
 // planes ahead of use through 16-byte cp.async copies (the z halos as the
 // 16-byte chunks that end and start next to the tile), so no thread holds
 // prefetched data in registers.  Wider z tiles make every row copy a longer
-// contiguous run of the plane.  The phase object provides
+// contiguous run of the plane.  Each thread's copy offsets are fixed per tile
+// and computed once.  The stencil is evaluated with fused multiply-adds and
+// one combined centre coefficient (these sweeps serve only the FP32
+// multigrid preconditioner, whose rounding is its own).  The phase object
+// provides
 //   NR input fields rf[] and NE (0 or 1) epilogue fields ef[],
 //   float op(const float* raw)  -- the stencil operand of a cell from its NR
 //                                  raw values,
@@ -279,11 +283,15 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
     using G = AsyncGeom<TY, TZ, Ph>;
     constexpr int SZ = G::SZ, RS = G::RS, ES = G::ES, RPos = G::RPos, EPos = G::EPos;
     constexpr int NR = Ph::NR, NE = Ph::NE, NCH = G::NCH;
+    constexpr int RCH = (TY + 2) * NCH, RPT = (RCH + 255) / 256;    // raw chunks per plane, per thread
+    constexpr int ECH = TY * (TZ / 4), EPT = (ECH + 255) / 256;     // epilogue chunks
     extern __shared__ __align__(16) float async_sm[];
     float* rr = async_sm;                    // [RS][NR][RPos]
     float* ee = async_sm + RS * NR * RPos;   // [ES][NE][EPos]
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const long long plane = (long long)d.ny * d.nz;
+    // the centre coefficient of the three directions, applied once
+    const float cc = (cf.c[0][1] + cf.c[1][1]) + cf.c[2][1];
     for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
         const int tz = (int)(t % tl.ntz);
         const long long r2 = t / tl.ntz;
@@ -291,26 +299,43 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
         const int k0 = tz * TZ, j0 = tyy * TY, i0 = txx * tl.xc;
         const int i1 = min(i0 + tl.xc, d.nx);
         const int ey = min(TY, d.ny - j0);
-        // a single wrap suffices for the halo rows unless the grid is
-        // shorter than a tile in y; nz is a multiple of TZ >= 32, so the
-        // halo chunks k0 - 4 and k0 + TZ need one
-        const bool short_y = d.ny <= TY;
-        auto yrow = [&](int yy) {
-            const int j = j0 + yy - 1;
-            return short_y ? pmod(j, d.ny) : wrap(j, d.ny);
-        };
+        // This thread's copies are the same in every plane of the tile:
+        // in-plane source offsets and shared-memory positions, computed once.
+        // A single wrap suffices for the halo rows unless the grid is
+        // shorter than a tile in y; nz is a multiple of TZ >= 32, so the halo
+        // chunks k0 - 4 and k0 + TZ need one.
         const int kl = wrap(k0 - 4, d.nz), kr = wrap(k0 + TZ, d.nz);
+        long long rg[RPT], eg[EPT];
+        int rs[RPT], es[EPT];
+        bool rv[RPT], ev[EPT];
+#pragma unroll
+        for (int m = 0; m < RPT; ++m) {
+            const int p = tid + 256 * m;
+            rv[m] = p < RCH;
+            const int yy = rv[m] ? p / NCH : 0, ch = rv[m] ? p - yy * NCH : 0;
+            const int j = j0 + yy - 1;
+            const int jj = d.ny <= TY ? pmod(j, d.ny) : wrap(j, d.ny);
+            const int k = ch == 0 ? kl : (ch == NCH - 1 ? kr : k0 + 4 * (ch - 1));
+            rg[m] = (long long)jj * d.nz + k;
+            rs[m] = yy * SZ + 4 * ch;
+        }
+#pragma unroll
+        for (int m = 0; m < EPT; ++m) {
+            const int p = tid + 256 * m;
+            const int yy = p / (TZ / 4), ch = p - yy * (TZ / 4);
+            ev[m] = p < ECH && yy < ey;
+            eg[m] = (long long)(j0 + yy) * d.nz + k0 + 4 * ch;
+            es[m] = yy * TZ + 4 * ch;
+        }
         auto load_raw = [&](int xp, int slot) {
             const long long base = (long long)pmod(xp, d.nx) * plane;
 #pragma unroll
             for (int f = 0; f < NR; ++f) {
                 float* dst = rr + (slot * NR + f) * RPos;
-                for (int p = tid; p < (TY + 2) * NCH; p += 256) {
-                    const int yy = p / NCH, ch = p - yy * NCH;
-                    const int k = ch == 0 ? kl : (ch == NCH - 1 ? kr : k0 + 4 * (ch - 1));
-                    cp_async_sm<16>(dst + yy * SZ + 4 * ch,
-                                    ph.rf[f] + base + (long long)yrow(yy) * d.nz + k);
-                }
+                const float* src = ph.rf[f] + base;
+#pragma unroll
+                for (int m = 0; m < RPT; ++m)
+                    if (rv[m]) cp_async_sm<16>(dst + rs[m], src + rg[m]);
             }
         };
         auto load_ext = [&](int xp, int slot) {
@@ -318,12 +343,10 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
 #pragma unroll
             for (int f = 0; f < NE; ++f) {
                 float* dst = ee + (slot * NE + f) * EPos;
-                for (int p = tid; p < TY * (TZ / 4); p += 256) {
-                    const int yy = p / (TZ / 4), ch = p - yy * (TZ / 4);
-                    if (yy < ey)
-                        cp_async_sm<16>(dst + yy * TZ + 4 * ch,
-                                        ph.ef[f] + base + (long long)(j0 + yy) * d.nz + k0 + 4 * ch);
-                }
+                const float* src = ph.ef[f] + base;
+#pragma unroll
+                for (int m = 0; m < EPT; ++m)
+                    if (ev[m]) cp_async_sm<16>(dst + es[m], src + eg[m]);
             }
         };
         auto rslot = [&](int xp) { return (xp - i0 + 1 + 4 * RS) % RS; };
@@ -338,6 +361,7 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
             if (i0 + a < i1) { load_raw(i0 + a + 1, rslot(i0 + a + 1)); load_ext(i0 + a, eslot(i0 + a)); }
             cp_async_commit_group();
         }
+        const long long orow = (long long)(j0 + ty) * d.nz + k0 + tx;
         for (int i = i0; i < i1; ++i) {
             cp_async_wait_groups<kAsyncDep>();
             __syncthreads();
@@ -350,7 +374,7 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
             const float* pc = rr + rslot(i) * NR * RPos;
             const float* pp = rr + rslot(i + 1) * NR * RPos;
             const float* eb = ee + eslot(i) * NE * EPos;
-            const long long bi = (long long)i * plane;
+            const long long bi = (long long)i * plane + orow;
             auto opat = [&](const float* pl, int c) {
                 float r[NR];
 #pragma unroll
@@ -366,20 +390,17 @@ __device__ __forceinline__ void sweep_async(const Dims& d, const Tiling& tl,
                     const int zl = tx + 32 * v;
                     const int c = (yl + 1) * SZ + zl + 4;
                     const float oc = opat(pc, c);
-                    float b = 0.0f;
-                    b += opat(pm, c) * cf.c[0][0];
-                    b += oc * cf.c[0][1];
-                    b += opat(pp, c) * cf.c[0][2];
-                    b += opat(pc, c - SZ) * cf.c[1][0];
-                    b += oc * cf.c[1][1];
-                    b += opat(pc, c + SZ) * cf.c[1][2];
-                    b += opat(pc, c - 1) * cf.c[2][0];
-                    b += oc * cf.c[2][1];
-                    b += opat(pc, c + 1) * cf.c[2][2];
+                    float b = oc * cc;
+                    b = fmaf(opat(pm, c), cf.c[0][0], b);
+                    b = fmaf(opat(pp, c), cf.c[0][2], b);
+                    b = fmaf(opat(pc, c - SZ), cf.c[1][0], b);
+                    b = fmaf(opat(pc, c + SZ), cf.c[1][2], b);
+                    b = fmaf(opat(pc, c - 1), cf.c[2][0], b);
+                    b = fmaf(opat(pc, c + 1), cf.c[2][2], b);
                     float e[NE > 0 ? NE : 1];
 #pragma unroll
                     for (int f = 0; f < NE; ++f) e[f] = eb[f * EPos + yl * TZ + zl];
-                    ph.epi(bi + (long long)(j0 + yl) * d.nz + k0 + zl, oc, b, e);
+                    ph.epi(bi + (long long)(8 * r) * d.nz + 32 * v, oc, b, e);
                 }
             }
         }
