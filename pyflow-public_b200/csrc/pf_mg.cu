@@ -37,6 +37,8 @@
 // finished by the last block (fixed order).  Scalars stay on the device.
 #include <cmath>
 
+#include <cooperative_groups.h>
+
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
 #include "pf_mg.cuh"
@@ -571,28 +573,23 @@ __device__ __forceinline__ void decode(int q, const Dims& d, float inv_p, float 
     k = r - j * d.nz;
 }
 
-__global__ void __launch_bounds__(kBottomThreads)
-mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
-          const BicgScalars* sc) {
-    pdl_wait();
-    if (sc->done) return;
-    extern __shared__ float sm[];
+// The coarsest pseudo-inverse (<= 64 x 64) into shared memory.
+__device__ __forceinline__ void bottom_load_pinv(const MgBottom& P, float* sm) {
+    if (!P.pinv) return;
+    const int last = P.nlev - 1;
+    const int nc = (int)P.d[last].n;
+    float* pv = sm + P.off[last] + 3 * nc;
+    for (int q = threadIdx.x; q < nc * nc; q += blockDim.x) pv[q] = __ldg(P.pinv + q);
+}
+
+// One V-cycle over the levels of P, all in this CTA's shared memory `sm`:
+// the first level's b is in place on entry (and the pseudo-inverse, if any);
+// its x is in place on exit.  Block-wide barriers only.
+__device__ void bottom_cycle(const MgBottom& P, float* sm) {
     __shared__ double shd[32];
     __shared__ float mean_s;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int last = P.nlev - 1;
-    {
-        const int n = (int)P.d[0].n;
-        float* b = sm + P.off[0];
-        for (int q = tid; q < n; q += nt) b[q] = gb[q];
-        // the coarsest pseudo-inverse (<= 64 x 64) into shared memory too
-        if (P.pinv) {
-            const int nc = (int)P.d[last].n;
-            float* pv = sm + P.off[last] + 3 * nc;
-            for (int q = tid; q < nc * nc; q += nt) pv[q] = __ldg(P.pinv + q);
-        }
-    }
-    __syncthreads();
     // down: pre-smooth from zero, restrict
     for (int l = 0; l < last; ++l) {
         const Dims d = P.d[l], c = P.d[l + 1];
@@ -715,10 +712,226 @@ mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
         }
         __syncthreads();
     }
-    {
-        const int n = (int)P.d[0].n;
-        const float* x = sm + P.off[0] + n;
-        for (int q = tid; q < n; q += nt) gx[q] = x[q];
+}
+
+__global__ void __launch_bounds__(kBottomThreads)
+mg_bottom(MgBottom P, const float* __restrict__ gb, float* __restrict__ gx,
+          const BicgScalars* sc) {
+    pdl_wait();
+    if (sc->done) return;
+    extern __shared__ float sm[];
+    const int n = (int)P.d[0].n;
+    float* b = sm + P.off[0];
+    for (int q = threadIdx.x; q < n; q += blockDim.x) b[q] = gb[q];
+    bottom_load_pinv(P, sm);
+    __syncthreads();
+    bottom_cycle(P, sm);
+    const float* x = sm + P.off[0] + n;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) gx[q] = x[q];
+}
+
+// ------------------------------------------------- cluster bottom
+// Levels of at most kMgClusterMax cells whose x extent divides among the
+// kClusterCtas CTAs of one thread-block cluster, together with the bottom
+// levels below them, run as ONE launch: each CTA keeps its x planes of b, x
+// and t of every split level in its shared memory and reads the neighbouring
+// CTAs' boundary planes through distributed shared memory (a per-CTA table
+// maps every plane of every split level to the owner's shared memory); the
+// hardware cluster barrier separates the phases.  The levels below the split
+// ones live in CTA 0, which runs bottom_cycle on them while the other CTAs
+// wait at the barrier.  Every operation is the one the per-level global
+// kernels perform (same arithmetic, same order): smoothing as mg_smooth0_pw
+// and mg_smooth_pw, restriction as mg_restrict, prolongation as prolong_at.
+struct MgCluster {
+    int ns;                               // split levels
+    Dims d[kMgMaxLevels];
+    LapCoef<float> cf[kMgMaxLevels];
+    float wd[kMgMaxLevels];
+    int pp[kMgMaxLevels];                 // x planes per CTA
+    float inv_p[kMgMaxLevels];            // 1 / (ny nz), 1 / nz: decode of plane-blocked indices
+    float inv_z[kMgMaxLevels];
+    int off[kMgMaxLevels];                // float offset of the level's b (pp ny nz); x, t follow
+    int toff[kMgMaxLevels];               // plane-table entry offset of the level: [3][nx]
+    int whole;                            // float offset of the whole levels (w.off relative to it)
+    int tab;                              // float offset of the plane table (8-byte entries)
+    MgBottom w;                           // the levels below, in CTA 0
+};
+
+// A x at (j, k) of the plane pc from the planes pm (i - 1) and pp (i + 1),
+// in the order of lap7.
+__device__ __forceinline__ float lap_planes(const float* pm, const float* pc, const float* pp,
+                                            const Dims& d, const LapCoef<float>& cf, int j, int k,
+                                            float xc) {
+    const int cj = j * d.nz;
+    float ax = 0.0f;
+    ax += pm[cj + k] * cf.c[0][0];
+    ax += xc * cf.c[0][1];
+    ax += pp[cj + k] * cf.c[0][2];
+    ax += pc[wrap(j - 1, d.ny) * d.nz + k] * cf.c[1][0];
+    ax += xc * cf.c[1][1];
+    ax += pc[wrap(j + 1, d.ny) * d.nz + k] * cf.c[1][2];
+    ax += pc[cj + wrap(k - 1, d.nz)] * cf.c[2][0];
+    ax += xc * cf.c[2][1];
+    ax += pc[cj + wrap(k + 1, d.nz)] * cf.c[2][2];
+    return ax;
+}
+
+__global__ void __launch_bounds__(kBottomThreads, 1)
+mg_cluster(MgCluster P, const float* __restrict__ gb, float* __restrict__ gx,
+           const BicgScalars* sc) {
+    pdl_wait();
+    // uniform over the cluster: no CTA has touched another's memory yet
+    if (sc->done) return;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) float sm[];
+    const int rank = (int)cl.block_rank();
+    const int tid = threadIdx.x, nt = blockDim.x;
+    float** tab = reinterpret_cast<float**>(sm + P.tab);
+    float* whole0 = cl.map_shared_rank(sm + P.whole, 0);
+    const Dims dw = P.w.d[0];
+    const int plw = dw.ny * dw.nz;
+    // plane i of array a (0 b, 1 x, 2 t) of level r: a split level's plane
+    // in its owner's shared memory, or the first whole level's in CTA 0's
+    auto plane = [&](int r, int a, int i) -> float* {
+        if (r < P.ns) return tab[P.toff[r] + a * P.d[r].nx + i];
+        return whole0 + P.w.off[0] + a * (int)dw.n + i * plw;
+    };
+    for (int r = 0; r < P.ns; ++r) {
+        const int nx = P.d[r].nx, pl = P.d[r].ny * P.d[r].nz, cells = P.pp[r] * pl;
+        for (int e = tid; e < 3 * nx; e += nt) {
+            const int a = e / nx, i = e - a * nx;
+            const int owner = i / P.pp[r], li = i - owner * P.pp[r];
+            tab[P.toff[r] + e] = cl.map_shared_rank(sm + P.off[r] + a * cells + li * pl, owner);
+        }
+    }
+    {   // this CTA's planes of the first level's b
+        const int cells = P.pp[0] * P.d[0].ny * P.d[0].nz;
+        const float* src = gb + (long long)rank * cells;
+        float* b = sm + P.off[0];
+        for (int q = tid; q < cells; q += nt) b[q] = src[q];
+    }
+    if (rank == 0) bottom_load_pinv(P.w, sm + P.whole);
+    cl.sync();
+    // down: pre-smooth from zero, restrict
+    for (int r = 0; r < P.ns; ++r) {
+        const Dims d = P.d[r];
+        const LapCoef<float> cf = P.cf[r];
+        const int pl = d.ny * d.nz, cells = P.pp[r] * pl, i0 = rank * P.pp[r];
+        const Dims loc{P.pp[r], d.ny, d.nz, (long long)cells};
+        float* b = sm + P.off[r];
+        float* x = b + cells;
+        const float wd = P.wd[r];
+        for (int q = tid; q < cells; q += nt) {
+            int il, j, k;
+            decode(q, loc, P.inv_p[r], P.inv_z[r], il, j, k);
+            const int i = i0 + il;
+            const float* pc = b + il * pl;
+            const float bc = pc[j * d.nz + k];
+            const float ab = lap_planes(plane(r, 0, wrap(i - 1, d.nx)), pc,
+                                        plane(r, 0, wrap(i + 1, d.nx)), d, cf, j, k, bc);
+            x[q] = wd * (2.0f * bc - wd * ab);
+        }
+        cl.sync();
+        // coarse planes I whose first child plane 2I is this CTA's
+        const bool cs = r + 1 < P.ns;
+        const Dims c = cs ? P.d[r + 1] : dw;
+        const float cip = cs ? P.inv_p[r + 1] : P.w.inv_p[0];
+        const float ciz = cs ? P.inv_z[r + 1] : P.w.inv_z[0];
+        const int I0 = (i0 + 1) >> 1, I1 = (i0 + P.pp[r] + 1) >> 1;
+        const int ccells = (I1 - I0) * c.ny * c.nz;
+        const Dims cloc{I1 - I0, c.ny, c.nz, (long long)ccells};
+        const float cen = (cf.c[0][1] + cf.c[1][1]) + cf.c[2][1];
+        for (int q = tid; q < ccells; q += nt) {
+            int Il, J, K;
+            decode(q, cloc, cip, ciz, Il, J, K);
+            const int I = I0 + Il;
+            float sum = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int i = 2 * I + a;
+                const float* xm = plane(r, 1, wrap(i - 1, d.nx));
+                const float* xc = plane(r, 1, i);
+                const float* xp = plane(r, 1, wrap(i + 1, d.nx));
+                const float* bi = plane(r, 0, i);
+#pragma unroll
+                for (int bb = 0; bb < 2; ++bb) {
+                    const int j = 2 * J + bb;
+                    const int jm = wrap(j - 1, d.ny) * d.nz, jp = wrap(j + 1, d.ny) * d.nz;
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const int k = 2 * K + cc, q0 = j * d.nz + k;
+                        float ax = xc[q0] * cen;
+                        ax = fmaf(xm[q0], cf.c[0][0], ax);
+                        ax = fmaf(xp[q0], cf.c[0][2], ax);
+                        ax = fmaf(xc[jm + k], cf.c[1][0], ax);
+                        ax = fmaf(xc[jp + k], cf.c[1][2], ax);
+                        ax = fmaf(xc[j * d.nz + wrap(k - 1, d.nz)], cf.c[2][0], ax);
+                        ax = fmaf(xc[j * d.nz + wrap(k + 1, d.nz)], cf.c[2][2], ax);
+                        sum += bi[q0] - ax;
+                    }
+                }
+            }
+            plane(r + 1, 0, I)[J * c.nz + K] = sum;
+        }
+        cl.sync();
+    }
+    // the levels below, in CTA 0
+    if (rank == 0) bottom_cycle(P.w, sm + P.whole);
+    cl.sync();
+    // up: x += P xc, two post-smoothing sweeps
+    for (int r = P.ns - 1; r >= 0; --r) {
+        const Dims d = P.d[r];
+        const LapCoef<float> cf = P.cf[r];
+        const int pl = d.ny * d.nz, cells = P.pp[r] * pl, i0 = rank * P.pp[r];
+        const Dims loc{P.pp[r], d.ny, d.nz, (long long)cells};
+        const Dims c = r + 1 < P.ns ? P.d[r + 1] : dw;
+        float* b = sm + P.off[r];
+        float* x = b + cells;
+        float* t = x + cells;
+        const float wd = P.wd[r];
+        for (int q = tid; q < cells; q += nt) {
+            int il, j, k;
+            decode(q, loc, P.inv_p[r], P.inv_z[r], il, j, k);
+            const int i = i0 + il;
+            const int I = i >> 1, J = j >> 1, K = k >> 1;
+            const int I2 = wrap(I + ((i & 1) ? 1 : -1), c.nx);
+            const int J2 = wrap(J + ((j & 1) ? 1 : -1), c.ny);
+            const int K2 = wrap(K + ((k & 1) ? 1 : -1), c.nz);
+            const float* c0 = plane(r + 1, 1, I);
+            const float* c1 = plane(r + 1, 1, I2);
+            const int b0 = J * c.nz, b1 = J2 * c.nz;
+            const float v000 = c0[b0 + K], v100 = c1[b0 + K];
+            const float v010 = c0[b1 + K], v001 = c0[b0 + K2];
+            const float v110 = c1[b1 + K], v101 = c1[b0 + K2];
+            const float v011 = c0[b1 + K2], v111 = c1[b1 + K2];
+            const float e = (27.0f * v000 + 9.0f * (v100 + v010 + v001) +
+                             3.0f * (v110 + v101 + v011) + v111) * (1.0f / 64.0f);
+            x[q] = x[q] + e;
+        }
+        cl.sync();
+        for (int pass = 0; pass < 2; ++pass) {
+            const int ai = pass == 0 ? 1 : 2;   // smooth x -> t, then t -> x
+            float* in = pass == 0 ? x : t;
+            float* out = pass == 0 ? t : x;
+            for (int q = tid; q < cells; q += nt) {
+                int il, j, k;
+                decode(q, loc, P.inv_p[r], P.inv_z[r], il, j, k);
+                const int i = i0 + il;
+                const float* pc = in + il * pl;
+                const float v = pc[j * d.nz + k];
+                const float ax = lap_planes(plane(r, ai, wrap(i - 1, d.nx)), pc,
+                                            plane(r, ai, wrap(i + 1, d.nx)), d, cf, j, k, v);
+                out[q] = fmaf(wd, b[q] - ax, v);
+            }
+            cl.sync();
+        }
+    }
+    {   // this CTA's planes of the first level's x
+        const int cells = P.pp[0] * P.d[0].ny * P.d[0].nz;
+        const float* x = sm + P.off[0] + cells;
+        float* dst = gx + (long long)rank * cells;
+        for (int q = tid; q < cells; q += nt) dst[q] = x[q];
     }
 }
 
@@ -745,6 +958,98 @@ static MgBottom bottom_params(const MgPlan& P) {
     }
     m.pinv = P.pinv;
     return m;
+}
+
+// Shared-memory layout of the cluster kernel (floats): split levels' planes,
+// the bottom levels (CTA 0), the plane table (8-byte entries).
+static MgCluster cluster_params(const MgPlan& P, size_t* floats) {
+    MgCluster m{};
+    m.ns = P.B - P.C;
+    int off = 0, toff = 0;
+    for (int l = P.C; l < P.B; ++l) {
+        const int r = l - P.C;
+        const MgLevel& v = P.lv[l];
+        m.d[r] = v.d;
+        m.cf[r] = v.cf;
+        m.wd[r] = v.wd;
+        m.pp[r] = v.d.nx / kClusterCtas;
+        m.inv_p[r] = 1.0f / float(v.d.ny * v.d.nz);
+        m.inv_z[r] = 1.0f / float(v.d.nz);
+        m.off[r] = off;
+        off += 3 * m.pp[r] * v.d.ny * v.d.nz;
+        m.toff[r] = toff;
+        toff += 3 * v.d.nx;
+    }
+    m.whole = off;
+    m.w = bottom_params(P);
+    off += (int)bottom_smem_floats(P);
+    off = (off + 1) & ~1;
+    m.tab = off;
+    off += 2 * toff;
+    *floats = (size_t)off;
+    return m;
+}
+
+static constexpr size_t kClusterSmemMax = 200 * 1024;
+
+static cudaError_t launch_cluster(const MgCluster& m, size_t smem, const float* gb, float* gx,
+                                  const BicgScalars* sc, cudaStream_t s) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(kClusterCtas);
+    cfg.blockDim = dim3(kBottomThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kClusterCtas;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    // programmatic dependent launch, as the per-level kernels (pdl_wait()
+    // at entry)
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    return cudaLaunchKernelEx(&cfg, mg_cluster, m, gb, gx, sc);
+}
+
+// Whether this device runs the plan's cluster kernel (shared memory within
+// kClusterSmemMax and at least one cluster resident); otherwise the split
+// levels fall back to the per-level kernels.
+static bool cluster_usable(const MgPlan& P) {
+    size_t fl = 0;
+    const MgCluster m = cluster_params(P, &fl);
+    const size_t bytes = fl * sizeof(float);
+    if (bytes > kClusterSmemMax) return false;
+    static int dev_done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !dev_done[dev]) {
+        if (cudaFuncSetAttribute(mg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kClusterSmemMax) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        dev_done[dev] = 1;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(kClusterCtas);
+    cfg.blockDim = dim3(kBottomThreads);
+    cfg.dynamicSmemBytes = bytes;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kClusterCtas;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    (void)m;
+    if (cudaOccupancyMaxActiveClusters(&nc, mg_cluster, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return nc >= 1;
 }
 
 // v = A ph, gamma = (v, res0), alpha = rho / gamma (TZ: cp.async tile width,
@@ -965,6 +1270,13 @@ int mg_levels(const pf_grid* g, MgLevel* lv, int* bottom) {
     int B = 0;
     while (B < L && lv[B].kind != kMgBottom) ++B;
     if (L < 2 || B == 0 || B == L) return 0;
+    // the cluster kernel takes the levels just above the bottom ones that
+    // split evenly into x planes per CTA
+    for (int l = B - 1; l >= 1; --l) {
+        const MgLevel& v = lv[l];
+        if (v.kind != kMgPointwise || v.d.n > kMgClusterMax || v.d.nx % kClusterCtas) break;
+        lv[l].kind = kMgCluster;
+    }
     *bottom = B;
     return L;
 }
@@ -1004,6 +1316,12 @@ static bool async_attrs() {
 int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
     P->L = mg_levels(g, P->lv, &P->B);
     if (!P->L) return PF_ERR_BAD_ARG;
+    P->C = P->B;
+    while (P->C > 1 && P->lv[P->C - 1].kind == kMgCluster) --P->C;
+    if (P->C < P->B && !cluster_usable(*P)) {
+        for (int l = P->C; l < P->B; ++l) P->lv[l].kind = kMgPointwise;
+        P->C = P->B;
+    }
     static int dev_done[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1069,7 +1387,7 @@ static void smooth_as(const MgLevel& f, const BicgScalars* sc, const AsyncSmooth
 static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars* sc,
                         cudaStream_t s) {
     const dim3 blk(32, 8);
-    for (int l = 0; l < P.B; ++l) {
+    for (int l = 0; l < P.C; ++l) {
         const MgLevel& f = P.lv[l];
         const MgLevel& c = P.lv[l + 1];
         const float* bl = l == 0 ? b0 : f.b;
@@ -1091,13 +1409,17 @@ static void vcycle_tail(const MgPlan& P, const float* b0, float* x0, BicgScalars
         PF_LAUNCH(l == 0 ? "mg_restrict_l0" : "mg_restrict", s, launch_pdl(mg_restrict, dim3(cgrid3h(c.d)), dim3(blk), 0, s,
             f.d, f.cf, bl, xl, c.d, c.b, sc));
     }
-    {
+    if (P.C < P.B) {
+        size_t fl = 0;
+        const MgCluster m = cluster_params(P, &fl);
+        PF_LAUNCH("mg_cluster", s, launch_cluster(m, fl * sizeof(float), P.lv[P.C].b, P.lv[P.C].x, sc, s));
+    } else {
         const MgBottom m = bottom_params(P);
         const size_t smem = bottom_smem_floats(P) * sizeof(float);
         PF_LAUNCH("mg_bottom", s, launch_pdl(mg_bottom, dim3(1), dim3(kBottomThreads), smem, s,
             m, P.lv[P.B].b, P.lv[P.B].x, sc));
     }
-    for (int l = P.B - 1; l >= 0; --l) {
+    for (int l = P.C - 1; l >= 0; --l) {
         const MgLevel& f = P.lv[l];
         const MgLevel& c = P.lv[l + 1];
         const float* bl = l == 0 ? b0 : f.b;

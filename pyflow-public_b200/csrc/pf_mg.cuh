@@ -10,12 +10,17 @@ constexpr long long kMgCoarseTarget = 64;     // coarsen down to at most this ma
 constexpr long long kMgBottomMax = 4096;      // largest coarsest level (solved in one CTA)
 constexpr long long kMgBottomLevel = 512;     // levels this small run inside that CTA
 constexpr long long kMgSweepMin = 1LL << 20;  // levels this large use the tiled sweep
+constexpr long long kMgClusterMax = 4096;     // levels this small may run in the cluster kernel
+constexpr int kClusterCtas = 8;               // CTAs of that cluster (x planes split among them)
 
 // How a level's kernels run: the tiled sweep (the finest level always, and
-// every level of at least kMgSweepMin cells), one thread per cell, or inside
+// every level of at least kMgSweepMin cells), one thread per cell, inside
 // the single-CTA bottom kernel (every level of at most kMgBottomLevel cells,
-// and the coarsest level, which must have at most kMgBottomMax cells).
-enum MgKind { kMgSwept = 0, kMgPointwise = 1, kMgBottom = 2 };
+// and the coarsest level, which must have at most kMgBottomMax cells), or
+// split by x planes across the CTAs of the cluster kernel, which also runs
+// the bottom levels (the levels just above the bottom ones with at most
+// kMgClusterMax cells and an x extent that kClusterCtas divides).
+enum MgKind { kMgSwept = 0, kMgPointwise = 1, kMgBottom = 2, kMgCluster = 3 };
 
 struct MgLevel {
     Dims d;
@@ -32,6 +37,7 @@ struct MgLevel {
 struct MgPlan {
     int L = 0;  // number of levels; 0 = multigrid does not apply to the grid
     int B = 0;  // first level handled by the bottom kernel
+    int C = 0;  // first level of the cluster kernel (C == B: the bottom kernel alone)
     MgLevel lv[kMgMaxLevels];
     // Krylov vectors (FP32, finest grid); p is double-buffered
     float *res, *res0, *p[2], *v, *s, *t, *ph, *sh, *e;
