@@ -88,9 +88,16 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
     const T w_zm = S.w(0, 0, -1), w_xm_zp = S.w(-1, 0, 1), w_xp_zm = S.w(1, 0, -1);
     const T w_ym_zp = S.w(0, -1, 1), w_yp_zm = S.w(0, 1, -1);
 
+    // FP64 keeps the reference's divisions (bit-exact parity); the FP32 stage
+    // of the mixed forms multiplies by the reciprocals instead (one rounding
+    // more, no IEEE division sequence per use)
+    constexpr bool f32 = sizeof(T) == 4;
+    const T irho = T(1) / rho;
+    auto over_rho = [&](T a) -> T { if constexpr (f32) return a * irho; else return a / rho; };
     // divergence / 3 at centres (div_vel_over, metric_staggered.py:424-433)
     auto div3 = [&](T ue, T uw, T vn, T vs, T wt, T wb) -> T {
-        return ((((ue - uw) * dxi) + ((vn - vs) * dyi)) + ((wt - wb) * dzi)) / T(3.0);
+        const T s = (((ue - uw) * dxi) + ((vn - vs) * dyi)) + ((wt - wb) * dzi);
+        if constexpr (f32) return s * T(1.0f / 3.0f); else return s / T(3.0);
     };
     const T D_c = div3(u_xp, u_c, v_yp, v_c, w_zp, w_c);
     const T D_xm = div3(u_c, u_xm, v_xm_yp, v_xm, w_xm_zp, w_xm);
@@ -99,12 +106,12 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
 
     const T two = T(2.0);
     // diagonal viscous fluxes at centres
-    const T fxx_c = ((u_xp - u_c) * dxi - D_c) * ((two * LV(0, 0, 0)) / rho);
-    const T fxx_m = ((u_c - u_xm) * dxi - D_xm) * ((two * LV(-1, 0, 0)) / rho);
-    const T fyy_c = ((v_yp - v_c) * dyi - D_c) * ((two * LV(0, 0, 0)) / rho);
-    const T fyy_m = ((v_c - v_ym) * dyi - D_ym) * ((two * LV(0, -1, 0)) / rho);
-    const T fzz_c = ((w_zp - w_c) * dzi - D_c) * ((two * LV(0, 0, 0)) / rho);
-    const T fzz_m = ((w_c - w_zm) * dzi - D_zm) * ((two * LV(0, 0, -1)) / rho);
+    const T fxx_c = ((u_xp - u_c) * dxi - D_c) * over_rho(two * LV(0, 0, 0));
+    const T fxx_m = ((u_c - u_xm) * dxi - D_xm) * over_rho(two * LV(-1, 0, 0));
+    const T fyy_c = ((v_yp - v_c) * dyi - D_c) * over_rho(two * LV(0, 0, 0));
+    const T fyy_m = ((v_c - v_ym) * dyi - D_ym) * over_rho(two * LV(0, -1, 0));
+    const T fzz_c = ((w_zp - w_c) * dzi - D_c) * over_rho(two * LV(0, 0, 0));
+    const T fzz_m = ((w_c - w_zm) * dzi - D_zm) * over_rho(two * LV(0, 0, -1));
 
     // edge viscosities (one cell below the flux, as in the reference)
     T vxy_c, vxy_ym, vxy_xm, vxz_c, vxz_zm, vxz_xm, vyz_c, vyz_zm, vyz_ym;
@@ -124,15 +131,15 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
         vxy_c = vxy_ym = vxy_xm = vxz_c = vxz_zm = vxz_xm = vyz_c = vyz_zm = vyz_ym = e;
     }
     // off-diagonal viscous fluxes on edges: (grad_y u + grad_x v) * (Vxy / rho)
-    const T fxy_c = (((u_yp - u_c) * dyi) + ((v_xp - v_c) * dxi)) * (vxy_c / rho);
-    const T fxy_ym = (((u_c - u_ym) * dyi) + ((v_xp_ym - v_ym) * dxi)) * (vxy_ym / rho);
-    const T fxy_xm = (((u_xm_yp - u_xm) * dyi) + ((v_c - v_xm) * dxi)) * (vxy_xm / rho);
-    const T fxz_c = (((u_zp - u_c) * dzi) + ((w_xp - w_c) * dxi)) * (vxz_c / rho);
-    const T fxz_zm = (((u_c - u_zm) * dzi) + ((w_xp_zm - w_zm) * dxi)) * (vxz_zm / rho);
-    const T fxz_xm = (((u_xm_zp - u_xm) * dzi) + ((w_c - w_xm) * dxi)) * (vxz_xm / rho);
-    const T fyz_c = (((v_zp - v_c) * dzi) + ((w_yp - w_c) * dyi)) * (vyz_c / rho);
-    const T fyz_zm = (((v_c - v_zm) * dzi) + ((w_yp_zm - w_zm) * dyi)) * (vyz_zm / rho);
-    const T fyz_ym = (((v_ym_zp - v_ym) * dzi) + ((w_c - w_ym) * dyi)) * (vyz_ym / rho);
+    const T fxy_c = (((u_yp - u_c) * dyi) + ((v_xp - v_c) * dxi)) * over_rho(vxy_c);
+    const T fxy_ym = (((u_c - u_ym) * dyi) + ((v_xp_ym - v_ym) * dxi)) * over_rho(vxy_ym);
+    const T fxy_xm = (((u_xm_yp - u_xm) * dyi) + ((v_c - v_xm) * dxi)) * over_rho(vxy_xm);
+    const T fxz_c = (((u_zp - u_c) * dzi) + ((w_xp - w_c) * dxi)) * over_rho(vxz_c);
+    const T fxz_zm = (((u_c - u_zm) * dzi) + ((w_xp_zm - w_zm) * dxi)) * over_rho(vxz_zm);
+    const T fxz_xm = (((u_xm_zp - u_xm) * dzi) + ((w_c - w_xm) * dxi)) * over_rho(vxz_xm);
+    const T fyz_c = (((v_zp - v_c) * dzi) + ((w_yp - w_c) * dyi)) * over_rho(vyz_c);
+    const T fyz_zm = (((v_c - v_zm) * dzi) + ((w_yp_zm - w_zm) * dyi)) * over_rho(vyz_zm);
+    const T fyz_ym = (((v_ym_zp - v_ym) * dzi) + ((w_c - w_ym) * dyi)) * over_rho(vyz_ym);
 
     T ux_p = fxx_c, ux_m = fxx_m, uy_p = fxy_c, uy_m = fxy_ym, uz_p = fxz_c, uz_m = fxz_zm;
     T vx_p = fxy_c, vx_m = fxy_xm, vy_p = fyy_c, vy_m = fyy_m, vz_p = fyz_c, vz_m = fyz_zm;
