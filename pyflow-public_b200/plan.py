@@ -73,3 +73,71 @@ class StepPlan:
             self.close()
         except Exception:
             pass
+
+
+class StepPipeline:
+    """Independent time steps on states that arrive in pinned host memory
+    (a request stream), with the host<->device copies overlapped with the
+    computation: two field sets with one captured StepPlan each are used
+    alternately, so the copy of request k+1 runs on a copy stream (the copy
+    engines) while request k computes on the compute stream.  Ordering is by
+    events only; nothing here synchronises the host.
+
+    ``submit(u, v, w, p, stats_out, state_out=None)`` takes pinned host FP64
+    tensors of the grid's shape and a pinned host FP64 tensor of 10 for the
+    step's statistics (the layout of ``StepPlan.stats_dev``); with
+    ``state_out`` (four pinned host tensors) the advanced u, v, w, p are
+    copied back too, on the copy stream.  The host tensors must stay
+    untouched until ``synchronize()`` (or a later event) shows the request
+    done.  DP starts from zero for every request, as in Domain.forwardStep.
+    """
+
+    def __init__(self, shape, spacing, mu, rho, dt, min_res=1e-10, max_it=20000,
+                 prec="fp64", rk4=True, device="cuda", stream=None):
+        dev = torch.device(device)
+        self.sets = [[torch.zeros(shape, dtype=torch.float64, device=dev) for _ in range(5)]
+                     for _ in range(2)]
+        self.plans = [StepPlan(*f, spacing, mu, rho, dt, min_res=min_res, max_it=max_it,
+                               prec=prec, rk4=rk4) for f in self.sets]
+        self.compute = stream if stream is not None else torch.cuda.current_stream(dev)
+        self.copy = torch.cuda.Stream(dev)
+        self.ready = [torch.cuda.Event() for _ in range(2)]
+        self.done = [torch.cuda.Event() for _ in range(2)]
+        self.free = [torch.cuda.Event() for _ in range(2)]
+        for e in self.free:
+            e.record(self.compute)
+        self.k = 0
+
+    def submit(self, u, v, w, p, stats_out, state_out=None):
+        s = self.k & 1
+        f = self.sets[s]
+        # the set is free once its previous request has computed and copied out
+        self.copy.wait_event(self.free[s])
+        with torch.cuda.stream(self.copy):
+            for d, h in zip(f[:4], (u, v, w, p)):
+                d.copy_(h, non_blocking=True)
+        self.ready[s].record(self.copy)
+        self.compute.wait_event(self.ready[s])
+        with torch.cuda.stream(self.compute):
+            f[4].zero_()
+        self.plans[s].launch(1, stream=self.compute)
+        with torch.cuda.stream(self.compute):
+            stats_out.copy_(self.plans[s].stats_dev, non_blocking=True)
+        if state_out is None:
+            self.free[s].record(self.compute)
+        else:
+            self.done[s].record(self.compute)
+            self.copy.wait_event(self.done[s])
+            with torch.cuda.stream(self.copy):
+                for h, d in zip(state_out, f[:4]):
+                    h.copy_(d, non_blocking=True)
+            self.free[s].record(self.copy)
+        self.k += 1
+
+    def synchronize(self):
+        self.compute.synchronize()
+        self.copy.synchronize()
+
+    def close(self):
+        for pl in self.plans:
+            pl.close()

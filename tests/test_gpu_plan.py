@@ -73,3 +73,40 @@ def test_plans_run_concurrently_on_streams():
             pl.close()
     for x, y in zip(alone, mixed):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed_mg"])
+def test_pipeline_matches_plan(prec):
+    """StepPipeline (two field sets, host copies on a copy stream overlapped
+    with the previous request's step) returns, for each independent request,
+    bitwise the state and statistics of one StepPlan step on that request."""
+    import pyflow_b200.initial as ic
+    from pyflow_b200.plan import StepPipeline, StepPlan
+    shape = (24, 24, 32)
+    sp = tuple(2 * np.pi / n for n in shape)
+    nu, dt = 0.01, 0.005
+    reqs = []
+    for seed in range(5):
+        u, v, w = ic.spectral_velocity(shape, k0=4.0, seed=20 + seed)
+        p = np.random.default_rng(seed).standard_normal(shape)
+        reqs.append([torch.tensor(a).pin_memory() for a in (u, v, w, p)])
+    pipe = StepPipeline(shape, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec)
+    stats = [torch.zeros(10, dtype=torch.float64).pin_memory() for _ in reqs]
+    states = [[torch.zeros(shape, dtype=torch.float64).pin_memory() for _ in range(4)]
+              for _ in reqs]
+    for r, s_, o in zip(reqs, stats, states):
+        pipe.submit(*r, s_, state_out=o)
+    pipe.synchronize()
+    pipe.close()
+    for r, s_, o in zip(reqs, stats, states):
+        f = [t.cuda() for t in r] + [torch.zeros(shape, dtype=torch.float64, device="cuda")]
+        plan = StepPlan(*f, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec)
+        plan.launch(1)
+        torch.cuda.synchronize()
+        ref = plan.stats_dev.cpu()
+        plan.close()
+        for a, b in zip(o, f[:4]):
+            assert torch.equal(a, b.cpu())
+        # statistics of the step (the running totals 8, 9 differ by design)
+        assert torch.equal(s_[:8], ref[:8])
+        assert int(s_[7]) == 0
