@@ -323,7 +323,7 @@ fold_correction(Dims d, const BicgScalars* sc, const T* e, double* x, int guard 
 
 // r = b - A x in FP64 and max|r| (the refinement's true residual)
 struct PhaseResidual {
-    static constexpr int R = 2;
+    static constexpr int R = 4;
     const double *x, *b;
     double* r;
     double mx;
