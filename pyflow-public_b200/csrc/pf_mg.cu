@@ -1049,24 +1049,33 @@ static MgCluster cluster_params(const MgPlan& P, size_t* floats) {
 
 static constexpr size_t kClusterSmemMax = 200 * 1024;
 
-static cudaError_t launch_cluster(const MgCluster& m, size_t smem, const float* gb, float* gx,
-                                  const BicgScalars* sc, cudaStream_t s) {
+// Launch configuration of the cluster kernel: one cluster of kClusterCtas
+// CTAs, optionally with programmatic dependent launch (`at` holds two entries).
+static cudaLaunchConfig_t cluster_config(size_t smem, cudaStream_t s, cudaLaunchAttribute* at,
+                                         bool pdl) {
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(kClusterCtas);
     cfg.blockDim = dim3(kBottomThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
-    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = kClusterCtas;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
-    // programmatic dependent launch, as the per-level kernels (pdl_wait()
-    // at entry)
-    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 2;
+    cfg.numAttrs = 1;
+    if (pdl) {  // as the per-level kernels (pdl_wait() at entry)
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.numAttrs = 2;
+    }
+    return cfg;
+}
+
+static cudaError_t launch_cluster(const MgCluster& m, size_t smem, const float* gb, float* gx,
+                                  const BicgScalars* sc, cudaStream_t s) {
+    cudaLaunchAttribute at[2];
+    const cudaLaunchConfig_t cfg = cluster_config(smem, s, at, true);
     return cudaLaunchKernelEx(&cfg, mg_cluster, m, gb, gx, sc);
 }
 
@@ -1075,7 +1084,7 @@ static cudaError_t launch_cluster(const MgCluster& m, size_t smem, const float* 
 // levels fall back to the per-level kernels.
 static bool cluster_usable(const MgPlan& P) {
     size_t fl = 0;
-    const MgCluster m = cluster_params(P, &fl);
+    cluster_params(P, &fl);
     const size_t bytes = fl * sizeof(float);
     if (bytes > kClusterSmemMax) return false;
     static int dev_done[64] = {0};
@@ -1089,19 +1098,9 @@ static bool cluster_usable(const MgPlan& P) {
         }
         dev_done[dev] = 1;
     }
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(kClusterCtas);
-    cfg.blockDim = dim3(kBottomThreads);
-    cfg.dynamicSmemBytes = bytes;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kClusterCtas;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cudaLaunchAttribute at[2];
+    const cudaLaunchConfig_t cfg = cluster_config(bytes, nullptr, at, false);
     int nc = 0;
-    (void)m;
     if (cudaOccupancyMaxActiveClusters(&nc, mg_cluster, &cfg) != cudaSuccess) {
         cudaGetLastError();
         return false;
