@@ -548,7 +548,6 @@ struct MgBottom {
     const float* pinv;          // coarsest level's pseudo-inverse, or null
 };
 
-constexpr int kMgPinvMax = 64;  // largest coarsest level solved with a pseudo-inverse
 
 // Pseudo-inverse of the periodic coarsest-level operator (singular: constant
 // null space), from its Fourier eigen-decomposition:

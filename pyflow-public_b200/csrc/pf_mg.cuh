@@ -12,6 +12,7 @@ constexpr long long kMgBottomLevel = 512;     // levels this small run inside th
 constexpr long long kMgSweepMin = 1LL << 20;  // levels this large use the tiled sweep
 constexpr long long kMgClusterMax = 4096;     // levels this small may run in the cluster kernel
 constexpr int kClusterCtas = 8;               // CTAs of that cluster (x planes split among them)
+constexpr int kMgPinvMax = 64;                // largest coarsest level solved with a pseudo-inverse
 
 // How a level's kernels run: the tiled sweep (the finest level always, and
 // every level of at least kMgSweepMin cells), one thread per cell, inside

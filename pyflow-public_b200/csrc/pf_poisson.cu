@@ -713,25 +713,32 @@ vel_corr_kernel(Dims d, const double* __restrict__ DP, double scale, double dxi,
     w[q] = fma(-scale, gz, w[q]);
 }
 
-// max|u|, max|v|, max|w|, sum(u^2+v^2+w^2), max|div u|
+// max|u|, max|v|, max|w|, sum(u^2+v^2+w^2), max|div u|: one warp per (i, j)
+// row of cells, its lanes along z (row and neighbour-row offsets computed
+// once per row)
 __global__ void __launch_bounds__(256)
 stats_kernel(Dims d, BicgScalars* sc, double* part, const double* __restrict__ u,
              const double* __restrict__ v, const double* __restrict__ w,
              double dxi, double dyi, double dzi, double* out) {
     __shared__ double sh[32];
     double mu_ = 0, mv = 0, mw = 0, s = 0, md = 0;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
-         q += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(q % d.nz);
-        const long long r = q / d.nz;
-        const int j = (int)(r % d.ny), i = (int)(r / d.ny);
-        const double a = u[q], b = v[q], c = w[q];
-        mu_ = nanmax(mu_, fabs(a)); mv = nanmax(mv, fabs(b)); mw = nanmax(mw, fabs(c));
-        s += (a * a + b * b) + c * c;
-        double dv = (u[idx(d, wrap(i + 1, d.nx), j, k)] - a) * dxi;
-        dv += (v[idx(d, i, wrap(j + 1, d.ny), k)] - b) * dyi;
-        dv += (w[idx(d, i, j, wrap(k + 1, d.nz))] - c) * dzi;
-        md = nanmax(md, fabs(dv));
+    const int lane = threadIdx.x & 31;
+    const int nrows = d.nx * d.ny, wpb = blockDim.x >> 5;
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += gridDim.x * wpb) {
+        const int i = row / d.ny, j = row - i * d.ny;
+        const long long base = (long long)row * d.nz;
+        const long long bx = ((long long)wrap(i + 1, d.nx) * d.ny + j) * d.nz;
+        const long long by = ((long long)i * d.ny + wrap(j + 1, d.ny)) * d.nz;
+        for (int k = lane; k < d.nz; k += 32) {
+            const long long q = base + k;
+            const double a = u[q], b = v[q], c = w[q];
+            mu_ = nanmax(mu_, fabs(a)); mv = nanmax(mv, fabs(b)); mw = nanmax(mw, fabs(c));
+            s += (a * a + b * b) + c * c;
+            double dv = (u[bx + k] - a) * dxi;
+            dv += (v[by + k] - b) * dyi;
+            dv += (w[base + wrap(k + 1, d.nz)] - c) * dzi;
+            md = nanmax(md, fabs(dv));
+        }
     }
     double r[5] = {block_max<kBlock>(mu_, sh), block_max<kBlock>(mv, sh),
                    block_max<kBlock>(mw, sh), block_sum<kBlock>(s, sh),
@@ -892,13 +899,18 @@ static int add_child(cudaGraph_t g, cudaGraphNode_t dep, cudaGraph_t child,
 // R holds, at different times of the step, the predictor's stage buffers, the
 // solver vectors and the statistics scratch.  The scalar block is written only
 // by the solver kernels.
+static constexpr size_t kPlanPinvBytes = (size_t)kMgPinvMax * kMgPinvMax * sizeof(float);
+
 size_t step_plan_ws_bytes(const pf_grid* g, int prec) {
     const size_t n = (size_t)g->nx * g->ny * g->nz;
     size_t vecs = prec == PF_FP64 ? 8 * align256(n * sizeof(double))
                                   : 11 * align256(n * sizeof(double));
     size_t r = std::max(std::max(predictor_ws_bytes(g, prec), vecs), stats_ws_bytes(g));
+    // PF_MIXED_MG: the coarsest level's pseudo-inverse in a slot of its own
+    // (the region r is reused by the predictor every step), computed once
+    const size_t pinv = prec == PF_MIXED_MG ? kPlanPinvBytes : 0;
     return align256(n * sizeof(double)) + align256(sizeof(BicgScalars)) +
-           align256(kNumPartials * kMaxPartials * sizeof(double)) + r;
+           align256(kNumPartials * kMaxPartials * sizeof(double)) + align256(r) + pinv;
 }
 
 int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
@@ -931,10 +943,20 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
     if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
         const int e = mg_setup(g, R, &mg);
         if (e != PF_OK && e != PF_ERR_BAD_ARG) return e;
+        // the pseudo-inverse lives in the last slot of the workspace, outside
+        // the region the predictor overwrites, and is computed once here
+        if (mg.L && mg.pinv)
+            mg.pinv = (float*)((char*)ws + step_plan_ws_bytes(g, prec) - kPlanPinvBytes);
     }
     if (predictor_prepare(prec) != cudaSuccess) return PF_ERR_CUDA;
     cudaStream_t cs;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return PF_ERR_CUDA;
+    if (mg.L) {
+        if (mg_enqueue_setup(mg, cs) != PF_OK || cudaStreamSynchronize(cs) != cudaSuccess) {
+            cudaStreamDestroy(cs);
+            return PF_ERR_CUDA;
+        }
+    }
     prof_suspend(true);
     StepPlan* plan = new StepPlan();
     int rc = PF_OK;
@@ -954,8 +976,6 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
             bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v64, DP);
         } else {
             mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, div, c1, c2, bb, DP, rr);
-            // after the predictor, whose stage buffers share the region
-            if (mg.L) mg_enqueue_setup(mg, cs);
         }
         if ((rc = capture_end(cs, &seg1))) break;
         cudaGraphNode_t n1, nw;
