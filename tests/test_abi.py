@@ -53,3 +53,29 @@ def test_host_only_calls():
     # argument validation happens before any CUDA call
     lib.pf_div_vel.restype = ctypes.c_int
     assert lib.pf_div_vel(ctypes.byref(g), None, None, None, None, None) == 1
+
+
+def test_step_plan_workspace_sizes():
+    """The step plan's workspace (host arithmetic only): the multigrid form
+    holds the mixed form's vectors plus a 256-byte aligned slot for the
+    coarsest level's pseudo-inverse (64 x 64 FP32), which the plan computes
+    once instead of in every step."""
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(LIB)
+
+    class Grid(ctypes.Structure):
+        _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                    ("nz", ctypes.c_int), ("dx", ctypes.c_double),
+                    ("dy", ctypes.c_double), ("dz", ctypes.c_double)]
+
+    lib.pf_step_plan_workspace_bytes.restype = ctypes.c_size_t
+    lib.pf_step_plan_workspace_bytes.argtypes = [ctypes.POINTER(Grid), ctypes.c_int]
+    for shape in ((64, 64, 64), (24, 20, 36), (33, 17, 70)):
+        g = Grid(*shape, 0.1, 0.1, 0.1)
+        fp64, mixed, mg = (lib.pf_step_plan_workspace_bytes(ctypes.byref(g), pr)
+                           for pr in (0, 1, 2))
+        n = shape[0] * shape[1] * shape[2]
+        assert fp64 >= 9 * 8 * n and mixed >= 12 * 8 * n
+        assert mg == mixed + 64 * 64 * 4
+        assert mg % 256 == 0 and mixed % 256 == 0
