@@ -1,41 +1,53 @@
 """Benchmark: cell-steps/s of the RK4 + pressure-Poisson time step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload dns128|dns256|dns512|serve] [--prec mixed|fp64]
+                    [--workload dns512|dns128|dns256|dns64|serve]
+                    [--prec mixed_mg|mixed|fp64]
 
 A "step" is one Domain.forwardStep (src/data/domain.py:342-402): staggered RK4
-predictor, divergence, BiCGStab pressure solve to max-norm relative residual
-1e-10, projection -- replayed as one captured CUDA graph per step (device-side
+predictor, divergence, pressure solve to max-norm relative residual 1e-10,
+projection -- replayed as one captured CUDA graph per step (device-side
 convergence loops, no host synchronisation inside the timed region).
 
-Precision (--prec): mixed_mg (default) runs the fluxes, RK4 stages and the
-Krylov vectors in FP32 with FP64 residuals, inner products and refinement, the
-FP32 passes preconditioned by a geometric multigrid V-cycle; mixed is the same
-without the preconditioner; fp64 is the reference's algorithm in FP64.  The
-mixed forms also time the fp64 form from the same field and report the
-relative velocity difference.
+Precision (--prec):
+  mixed_mg (default)  fluxes, RK4 stages and Krylov vectors in FP32; FP64
+                      residuals, inner products and iterative refinement to the
+                      reference's tolerance on the FP64 true residual; the FP32
+                      passes run BiCGStab right-preconditioned by one FP32
+                      geometric-multigrid V(2,2) cycle
+  mixed               the same refinement with unpreconditioned FP32 BiCGStab
+  fp64                the reference's algorithm (unpreconditioned BiCGStab) in FP64
+The mixed forms also run the FP64 form from the same field for the
+workload's full step count and report its rate and the error of the mixed
+form against it (relative L2 / max-norm velocity error after the last step,
+largest relative KE(t) and dissipation(t) errors, max|div u| of both).
 
 Workloads (synthetic inputs: the seeded k^4 exp(-2 (k/k0)^2) spectral field,
 urms = 1, in place of the reference's DNS restart data):
-  dns128  128^3 decaying turbulence, k0 = 4, nu = 0.005, dt = 0.0025 (default)
+  dns512  512^3, k0 = 8, nu = 0.0012, dt = 0.001, 50 steps (default)
+  dns128  128^3, k0 = 4, nu = 0.005, dt = 0.0025, 100 steps
   dns256  256^3, k0 = 4, nu = 0.0025, dt = 0.00125 (profiling size)
-  dns512  512^3, k0 = 8, nu = 0.0012, dt = 0.001
+  dns64   64^3, k0 = 4, nu = 0.01, dt = 0.005, 20 steps (FP64 plain DNS)
   serve   request stream of 32..192^3 solves (50 steps each, nu = 0.02*32/N)
           with Poisson arrivals at 80 % of the measured capacity; reports
           p50/p99 latency and aggregate cell-steps/s
-The per-step working set (~0.3 GB at 128^3) exceeds the 126 MB L2, so no
-explicit flush is done between steps.
+The per-step working set (> 0.3 GB) exceeds the 126 MB L2, so no explicit
+flush is done between steps.
 
-Under torchrun (N > 1) every rank advances its own independent replica (a
-single solve of this size does not shard: "replicas only"); value is the sum of
-all ranks' cell-steps over the max-over-ranks device time.
+--gpus N without torchrun re-launches this script under torch.distributed.run
+with N ranks.  Every rank advances its own independent replica (a single solve
+of this size does not shard: "replicas only"); value is the sum of all ranks'
+cell-steps over the max-over-ranks device time.
 
 --impl reference times the reference algorithm's CPU restatement
-(oracle/liboracle.so, FP64, OpenMP on all host cores) on the same workload.
+(oracle/liboracle.so, FP64, OpenMP on all host cores) on the same workload; at
+grids of 256^3 and more each step is a bounded sample (one step with the
+pressure solve cut short, scaled to the reference's iteration count).
 """
 import argparse
 import json
 import os
+import socket
 import subprocess
 import sys
 import time
@@ -45,45 +57,98 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
+# fp64_its: BiCGStab iterations per step of the reference's algorithm on the
+# workload (mean over the workload's steps, FP64 path on B200, which runs the
+# reference's BiCGStab and stop test); used only to scale the CPU samples of
+# grids too large to solve on the host within the benchmark's time.
 WORKLOADS = {
-    "dns128": dict(n=128, k0=4.0, nu=0.005, dt=0.0025, seed=0),
-    "dns256": dict(n=256, k0=4.0, nu=0.0025, dt=0.00125, seed=0),
-    "dns512": dict(n=512, k0=8.0, nu=0.0012, dt=0.001, seed=0),
+    "dns512": dict(n=512, k0=8.0, nu=0.0012, dt=0.001, seed=0, steps=50, fp64_its=1284),
+    "dns256": dict(n=256, k0=4.0, nu=0.0025, dt=0.00125, seed=0, steps=20, fp64_its=620),
+    "dns128": dict(n=128, k0=4.0, nu=0.005, dt=0.0025, seed=0, steps=100, fp64_its=306),
+    "dns64": dict(n=64, k0=4.0, nu=0.01, dt=0.005, seed=0, steps=20, fp64_its=150),
 }
+DEFAULT_WORKLOAD = "dns512"
 METRIC = "cell-steps/s (RK4+Poisson)"
 TOL = 1e-10
 MAX_IT = 20000
+SOLVER = {
+    "mixed_mg": "bicgstab right-preconditioned by an fp32 multigrid V(2,2) cycle, "
+                "inside fp64 iterative refinement",
+    "mixed": "fp32 bicgstab inside fp64 iterative refinement",
+    "fp64": "bicgstab (fp64, the reference's algorithm)",
+}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="dns128",
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
                     choices=sorted(WORKLOADS) + ["serve"])
-    ap.add_argument("--prec", default="mixed_mg", choices=["mixed_mg", "mixed", "fp64"],
-                    help="mixed_mg: FP32 refinement passes preconditioned by multigrid "
-                         "(default); mixed: unpreconditioned FP32 passes; fp64: the "
-                         "reference's FP64 algorithm")
+    ap.add_argument("--prec", default="mixed_mg", choices=["mixed_mg", "mixed", "fp64"])
     ap.add_argument("--path", default="graph", choices=["graph", "host"],
                     help="graph: captured steps replayed (default); host: host-driven "
                          "pf_forward_step per step (same kernels, host polls the solver)")
-    ap.add_argument("--no-fp64-arm", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=None,
+                    help="steps of the mixed-vs-FP64 comparison (default: the "
+                         "workload's step count; 0 skips it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the per-kernel, e2e and MLP measurements")
-    ap.add_argument("--cpu-sample-steps", type=int, default=8,
-                    help="oracle steps timed for cpu_baseline (about 10 s at 128^3)")
-    ap.add_argument("--requests", type=int, default=64,
+    ap.add_argument("--cpu-budget", type=float, default=25.0,
+                    help="seconds of oracle work for cpu_baseline / the reference arm step")
+    ap.add_argument("--ref-sample", action="store_true",
+                    help="reference arm: use the bounded per-step sample at any grid size")
+    ap.add_argument("--requests", type=int, default=512,
                     help="serve workload: number of requests")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def relaunch_command(argv, n, port):
+    """torch.distributed.run command that runs this script with n ranks."""
+    return ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run",
+            "--nnodes=1", "--nproc-per-node", str(n), "--master-addr", "127.0.0.1",
+            "--master-port", str(port), os.path.abspath(__file__)] + list(argv)
+
+
+def max_over_ranks(torch, dist, ms, device, world):
+    """The largest of the ranks' times (the job's time)."""
+    if world <= 1:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def config(a, wl):
+    """The workload, printed identically by both arms (how each arm computes
+    it is in the line's "method")."""
+    n = wl["n"]
+    return {"workload": a.workload, "grid": [n, n, n], "k0": wl["k0"], "nu": wl["nu"],
+            "dt": wl["dt"], "rho": 1.0, "tol": TOL, "steps_in_config": wl["steps"],
+            "advancer": "RK4", "seed": wl["seed"],
+            "l2": "working set > L2 (126 MB), no flush"}
+
+
+def method(a, world):
+    """How the GPU arm computes the workload."""
+    return {"precision": a.prec, "solver": SOLVER[a.prec],
+            "parallelism": "replicas" if world > 1 else "single",
+            "timing": ("captured-graph steps, device-side solver loops"
+                       if a.path == "graph" else "host-driven steps")}
 
 
 class Clocks:
@@ -141,7 +206,7 @@ class Clocks:
 
 def make_fields(wl, device=None):
     """Seeded spectral initial field as float64 numpy arrays (device FFTs
-    above 256^3)."""
+    above 256^3 when a device is given; same noise, same field)."""
     import pyflow_b200.initial as ic
     n = wl["n"]
     if n > 256 and device is not None:
@@ -155,21 +220,67 @@ def make_fields(wl, device=None):
     return ic.spectral_velocity((n, n, n), k0=wl["k0"], urms=1.0, seed=wl["seed"])
 
 
-def oracle_steps(wl, u0, v0, w0, steps, budget=None):
+def _oracle():
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
+    return O
+
+
+def oracle_full_steps(wl, u0, v0, w0, budget):
+    """Whole oracle steps from the initial field until ``budget`` seconds
+    pass (at least one); returns (seconds, iterations per step)."""
+    O = _oracle()
     n = wl["n"]
     sp = (2 * np.pi / n,) * 3
     u, v, w, p = u0.copy(), v0.copy(), w0.copy(), np.zeros_like(u0)
     t0 = time.perf_counter()
     its = []
-    for _ in range(steps):
+    while True:
         u, v, w, p, DP, r, it = O.forward_step(sp, u, v, w, p, wl["nu"], 1.0, wl["dt"],
                                                min_res=TOL, max_it=MAX_IT)
         its.append(it)
-        if budget and time.perf_counter() - t0 > budget:
+        if time.perf_counter() - t0 > budget:
             break
     return time.perf_counter() - t0, its
+
+
+def oracle_sampled_step(wl, u0, v0, w0, its_ref, m=(4, 24)):
+    """Bounded sample of one oracle step: the step run twice from the initial
+    field with the pressure solve cut at m[0] and m[1] BiCGStab iterations;
+    the difference gives the time per iteration, the rest the predictor,
+    divergence and projection; the step's time is scaled to ``its_ref``
+    iterations.  Returns (seconds per step, description)."""
+    O = _oracle()
+    n = wl["n"]
+    sp = (2 * np.pi / n,) * 3
+    ts = []
+    for mi in m:
+        t0 = time.perf_counter()
+        O.forward_step(sp, u0, v0, w0, np.zeros_like(u0), wl["nu"], 1.0, wl["dt"],
+                       min_res=TOL, max_it=mi)
+        ts.append(time.perf_counter() - t0)
+    t_it = max(0.0, (ts[1] - ts[0]) / (m[1] - m[0]))
+    t_fixed = max(0.0, ts[0] - m[0] * t_it)
+    t_step = t_fixed + its_ref * t_it
+    desc = ("bounded sample: one %d^3 step run twice from the seeded field with the "
+            "BiCGStab solve cut at %d and %d iterations (%.2f s, %.2f s): %.3f s predictor"
+            "+divergence+projection, %.4f s per iteration, scaled to %g iterations per step "
+            "(the reference's BiCGStab on this workload)"
+            % (n, m[0], m[1], ts[0], ts[1], t_fixed, t_it, its_ref))
+    return t_step, desc, sum(ts)
+
+
+def cpu_rate(wl, u0, v0, w0, budget, sampled, its_ref):
+    """Oracle cell-steps/s on the host cores: whole steps, or the bounded
+    sample.  Returns (value, sample description, seconds of work)."""
+    n = wl["n"]
+    if not sampled:
+        el, its = oracle_full_steps(wl, u0, v0, w0, budget)
+        return (n ** 3 * len(its) / el,
+                "%d whole FP64 step(s) of the %d^3 workload from the seeded field "
+                "(BiCGStab iterations %s)" % (len(its), n, its), el)
+    t_step, desc, work = oracle_sampled_step(wl, u0, v0, w0, its_ref)
+    return n ** 3 / t_step, desc, work
 
 
 def run_reference(a):
@@ -181,24 +292,34 @@ def run_reference(a):
                           "the reference has no serving path"}), flush=True)
         return
     wl = WORKLOADS[a.workload]
-    u0, v0, w0 = make_fields(wl)
     n = wl["n"]
-    if min(a.warmup, 1):
-        oracle_steps(wl, u0, v0, w0, 1)
-    el, its = oracle_steps(wl, u0, v0, w0, a.steps, budget=240.0)
-    done = len(its)
-    val = n ** 3 * done / el
-    sample = ("%d FP64 step(s) of the %d^3 workload from the seeded initial field "
-              "(BiCGStab iterations %s)" % (done, n, its))
+    dev = None
+    if n > 256:
+        try:
+            import torch
+            dev = torch.device("cuda", 0) if torch.cuda.is_available() else None
+        except ImportError:
+            dev = None
+    u0, v0, w0 = make_fields(wl, dev)
+    sampled = a.ref_sample or n >= 256
+    steps = max(1, a.steps)
+    warm = min(a.warmup, 1)
+    if warm and not sampled:
+        oracle_full_steps(wl, u0, v0, w0, 0.0)
+    vals, desc = [], ""
+    for _ in range(steps):
+        v, desc, _ = cpu_rate(wl, u0, v0, w0, a.cpu_budget / steps, sampled, wl["fp64_its"])
+        vals.append(v)
+    val = float(np.mean(vals))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": val, "unit": "cell-steps/s",
-        "n_gpus": a.gpus, "steps": done, "warmup": min(a.warmup, 1),
-        "ms_per_step": 1e3 * el / done, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": a.workload, "grid": [n, n, n], "nu": wl["nu"],
-                   "dt": wl["dt"], "tol": TOL, "solver": "bicgstab", "advancer": "RK4"},
+        "n_gpus": a.gpus, "steps": steps, "warmup": warm,
+        "ms_per_step": 1e3 * n ** 3 / val, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(a, wl),
+        "method": {"precision": "fp64", "solver": SOLVER["fp64"], "parallelism": "single",
+                   "timing": "host wall clock of oracle steps (rank 0 only)"},
         "cpu_baseline": {"value": val, "unit": "cell-steps/s", "cores": os.cpu_count(),
-                         "kind": "port", "sample": sample},
+                         "kind": "port", "sample": desc},
         "e2e": {"value": val, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}), flush=True)
 
@@ -212,14 +333,14 @@ def timed_plan(torch, dev, u0, v0, w0, wl, prec, steps, warmup, barrier, world, 
     sp = (2 * np.pi / n,) * 3
     f = [torch.tensor(x, device=dev) for x in (u0, v0, w0)]
     f += [torch.zeros_like(f[0]), torch.zeros_like(f[0])]
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if path == "host":
         import pyflow_b200.ops as ops
-        st = torch.cuda.current_stream(dev)
         for _ in range(warmup):
             ops.forward_step(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
                              prec=prec)
         barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         its, info = 0, None
         e0.record(st)
         for _ in range(steps):
@@ -228,39 +349,70 @@ def timed_plan(torch, dev, u0, v0, w0, wl, prec, steps, warmup, barrier, world, 
             its += info.iterations
         e1.record(st)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        sv = ops.stats(*f[:3], sp).cpu().tolist()
-        stats = dict(zip(("max_u", "max_v", "max_w", "tke", "max_div"), sv))
+        stats = dict(zip(("max_u", "max_v", "max_w", "tke", "max_div"),
+                         ops.stats(*f[:3], sp).cpu().tolist()))
         stats.update(max_res=info.max_res, iterations=info.iterations, status=info.status,
                      total_iterations=its, steps=steps)
-        return ms, stats, f
-    plan = StepPlan(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT, prec=prec)
-    st = torch.cuda.current_stream(dev)
-    plan.launch(warmup, stream=st)
-    barrier()
-    plan.reset_counters()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    plan.launch(steps, stream=st)
-    e1.record(st)
-    barrier()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    stats = plan.stats()
-    plan.close()
+    else:
+        plan = StepPlan(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
+                        prec=prec)
+        plan.launch(warmup, stream=st)
+        barrier()
+        plan.reset_counters()
+        e0.record(st)
+        plan.launch(steps, stream=st)
+        e1.record(st)
+        barrier()
+        stats = plan.stats()
+        plan.close()
+    ms = max_over_ranks(torch, dist, e0.elapsed_time(e1), dev, world)
     return ms, stats, f
 
 
+def e2e_measurement(torch, dev, wl, u0, v0, w0, prec, steps, barrier, world, dist):
+    """The metric through the public API with host buffers: every step copies
+    its state (u, v, w, p, FP64) from pinned host memory to the device and the
+    advanced state plus the step statistics back (plan.StepPipeline: two field
+    sets; host->device and device->host copies on their own streams, so both
+    copy directions and the computation overlap)."""
+    from pyflow_b200.plan import StepPipeline
+    n = wl["n"]
+    sp = (2 * np.pi / n,) * 3
+    hosts = [torch.tensor(x).pin_memory() for x in (u0, v0, w0)]
+    hosts.append(torch.zeros_like(hosts[0]).pin_memory())
+    outs = [[torch.empty_like(hosts[0]).pin_memory() for _ in range(4)] for _ in range(2)]
+    stat_out = [torch.zeros(10, dtype=torch.float64).pin_memory() for _ in range(2)]
+    pipe = StepPipeline((n, n, n), sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
+                        prec=prec, device=dev)
+    pipe.submit(*hosts, stat_out[0], state_out=outs[0])   # warm-up
+    pipe.synchronize()
+    barrier()
+    st = pipe.compute
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    pipe.start(e0)
+    for k in range(steps):
+        pipe.submit(*hosts, stat_out[k & 1], state_out=outs[k & 1])
+    pipe.finish(st)
+    e1.record(st)
+    barrier()
+    ms = max_over_ranks(torch, dist, e0.elapsed_time(e1), dev, world)
+    pipe.close()
+    # the round trip returned the state of a single step from (u0, v0, w0)
+    check = float(stat_out[(steps - 1) & 1][7])
+    del hosts, outs
+    return {"value": world * n ** 3 * steps / (ms / 1e3), "unit": "cell-steps/s",
+            "h2d_bytes_per_step": 4 * 8 * n ** 3, "d2h_bytes_per_step": 4 * 8 * n ** 3 + 80,
+            "steps": steps, "last_status": check,
+            "path": "pinned host u,v,w,p -> device (h2d stream) -> captured step -> "
+                    "u,v,w,p and statistics -> pinned host (d2h stream); two field sets, "
+                    "copies of neighbouring requests overlap the computation"}
+
+
 def mlp_measurement(torch, dev):
-    """Tensor-core MLP closure throughput (FLOPs of the three layers as padded
-    on the tensor cores: 2*(16*128 + 128*128 + 128*16) per cell)."""
+    """Tensor-core MLP closure throughput: FLOPs of the three layers as run on
+    the tensor cores (2*(16*128 + 128*128 + 128*16) per cell) and the useful
+    FLOPs of the 9 -> 128 -> 128 -> 6 network (2*(9*128 + 128*128 + 128*6))."""
     import pyflow_b200.initial as ic
     import pyflow_b200.sfsmodel_mlp as M
     import pyflow_b200.profiling as prof
@@ -280,9 +432,14 @@ def mlp_measurement(torch, dev):
         torch.cuda.synchronize(dev)
         kt = prof.read().get("mlp_closure")
         prof.enable(False)
-        flops = 2.0 * (16 * 128 + 128 * 128 + 128 * 16) * n ** 3
         ms = kt["ms"] / kt["launches"]
-        out["%d^3" % n] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+        padded = 2.0 * (16 * 128 + 128 * 128 + 128 * 16) * n ** 3
+        useful = 2.0 * (9 * 128 + 128 * 128 + 128 * 6) * n ** 3
+        pk, src = prof.tensor_peak()
+        out["%d^3" % n] = {"ms": ms, "tflops_padded": padded / (ms * 1e-3) / 1e12,
+                           "tflops_useful": useful / (ms * 1e-3) / 1e12,
+                           "frac_useful_of_bf16_peak": useful / (ms * 1e-3) / 1e12 / pk,
+                           "peak_tflops": pk, "peak_source": src}
         del u, v, w, res
     return out
 
@@ -290,15 +447,13 @@ def mlp_measurement(torch, dev):
 def run_serve(a, torch, dev):
     import pyflow_b200.serving as S
     sizes = (32, 48, 64, 96, 128, 192)
-    # capacity: run one request of each size alone (50 steps)
     srv = S.Server(max_slots=8, prec=a.prec, device=dev)
+    # capacity: requests of every size served back to back (50 steps each)
     cal = [S.Request(id=i, n=n, seed=999000 + i, nu=0.02 * 32 / n,
                      dt=0.3 * (2 * np.pi / n) / 4.0, steps=50) for i, n in enumerate(sizes)]
     t0 = time.perf_counter()
-    for r in cal:
-        srv.run([r])
-    per_req = (time.perf_counter() - t0) / len(cal)   # mean service time of a request
-    capacity = 1.0 / per_req
+    srv.run(cal)
+    capacity = len(cal) / (time.perf_counter() - t0)
     reqs = S.stream_requests(a.requests, sizes=sizes, steps=50, rate=0.8 * capacity)
     srv = S.Server(max_slots=8, prec=a.prec, device=dev)
     t0 = time.perf_counter()
@@ -313,7 +468,7 @@ def run_serve(a, torch, dev):
             "config": {"workload": "serve", "requests": a.requests, "sizes": list(sizes),
                        "steps_per_request": 50, "arrivals": "poisson",
                        "rate_per_s": 0.8 * capacity, "capacity_per_s": capacity,
-                       "max_slots": 8, "precision": a.prec},
+                       "max_slots": 8, "precision": a.prec, "solver": SOLVER[a.prec]},
             "p50_latency_s": summ["p50_latency_s"], "p99_latency_s": summ["p99_latency_s"],
             "completed": summ["completed"], "max_active": srv.max_active,
             "wall_s": wall}
@@ -353,101 +508,79 @@ def run_b200(a):
         ms, stats, fields = timed_plan(torch, dev, u0, v0, w0, wl, a.prec, a.steps,
                                        a.warmup, barrier, world, dist, a.path)
     clocks = clk.summary()
+    del fields
     value = world * n ** 3 * a.steps / (ms / 1e3)
     its_per_step = stats["total_iterations"] / max(1.0, stats["steps"])
 
+    # mixed vs FP64 over the workload's step count (rank 0 of a single-GPU
+    # run: the replicas would repeat the same numbers)
     fp64 = None
-    if a.prec != "fp64" and not a.no_fp64_arm:
-        ms64, st64, f64 = timed_plan(torch, dev, u0, v0, w0, wl, "fp64", a.steps, a.warmup,
-                                     barrier, world, dist, a.path)
-        err = max(float((x - y).abs().max() / y.abs().max()) for x, y in zip(fields[:3], f64[:3]))
-        fp64 = {"value": world * n ** 3 * a.steps / (ms64 / 1e3), "ms_per_step": ms64 / a.steps,
-                "iterations_per_step": st64["total_iterations"] / max(1.0, st64["steps"]),
-                "mixed_rel_velocity_err_vs_fp64": err,
-                "note": "same %d warm-up + %d timed steps from the same field" % (a.warmup, a.steps)}
-        del f64
-    del fields
+    acc_steps = wl["steps"] if a.accuracy_steps is None else a.accuracy_steps
+    if a.prec != "fp64" and acc_steps > 0 and world == 1:
+        from pyflow_b200.accuracy import compare_forms
+        rep = compare_forms(u0, v0, w0, sp, wl["nu"], wl["dt"], acc_steps, prec=a.prec,
+                            device=dev)
+        rep.pop("per_step")
+        fp64 = {"value": n ** 3 / (rep["fp64_ms_per_step"] / 1e3),
+                "ms_per_step": rep["fp64_ms_per_step"],
+                "iterations_per_step": rep["fp64_iterations_per_step"],
+                "solver": SOLVER["fp64"],
+                "errors_of_%s_vs_fp64" % a.prec: {
+                    k: rep[k] for k in ("steps", "u_rel_l2", "u_rel_linf", "ke_rel_err_max",
+                                        "dissipation_rel_err_max", "max_div_fp64",
+                                        "max_div_mixed", "ke_decay", "mixed_status",
+                                        "fp64_status")},
+                "note": "%d steps of each form from the same field, per-step flow statistics "
+                        "included in both times" % acc_steps}
+        torch.cuda.empty_cache()
 
     roof, ktimes, e2e, mlp, cpu = None, {}, None, None, None
+    prof_steps = 2
     if not a.no_extras:
-        # per-kernel device time (CUDA events around each launch of the
-        # host-driven path, which runs the same kernels as the graph)
+        # per-kernel device time: CUDA events around each launch of the
+        # host-driven path, which runs the kernels of the captured step
         prof.enable(True)
         f = [torch.tensor(x, device=dev) for x in (u0, v0, w0)]
         f += [torch.zeros_like(f[0]), torch.zeros_like(f[0])]
-        for _ in range(max(1, min(a.steps, 2))):
+        for _ in range(prof_steps):
             ops.forward_step(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
                              prec=a.prec)
         torch.cuda.synchronize(dev)
         ktimes = prof.read()
         prof.enable(False)
+        del f
         roof = prof.roofline(ktimes, n ** 3, a.prec)
         if roof is not None:
-            roof["step"] = prof.step_roofline(ktimes, n ** 3, max(1, min(a.steps, 2)),
-                                              ms / a.steps)
-        del f
-        # end to end through the public API with pinned host buffers: every
-        # step copies its input state in and reads the statistics back, the
-        # copy of step k+1 overlapping the computation of step k
-        # (plan.StepPipeline: two field sets, a copy stream)
-        from pyflow_b200.plan import StepPipeline
-        hosts = [torch.tensor(x).pin_memory() for x in (u0, v0, w0)]
-        hp = torch.zeros_like(hosts[0]).pin_memory()
-        pipe = StepPipeline((n, n, n), sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
-                            prec=a.prec, device=dev)
-        outs = [torch.zeros(10, dtype=torch.float64).pin_memory() for _ in range(2)]
-        st = pipe.compute
-        e2e_steps = max(2, min(a.steps, 10))
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        pipe.copy.wait_event(e0)
-        for k in range(e2e_steps):
-            pipe.submit(*hosts, hp, outs[k & 1])
-        pipe.copy.wait_stream(st)
-        st.wait_stream(pipe.copy)
-        e1.record(st)
-        barrier()
-        ms_e2e = e0.elapsed_time(e1)
-        pipe.close()
-        if world > 1:
-            t = torch.tensor([ms_e2e], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_e2e = float(t.item())
-        e2e = {"value": world * n ** 3 * e2e_steps / (ms_e2e / 1e3), "unit": "cell-steps/s",
-               "h2d_bytes_per_step": 4 * 8 * n ** 3, "d2h_bytes_per_step": 10 * 8,
-               "steps": e2e_steps,
-               "path": "pinned host u,v,w,p -> device (copy stream, overlapped with the previous "
-                       "step); captured step; stats -> host"}
-        del pipe, hosts
+            roof["step"] = prof.step_roofline(ktimes, n ** 3, prof_steps, ms / a.steps)
+            roof["kernel_times"] = ("CUDA events around every launch of %d host-driven steps "
+                                    "(%.3f ms of kernel time per step against %.3f ms per "
+                                    "graph-replayed step)"
+                                    % (prof_steps, sum(k["ms"] for k in ktimes.values())
+                                       / prof_steps, ms / a.steps))
+        torch.cuda.empty_cache()
+        e2e = e2e_measurement(torch, dev, wl, u0, v0, w0, a.prec, max(2, min(a.steps, 10)),
+                              barrier, world, dist)
         torch.cuda.empty_cache()
         if rank == 0:
             mlp = mlp_measurement(torch, dev)
     if rank == 0 and not a.no_cpu_baseline:
-        el, its = oracle_steps(wl, u0, v0, w0, a.cpu_sample_steps)
-        cpu = {"value": n ** 3 * len(its) / el, "unit": "cell-steps/s", "cores": os.cpu_count(),
-               "kind": "port",
-               "sample": "%d FP64 step(s) of the %d^3 workload from the same initial field "
-                         "(%s BiCGStab iterations), oracle/liboracle.so with OpenMP"
-                         % (len(its), n, its), "seconds": el}
+        its_ref = fp64["iterations_per_step"] if fp64 else wl["fp64_its"]
+        val, desc, work = cpu_rate(wl, u0, v0, w0, a.cpu_budget, n >= 256, its_ref)
+        cpu = {"value": val, "unit": "cell-steps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": desc + "; oracle/liboracle.so (FP64, OpenMP)", "seconds": work}
     launches_per_step = None
     if ktimes:
-        launches_per_step = sum(k["launches"] for k in ktimes.values()) / max(1, min(a.steps, 2))
+        launches_per_step = sum(k["launches"] for k in ktimes.values()) / prof_steps
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if a.prec != "fp64" else "f64", "data": "synthetic",
-            "config": {"workload": a.workload, "grid": [n, n, n], "k0": wl["k0"],
-                       "nu": wl["nu"], "dt": wl["dt"], "tol": TOL, "solver": "bicgstab",
-                       "advancer": "RK4", "precision": a.prec,
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "timing": ("captured-graph steps, device-side solver loops"
-                                  if a.path == "graph" else "host-driven steps"),
-                       "l2": "working set > L2, no flush"},
+            "config": config(a, wl), "method": method(a, world),
             "iterations_per_step": its_per_step,
-            "last_step": {k: stats[k] for k in ("max_res", "iterations", "status", "tke", "max_div")},
+            "last_step": {k: stats[k] for k in ("max_res", "iterations", "status", "tke",
+                                                "max_div")},
             "fp64_arm": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * a.steps)) if launches_per_step else None,
             "clocks": clocks, "mlp_tensor_core": mlp,
@@ -458,8 +591,12 @@ def run_b200(a):
         dist.destroy_process_group()
 
 
-def main():
-    a = parse()
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    a = parse(argv)
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: re-launch under torch.distributed.run
+        sys.exit(subprocess.call(relaunch_command(argv, a.gpus, free_port())))
     if a.impl == "reference":
         run_reference(a)
     else:

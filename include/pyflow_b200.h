@@ -134,6 +134,17 @@ int pf_stats(const pf_grid* g, const double* u, const double* v,
              const double* w, double* out_dev, void* ws, size_t ws_bytes,
              void* stream);
 
+/* pf_stats plus the dissipation rate: out_dev[0..5] = max|u|, max|v|, max|w|,
+ * TKE, max|div u| (as pf_stats, src/core/PyFlow.py:379-395) and
+ * eps = 2 nu <S_ij S_ij>, the mean over cells of the cell-centred strain rate
+ * of metric_uniform.grad_vel_center (src/metric/metric_staggered.py:215-268)
+ * with periodic wrap.  The reference computes no dissipation; this is the
+ * quantity its monitor would need for the energy budget dKE/dt = -eps.
+ * FP64, 6 doubles of DEVICE memory, asynchronous; ws as for pf_stats. */
+int pf_flow_stats(const pf_grid* g, const double* u, const double* v,
+                  const double* w, double nu, double* out_dev, void* ws,
+                  size_t ws_bytes, void* stream);
+
 /* Cell-centred SGS closures (FP64), computed from the cell-centred velocity
  * gradients of metric_uniform.grad_vel_center
  * (src/metric/metric_staggered.py:215-268) with periodic wrap:

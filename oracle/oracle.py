@@ -180,3 +180,38 @@ def stats(spacing, u, v, w):
     out = np.zeros(5)
     lib().or_stats(ctypes.byref(g), _p(u), _p(v), _p(w), _p(out))
     return out
+
+
+def grad_center(spacing, u, v, w):
+    """Cell-centred velocity gradients of metric_uniform.grad_vel_center
+    (src/metric/metric_staggered.py:215-268) with periodic wrap, as numpy:
+    the normal derivative is the difference of the two face values, a
+    transverse derivative the difference of the face-to-centre interpolant
+    averaged back to the neighbouring faces.  Returns the nine arrays
+    (ux, uy, uz, vx, vy, vz, wx, wy, wz)."""
+    u, v, w = _f64(u), _f64(v), _f64(w)
+    dxi, dyi, dzi = (1.0 / s for s in spacing)
+    sh = lambda a, ax, k: np.roll(a, -k, axis=ax)   # a[i + k] along ax
+
+    def tangential(f, ax_c, ax_t, di):
+        c0 = 0.5 * (sh(f, ax_c, 1) + f)          # value at the cell centre
+        cp, cm = sh(c0, ax_t, 1), sh(c0, ax_t, -1)
+        return (0.5 * (cp + c0) - 0.5 * (c0 + cm)) * di
+
+    ux = (sh(u, 0, 1) - u) * dxi
+    vy = (sh(v, 1, 1) - v) * dyi
+    wz = (sh(w, 2, 1) - w) * dzi
+    return (ux, tangential(u, 0, 1, dyi), tangential(u, 0, 2, dzi),
+            tangential(v, 1, 0, dxi), vy, tangential(v, 1, 2, dzi),
+            tangential(w, 2, 0, dxi), tangential(w, 2, 1, dyi), wz)
+
+
+def flow_stats(spacing, u, v, w, nu):
+    """Monitor statistics (src/core/PyFlow.py:379-395) plus the dissipation
+    rate eps = 2 nu <S_ij S_ij> of the cell-centred strain rate built from
+    grad_center: (max|u|, max|v|, max|w|, TKE, max|div u|, eps)."""
+    st = stats(spacing, u, v, w)
+    ux, uy, uz, vx, vy, vz, wx, wy, wz = grad_center(spacing, u, v, w)
+    s12, s13, s23 = 0.5 * (uy + vx), 0.5 * (uz + wx), 0.5 * (vz + wy)
+    ss = ((ux * ux + vy * vy) + wz * wz) + 2.0 * ((s12 * s12 + s13 * s13) + s23 * s23)
+    return np.concatenate([st, [2.0 * nu * ss.mean()]])

@@ -11,7 +11,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libpyflow_b200.so")
 
 PF_OK, PF_ERR_BAD_ARG, PF_ERR_CUDA, PF_BREAKDOWN, PF_MAXIT, PF_NONFINITE, \
-    PF_STAGNATION = range(7)
+    PF_STAGNATION, PF_ERR_TOO_LARGE = range(8)
 PF_FP64, PF_MIXED, PF_MIXED_MG = 0, 1, 2
 
 
@@ -59,6 +59,7 @@ def _load():
         "pf_forward_step": ([G, I, I, I, P, P, P, P, P, P, D, D, P, D, D, I, P,
                              S, P, ctypes.POINTER(SolveInfo)], I),
         "pf_stats": ([G, P, P, P, P, P, S, P], I),
+        "pf_flow_stats": ([G, P, P, P, D, P, P, S, P], I),
         "pf_sgs_closure": ([G, I, P, P, P, D, P, P], I),
         "pf_mlp_pack_bytes": ([], S),
         "pf_mlp_closure": ([G, P, P, P, P, P, P, P, P], I),

@@ -54,21 +54,28 @@ def build(force=False, verbose=False, ptxas_info=False):
     if not force and up_to_date():
         return OUT
     os.makedirs(OBJ, exist_ok=True)
-    objs = []
     nv = nvcc()
     extra = ["-Xptxas", "-v"] if ptxas_info else []
+    jobs = []
     for src in sources():
         obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
         cmd = [nv, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError("nvcc failed on " + src)
-        if ptxas_info or verbose:
-            sys.stderr.write(r.stderr)
+        # the translation units are independent: compile them concurrently
+        jobs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                                stderr=subprocess.PIPE, text=True)))
+    objs, failed = [], None
+    for src, obj, proc in jobs:
+        out, err = proc.communicate()
+        if proc.returncode != 0:
+            sys.stderr.write(out + err)
+            failed = failed or src
+        elif ptxas_info or verbose:
+            sys.stderr.write(err)
         objs.append(obj)
+    if failed:
+        raise RuntimeError("nvcc failed on " + failed)
     cmd = [nv, *ARCH, "-shared", "-o", OUT + ".tmp", *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -151,6 +151,14 @@ int pf_stats(const pf_grid* g, const double* u, const double* v,
     return cuda_rc(launch_stats(g, u, v, w, out_dev, ws, S(stream)));
 }
 
+int pf_flow_stats(const pf_grid* g, const double* u, const double* v,
+                  const double* w, double nu, double* out_dev, void* ws,
+                  size_t ws_bytes, void* stream) {
+    if (!grid_ok(g) || !u || !v || !w || !out_dev || !(nu >= 0.0)) return PF_ERR_BAD_ARG;
+    if (!ws || ws_bytes < stats_ws_bytes(g)) return PF_ERR_BAD_ARG;
+    return cuda_rc(launch_flow_stats(g, u, v, w, nu, out_dev, ws, S(stream)));
+}
+
 size_t pf_step_plan_workspace_bytes(const pf_grid* g, int prec) {
     if (!grid_ok(g) || !prec_ok(prec)) return 0;
     return step_plan_ws_bytes(g, prec);

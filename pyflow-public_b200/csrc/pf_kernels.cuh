@@ -39,6 +39,9 @@ size_t stats_ws_bytes(const pf_grid* g);
 cudaError_t launch_stats(const pf_grid* g, const double* u, const double* v,
                          const double* w, double* out, void* ws,
                          cudaStream_t s);
+cudaError_t launch_flow_stats(const pf_grid* g, const double* u, const double* v,
+                              const double* w, double nu, double* out, void* ws,
+                              cudaStream_t s);
 
 size_t step_plan_ws_bytes(const pf_grid* g, int prec);
 int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,

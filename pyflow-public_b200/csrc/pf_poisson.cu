@@ -40,6 +40,7 @@
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
 #include "pf_sweep.cuh"
+#include "pf_grad.cuh"
 #include "pf_mg.cuh"
 #include "pf_profile.cuh"
 
@@ -713,15 +714,18 @@ vel_corr_kernel(Dims d, const double* __restrict__ DP, double scale, double dxi,
     w[q] = fma(-scale, gz, w[q]);
 }
 
-// max|u|, max|v|, max|w|, sum(u^2+v^2+w^2), max|div u|: one warp per (i, j)
-// row of cells, its lanes along z (row and neighbour-row offsets computed
-// once per row)
+// max|u|, max|v|, max|w|, sum(u^2+v^2+w^2), max|div u| (and, with DISS, the
+// sum of S_ij S_ij of the cell-centred strain rate): one warp per (i, j) row
+// of cells, its lanes along z (row and neighbour-row offsets computed once per
+// row).  out[3] = TKE = 0.5 <u^2 + v^2 + w^2>, out[5] = 2 nu <S_ij S_ij>.
+template <bool DISS>
 __global__ void __launch_bounds__(256)
 stats_kernel(Dims d, BicgScalars* sc, double* part, const double* __restrict__ u,
              const double* __restrict__ v, const double* __restrict__ w,
-             double dxi, double dyi, double dzi, double* out) {
+             double dxi, double dyi, double dzi, double nu, double* out) {
+    constexpr int NC = DISS ? 6 : 5;
     __shared__ double sh[32];
-    double mu_ = 0, mv = 0, mw = 0, s = 0, md = 0;
+    double mu_ = 0, mv = 0, mw = 0, s = 0, md = 0, ss = 0;
     const int lane = threadIdx.x & 31;
     const int nrows = d.nx * d.ny, wpb = blockDim.x >> 5;
     for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < nrows; row += gridDim.x * wpb) {
@@ -738,41 +742,67 @@ stats_kernel(Dims d, BicgScalars* sc, double* part, const double* __restrict__ u
             dv += (v[by + k] - b) * dyi;
             dv += (w[base + wrap(k + 1, d.nz)] - c) * dzi;
             md = nanmax(md, fabs(dv));
+            if (DISS) {
+                const Grad9 g = grad_center(d, u, v, w, i, j, k, dxi, dyi, dzi);
+                const double s12 = 0.5 * (g.uy + g.vx);
+                const double s13 = 0.5 * (g.uz + g.wx);
+                const double s23 = 0.5 * (g.vz + g.wy);
+                ss += ((g.ux * g.ux + g.vy * g.vy) + g.wz * g.wz) +
+                      2.0 * ((s12 * s12 + s13 * s13) + s23 * s23);
+            }
         }
     }
-    double r[5] = {block_max<kBlock>(mu_, sh), block_max<kBlock>(mv, sh),
+    double r[6] = {block_max<kBlock>(mu_, sh), block_max<kBlock>(mv, sh),
                    block_max<kBlock>(mw, sh), block_sum<kBlock>(s, sh),
-                   block_max<kBlock>(md, sh)};
+                   block_max<kBlock>(md, sh), DISS ? block_sum<kBlock>(ss, sh) : 0.0};
     if (threadIdx.x == 0)
-        for (int c = 0; c < 5; ++c) part[c * kMaxPartials + blockIdx.x] = r[c];
+        for (int c = 0; c < NC; ++c) part[c * kMaxPartials + blockIdx.x] = r[c];
     if (arrive_last(sc)) {
-        double f[5];
-        for (int c = 0; c < 5; ++c)
-            f[c] = (c == 3) ? finish<false>(part + c * kMaxPartials, sh)
-                            : finish<true>(part + c * kMaxPartials, sh);
+        double f[6];
+        for (int c = 0; c < NC; ++c)
+            f[c] = (c == 3 || c == 5) ? finish<false>(part + c * kMaxPartials, sh)
+                                      : finish<true>(part + c * kMaxPartials, sh);
         if (threadIdx.x == 0) {
             out[0] = f[0]; out[1] = f[1]; out[2] = f[2];
             out[3] = f[3] / double(d.n) * 0.5;
             out[4] = f[4];
+            if (DISS) out[5] = 2.0 * nu * (f[5] / double(d.n));
             sc->counter = 0u;
         }
     }
 }
 
 size_t stats_ws_bytes(const pf_grid*) {
-    return align256(sizeof(BicgScalars)) + align256(5 * kMaxPartials * sizeof(double));
+    return align256(sizeof(BicgScalars)) + align256(6 * kMaxPartials * sizeof(double));
 }
 
-cudaError_t launch_stats(const pf_grid* g, const double* u, const double* v,
-                         const double* w, double* out, void* ws, cudaStream_t s) {
+static cudaError_t launch_stats_impl(const pf_grid* g, const double* u, const double* v,
+                                     const double* w, bool diss, double nu, double* out,
+                                     void* ws, cudaStream_t s) {
     Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     char* ptr = (char*)ws;
     BicgScalars* sc = (BicgScalars*)ptr; ptr += align256(sizeof(BicgScalars));
     double* part = (double*)ptr;
     cudaMemsetAsync(sc, 0, sizeof(BicgScalars), s);
-    PF_LAUNCH("stats", s, stats_kernel<<<pointwise_grid(d.n), kBlock, 0, s>>>(d, sc, part, u, v, w, 1.0 / g->dx,
-                                                       1.0 / g->dy, 1.0 / g->dz, out));
+    const double dxi = 1.0 / g->dx, dyi = 1.0 / g->dy, dzi = 1.0 / g->dz;
+    if (diss)
+        PF_LAUNCH("flow_stats", s, stats_kernel<true><<<pointwise_grid(d.n), kBlock, 0, s>>>(
+            d, sc, part, u, v, w, dxi, dyi, dzi, nu, out));
+    else
+        PF_LAUNCH("stats", s, stats_kernel<false><<<pointwise_grid(d.n), kBlock, 0, s>>>(
+            d, sc, part, u, v, w, dxi, dyi, dzi, 0.0, out));
     return cudaGetLastError();
+}
+
+cudaError_t launch_stats(const pf_grid* g, const double* u, const double* v,
+                         const double* w, double* out, void* ws, cudaStream_t s) {
+    return launch_stats_impl(g, u, v, w, false, 0.0, out, ws, s);
+}
+
+cudaError_t launch_flow_stats(const pf_grid* g, const double* u, const double* v,
+                              const double* w, double nu, double* out, void* ws,
+                              cudaStream_t s) {
+    return launch_stats_impl(g, u, v, w, true, nu, out, ws, s);
 }
 
 static dim3 cgrid(const Dims& d) { return dim3((d.nz + 31) / 32, (d.ny + 7) / 8, d.nx); }

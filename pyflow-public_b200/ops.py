@@ -197,6 +197,22 @@ def stats(u, v, w, spacing, out=None):
     return out
 
 
+def flow_stats(u, v, w, spacing, nu, out=None):
+    """Monitor statistics plus the dissipation rate (pf_flow_stats) as a
+    device tensor [max|u|, max|v|, max|w|, TKE, max|div u|, eps], with
+    eps = 2 nu <S_ij S_ij> from the cell-centred strain rate of
+    metric_uniform.grad_vel_center (src/metric/metric_staggered.py:215-268)."""
+    for t, nm in ((u, "u"), (v, "v"), (w, "w")):
+        _check(t, u.shape, torch.float64, nm)
+    out = torch.empty(6, dtype=torch.float64, device=u.device) if out is None else out
+    g = grid(u.shape, spacing)
+    ws = workspace(g, L.PF_FP64, u.device)
+    L.check("pf_flow_stats", L.lib().pf_flow_stats(
+        ctypes.byref(g), _p(u), _p(v), _p(w), float(nu), _p(out), _p(ws), ws.numel(),
+        _stream(u)))
+    return out
+
+
 SGS_MODELS = {"smagorinsky": (0, 1), "gradient": (1, 6), "gradients": (2, 9)}
 
 

@@ -79,17 +79,21 @@ class StepPipeline:
     """Independent time steps on states that arrive in pinned host memory
     (a request stream), with the host<->device copies overlapped with the
     computation: two field sets with one captured StepPlan each are used
-    alternately, so the copy of request k+1 runs on a copy stream (the copy
-    engines) while request k computes on the compute stream.  Ordering is by
-    events only; nothing here synchronises the host.
+    alternately; host->device copies run on one copy stream and
+    device->host copies on another (the two copy engines), so the input of
+    request k+1 and the output of request k-1 move while request k computes.
+    Ordering is by events only; nothing here synchronises the host.
 
     ``submit(u, v, w, p, stats_out, state_out=None)`` takes pinned host FP64
     tensors of the grid's shape and a pinned host FP64 tensor of 10 for the
     step's statistics (the layout of ``StepPlan.stats_dev``); with
     ``state_out`` (four pinned host tensors) the advanced u, v, w, p are
-    copied back too, on the copy stream.  The host tensors must stay
-    untouched until ``synchronize()`` (or a later event) shows the request
-    done.  DP starts from zero for every request, as in Domain.forwardStep.
+    copied back too.  The host tensors must stay untouched until
+    ``synchronize()`` (or a later event) shows the request done.  DP starts
+    from zero for every request, as in Domain.forwardStep.  ``start(event)``
+    makes the copy streams wait for an event of the caller (e.g. the start of
+    a timed region) and ``finish(stream)`` makes ``stream`` wait for all
+    submitted work.
     """
 
     def __init__(self, shape, spacing, mu, rho, dt, min_res=1e-10, max_it=20000,
@@ -100,7 +104,8 @@ class StepPipeline:
         self.plans = [StepPlan(*f, spacing, mu, rho, dt, min_res=min_res, max_it=max_it,
                                prec=prec, rk4=rk4) for f in self.sets]
         self.compute = stream if stream is not None else torch.cuda.current_stream(dev)
-        self.copy = torch.cuda.Stream(dev)
+        self.h2d = torch.cuda.Stream(dev)
+        self.d2h = torch.cuda.Stream(dev)
         self.ready = [torch.cuda.Event() for _ in range(2)]
         self.done = [torch.cuda.Event() for _ in range(2)]
         self.free = [torch.cuda.Event() for _ in range(2)]
@@ -108,35 +113,42 @@ class StepPipeline:
             e.record(self.compute)
         self.k = 0
 
+    def start(self, event):
+        self.h2d.wait_event(event)
+        self.d2h.wait_event(event)
+
     def submit(self, u, v, w, p, stats_out, state_out=None):
         s = self.k & 1
         f = self.sets[s]
         # the set is free once its previous request has computed and copied out
-        self.copy.wait_event(self.free[s])
-        with torch.cuda.stream(self.copy):
+        self.h2d.wait_event(self.free[s])
+        with torch.cuda.stream(self.h2d):
             for d, h in zip(f[:4], (u, v, w, p)):
                 d.copy_(h, non_blocking=True)
-        self.ready[s].record(self.copy)
+        self.ready[s].record(self.h2d)
         self.compute.wait_event(self.ready[s])
         with torch.cuda.stream(self.compute):
             f[4].zero_()
         self.plans[s].launch(1, stream=self.compute)
-        with torch.cuda.stream(self.compute):
+        self.done[s].record(self.compute)
+        self.d2h.wait_event(self.done[s])
+        with torch.cuda.stream(self.d2h):
             stats_out.copy_(self.plans[s].stats_dev, non_blocking=True)
-        if state_out is None:
-            self.free[s].record(self.compute)
-        else:
-            self.done[s].record(self.compute)
-            self.copy.wait_event(self.done[s])
-            with torch.cuda.stream(self.copy):
+            if state_out is not None:
                 for h, d in zip(state_out, f[:4]):
                     h.copy_(d, non_blocking=True)
-            self.free[s].record(self.copy)
+        self.free[s].record(self.d2h)
         self.k += 1
+
+    def finish(self, stream):
+        stream.wait_stream(self.h2d)
+        stream.wait_stream(self.d2h)
+        stream.wait_stream(self.compute)
 
     def synchronize(self):
         self.compute.synchronize()
-        self.copy.synchronize()
+        self.h2d.synchronize()
+        self.d2h.synchronize()
 
     def close(self):
         for pl in self.plans:

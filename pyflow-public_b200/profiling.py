@@ -83,6 +83,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def tensor_peak():
+    """Measured dense BF16 tensor throughput (TFLOP/s, the burst figure for a
+    kernel timed alone) with its source."""
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = os.path.join(here, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
 def traffic_table():
     """Per-launch DRAM bytes of the kernels captured with ncu (committed
     summary, scaled to cells); {kernel: bytes_per_cell} or {}."""

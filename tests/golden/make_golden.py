@@ -1,9 +1,9 @@
 """Generate golden fixtures by running the unmodified reference PyFlow.
 
-Run in a container that has the reference source tree (default
-``/root/reference``, override with PF_REFERENCE_ROOT):
+Run in a container that has the reference source tree, naming its root in
+PF_REFERENCE_ROOT (required; the directory that holds the reference's src/):
 
-    python tests/golden/make_golden.py
+    PF_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 
 Writes ``tests/golden/*.npz``.  The fixtures pin the CPU oracle
 (oracle/pf_oracle.c) to the reference, and the CUDA path to the oracle.  The

@@ -22,7 +22,8 @@ import types
 
 import numpy as np
 
-REF_ROOT = os.environ.get("PF_REFERENCE_ROOT", "/root/reference")
+# root of the reference checkout (the directory holding its src/); required
+REF_ROOT = os.environ.get("PF_REFERENCE_ROOT")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 _loaded = {}
@@ -33,6 +34,9 @@ def load_reference():
     its modules.  Returns a namespace of the reference modules."""
     if "ns" in _loaded:
         return _loaded["ns"]
+    if not REF_ROOT or not os.path.isdir(os.path.join(REF_ROOT, "src")):
+        raise RuntimeError("set PF_REFERENCE_ROOT to the reference checkout (the directory "
+                           "that holds its src/)")
     import torch  # noqa: F401  (the reference imports torch itself)
 
     tmp = tempfile.mkdtemp(prefix="pyflow_ref_")

@@ -117,3 +117,43 @@ def test_forward_run_64_twenty_steps(golden):
         m = g["moments"][mi]
         np.testing.assert_allclose((a * a).sum(), m[1], rtol=1e-9)
         np.testing.assert_allclose(np.abs(a).max(), m[2], rtol=tol)
+
+
+def test_grad_center_pinned_by_gradient_model_golden(golden):
+    """The numpy cell-centred gradients reproduce the reference's
+    gradient-model stresses (sfsmodel_gradient.py:77-148 on top of
+    grad_vel_center, metric_staggered.py:215-268) bit for bit."""
+    g = golden("sgs_12x16x20.npz")
+    ux, uy, uz, vx, vy, vz, wx, wy, wz = O.grad_center(g["spacing"], g["u"], g["v"], g["w"])
+    c = g["spacing"][0] ** 2 / 12.0
+    F = np.stack([((ux * ux + uy * uy) + uz * uz) * c, ((vx * vx + vy * vy) + vz * vz) * c,
+                  ((wx * wx + wy * wy) + wz * wz) * c, ((ux * vx + uy * vy) + uz * vz) * c,
+                  ((ux * wx + uy * wy) + uz * wz) * c, ((vx * wx + vy * wy) + vz * wz) * c])
+    assert np.array_equal(F, g["grad_F"])
+
+
+def _taylor_green(n):
+    """u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 at the staggered
+    face positions of an n^3 periodic box [0, 2 pi)^3."""
+    h = 2 * np.pi / n
+    f = np.arange(n) * h          # face coordinate
+    c = f + 0.5 * h               # centre coordinate
+    X, Yc, Zc = np.meshgrid(f, c, c, indexing="ij")
+    u = np.sin(X) * np.cos(Yc) * np.cos(Zc)
+    Xc, Y, Zc2 = np.meshgrid(c, f, c, indexing="ij")
+    v = -np.cos(Xc) * np.sin(Y) * np.cos(Zc2)
+    return u, v, np.zeros_like(u), (h, h, h)
+
+
+def test_dissipation_of_taylor_green_field():
+    """eps = 2 nu <S_ij S_ij> = 3/4 nu for the Taylor-Green field; the
+    second-order cell-centred gradients approach it as h^2."""
+    nu = 0.01
+    errs = []
+    for n in (16, 32):
+        u, v, w, sp = _taylor_green(n)
+        st = O.flow_stats(sp, u, v, w, nu)
+        assert np.array_equal(st[:5], O.stats(sp, u, v, w))
+        assert st[4] < 1e-12                      # discretely divergence free
+        errs.append(abs(st[5] / (0.75 * nu) - 1.0))
+    assert errs[1] < 1e-2 and 3.5 < errs[0] / errs[1] < 4.5, errs
