@@ -28,9 +28,10 @@ urms = 1, in place of the reference's DNS restart data):
   dns128  128^3, k0 = 4, nu = 0.005, dt = 0.0025, 100 steps
   dns256  256^3, k0 = 4, nu = 0.0025, dt = 0.00125 (profiling size)
   dns64   64^3, k0 = 4, nu = 0.01, dt = 0.005, 20 steps (FP64 plain DNS)
-  serve   request stream of 32..192^3 solves (50 steps each, nu = 0.02*32/N)
-          with Poisson arrivals at 80 % of the measured capacity; reports
-          p50/p99 latency and aggregate cell-steps/s
+  serve   only the request stream: 512 solves of 32..192^3 (50 steps each,
+          nu = 0.02*32/N) with Poisson arrivals at 80 % of the measured
+          capacity, batched serving; p50/p99 latency and aggregate
+          cell-steps/s (the main run reports the same under "serve")
 The per-step working set (> 0.3 GB) exceeds the 126 MB L2, so no explicit
 flush is done between steps.
 
@@ -103,6 +104,8 @@ def parse(argv=None):
                     help="reference arm: use the bounded per-step sample at any grid size")
     ap.add_argument("--requests", type=int, default=512,
                     help="serve workload: number of requests")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the request-stream measurement in the main run")
     return ap.parse_args(argv)
 
 
@@ -444,34 +447,46 @@ def mlp_measurement(torch, dev):
     return out
 
 
-def run_serve(a, torch, dev):
+def serve_measurement(a, torch, dev):
+    """The request-stream workload: capacity from a burst of requests of
+    every size served together, then ``a.requests`` requests with Poisson
+    arrivals at 80 % of that capacity through the batched server."""
     import pyflow_b200.serving as S
     sizes = (32, 48, 64, 96, 128, 192)
-    srv = S.Server(max_slots=8, prec=a.prec, device=dev)
-    # capacity: requests of every size served back to back (50 steps each)
-    cal = [S.Request(id=i, n=n, seed=999000 + i, nu=0.02 * 32 / n,
-                     dt=0.3 * (2 * np.pi / n) / 4.0, steps=50) for i, n in enumerate(sizes)]
+    slots = 8
+    burst = [S.Request(id=i, n=n, seed=999000 + i, nu=0.02 * 32 / n,
+                       dt=0.3 * (2 * np.pi / n) / 4.0, steps=50)
+             for i, n in enumerate(sizes * 4)]
+    S.Server(max_slots=slots, prec=a.prec, device=dev).run(burst[:len(sizes)])   # warm-up
     t0 = time.perf_counter()
-    srv.run(cal)
-    capacity = len(cal) / (time.perf_counter() - t0)
+    S.Server(max_slots=slots, prec=a.prec, device=dev).run(burst)
+    capacity = len(burst) / (time.perf_counter() - t0)
     reqs = S.stream_requests(a.requests, sizes=sizes, steps=50, rate=0.8 * capacity)
-    srv = S.Server(max_slots=8, prec=a.prec, device=dev)
+    srv = S.Server(max_slots=slots, prec=a.prec, device=dev)
     t0 = time.perf_counter()
     res = srv.run(reqs)
     wall = time.perf_counter() - t0
     summ = S.summarize(res, wall)
+    return {"requests": a.requests, "completed": summ["completed"],
+            "p50_latency_s": summ["p50_latency_s"], "p99_latency_s": summ["p99_latency_s"],
+            "cell_steps_per_s": summ["cell_steps_per_s"], "wall_s": wall,
+            "capacity_requests_per_s": capacity, "rate_requests_per_s": 0.8 * capacity,
+            "sizes": list(sizes), "steps_per_request": 50, "arrivals": "poisson",
+            "max_slots": slots, "max_active": srv.max_active, "batch_graphs": srv.rebuilds,
+            "precision": a.prec, "solver": SOLVER[a.prec],
+            "mode": "batched: one graph per active set, RK4 stages of all requests as one "
+                    "grouped launch per stage, solves as parallel graph branches; "
+                    "admission by live free HBM"}
+
+
+def run_serve(a, torch, dev):
+    sv = serve_measurement(a, torch, dev)
     line = {"metric": "serve latency p50/p99 (s) and aggregate cell-steps/s",
-            "value": summ["cell_steps_per_s"], "unit": "cell-steps/s", "n_gpus": 1,
+            "value": sv["cell_steps_per_s"], "unit": "cell-steps/s", "n_gpus": 1,
             "steps": 50, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": "serve", "requests": a.requests, "sizes": list(sizes),
-                       "steps_per_request": 50, "arrivals": "poisson",
-                       "rate_per_s": 0.8 * capacity, "capacity_per_s": capacity,
-                       "max_slots": 8, "precision": a.prec, "solver": SOLVER[a.prec]},
-            "p50_latency_s": summ["p50_latency_s"], "p99_latency_s": summ["p99_latency_s"],
-            "completed": summ["completed"], "max_active": srv.max_active,
-            "wall_s": wall}
+            "data": "synthetic", "config": {"workload": "serve", "requests": a.requests},
+            "serve": sv}
     print(json.dumps(line), flush=True)
 
 
@@ -534,7 +549,7 @@ def run_b200(a):
                         "included in both times" % acc_steps}
         torch.cuda.empty_cache()
 
-    roof, ktimes, e2e, mlp, cpu = None, {}, None, None, None
+    roof, ktimes, e2e, mlp, cpu, serve = None, {}, None, None, None, None
     prof_steps = 2
     if not a.no_extras:
         # per-kernel device time: CUDA events around each launch of the
@@ -563,6 +578,10 @@ def run_b200(a):
         torch.cuda.empty_cache()
         if rank == 0:
             mlp = mlp_measurement(torch, dev)
+            torch.cuda.empty_cache()
+            if not a.no_serve and world == 1:
+                serve = serve_measurement(a, torch, dev)
+                torch.cuda.empty_cache()
     if rank == 0 and not a.no_cpu_baseline:
         its_ref = fp64["iterations_per_step"] if fp64 else wl["fp64_its"]
         val, desc, work = cpu_rate(wl, u0, v0, w0, a.cpu_budget, n >= 256, its_ref)
@@ -583,7 +602,7 @@ def run_b200(a):
                                                 "max_div")},
             "fp64_arm": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * a.steps)) if launches_per_step else None,
-            "clocks": clocks, "mlp_tensor_core": mlp,
+            "clocks": clocks, "mlp_tensor_core": mlp, "serve": serve,
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ktimes.items()},
         }
         print(json.dumps(line), flush=True)

@@ -229,6 +229,41 @@ int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u,
 int pf_step_plan_launch(pf_step_plan* plan, int nsteps, void* stream);
 int pf_step_plan_destroy(pf_step_plan* plan);
 
+/* A batch of independent time steps (the serving loop's active requests,
+ * any grid sizes, one precision form) captured as ONE CUDA graph: each
+ * replay advances every member by one Domain.forwardStep
+ * (src/data/domain.py:342-402; constant viscosity, no SFS model).  The RK4
+ * stages of all members run as one grouped launch per stage (a persistent
+ * kernel walking the members' tiles, src/solver/advancer.py:75-113), then
+ * each member's divergence, pressure solve (device-side WHILE loops),
+ * projection and statistics run as independent branches of the graph, so
+ * the members' solves overlap on the device.  Every member computes exactly
+ * what its own pf_step_plan would: results are the same alone and in any
+ * batch.  A member's fields, workspace (pf_step_plan_workspace_bytes) and
+ * stats (10 doubles, the layout of pf_step_plan_create) belong to the plan
+ * while it exists; table is a caller device buffer of
+ * pf_batch_table_bytes(count) bytes (256-byte aligned) that holds the
+ * grouped launches' per-member arguments.  At most 64 members.  A member
+ * with fresh != 0 joins a plan for the first time: creation initialises its
+ * solver state (synchronously, on a stream of its own).  A member with
+ * fresh == 0 is carried over from an earlier plan, whose launches may still
+ * be running: creation does not touch its memory, and launches of the new
+ * plan on the same stream follow the old plan's in stream order. */
+typedef struct pf_batch_member {
+    pf_grid grid;
+    double *u, *v, *w, *p, *DP;
+    double mu, rho, dt, min_res;
+    int max_it;
+    int fresh;
+    void* ws;
+    size_t ws_bytes;
+    double* stats;
+} pf_batch_member;
+size_t pf_batch_table_bytes(int count);
+int pf_batch_plan_create(int prec, int rk4, const pf_batch_member* members,
+                         int count, void* table, size_t table_bytes,
+                         pf_step_plan** plan);
+
 /* Optional per-kernel device-time accounting: when enabled, each kernel launch
  * of the library is bracketed by CUDA events on its stream.  pf_profile_read
  * waits for pending events and fills up to max_entries records (per kernel

@@ -60,12 +60,16 @@ def sfs_adjoint_accumulate(lam, spacing, weight, out):
         float(weight), ops._p(out), ops._stream(lam[0])))
 
 
-def project(vel, spacing, rho, dt, tol=1e-12, max_it=20000):
-    """In-place projection P vel = vel - G L^-1 D vel (FP64 BiCGStab)."""
+def project(vel, spacing, rho, dt, tol=1e-12, max_it=20000, p=None, DP=None):
+    """In-place projection P vel = vel - G L^-1 D vel (FP64 BiCGStab): the
+    target-data corrector Domain.TargetDataVelCorr (src/data/domain.py:445-468),
+    divergence, pressure solve from DP = 0, vel -= dt/rho grad DP.  The
+    reference's solve also adds DP to the pressure it is given (the
+    simulation's p): pass ``p`` to get that; ``DP`` receives the solution."""
     u, v, w = vel
     src = ops.div_vel(u, v, w, spacing)
-    DP = torch.zeros_like(u)
-    p = torch.zeros_like(u)
+    DP = torch.zeros_like(u) if DP is None else DP.zero_()
+    p = torch.zeros_like(u) if p is None else p
     info = ops.bicgstab_solve(src, DP, p, spacing, rho, dt, tol, max_it)
     ops.vel_corr(DP, dt / rho, u, v, w, spacing)
     return info
@@ -296,7 +300,7 @@ def run_training(inputConfig, comms, decomp, geometry, metric, D, startTime):
             tgt = [torch.tensor(data[..., c], dtype=torch.float64, device=state[0].device)
                    for c in range(3)]
             if getattr(inputConfig, "targetDataVelCorr", False):
-                project(tgt, sp, rho, simDt, tol, max_it)
+                project(tgt, sp, rho, simDt, tol, max_it, p=D.state_p_P.interior())
             L = sum(torch.sum(torch.abs(c - g)) for c, g in zip(cur, tgt)) / n
             L.backward()
             if model is not None:

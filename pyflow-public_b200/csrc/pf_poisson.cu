@@ -943,166 +943,295 @@ size_t step_plan_ws_bytes(const pf_grid* g, int prec) {
            align256(kNumPartials * kMaxPartials * sizeof(double)) + align256(r) + pinv;
 }
 
-int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
-                     double* w, double* p, double* DP, double mu, double rho,
-                     double dt, double min_res, int max_it, void* ws,
-                     double* stats, void** out) {
-    Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
-    const size_t n = (size_t)d.n;
+// Pointers of one request's plan workspace (see step_plan_ws_bytes).
+struct PlanLayout {
+    Dims d;
+    double* div;
+    BicgScalars* sc;
+    double* part;
+    char* R;
+    BicgVecs<double> v64;
+    BicgVecs<float> v32;
+    float* e32;
+    double *bb, *rr;
+    MgPlan mg;
+};
+
+static int plan_layout(const pf_grid* g, int prec, void* ws, PlanLayout* L) {
+    L->d = Dims{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
+    const size_t n = (size_t)L->d.n;
     char* ptr = (char*)ws;
-    double* div = (double*)ptr; ptr += align256(n * sizeof(double));
-    BicgScalars* sc = (BicgScalars*)ptr; ptr += align256(sizeof(BicgScalars));
-    double* part = (double*)ptr; ptr += align256(kNumPartials * kMaxPartials * sizeof(double));
-    char* R = ptr;
+    L->div = (double*)ptr; ptr += align256(n * sizeof(double));
+    L->sc = (BicgScalars*)ptr; ptr += align256(sizeof(BicgScalars));
+    L->part = (double*)ptr; ptr += align256(kNumPartials * kMaxPartials * sizeof(double));
+    L->R = ptr;
+    // FP64 vectors, or FP32 vectors + correction followed by b and r (FP64)
+    char* vp = L->R;
+    L->v64 = carve<double>(vp, n);
+    vp = L->R;
+    L->v32 = carve<float>(vp, n);
+    L->e32 = (float*)vp;
+    L->bb = (double*)(L->R + 9 * align256(n * sizeof(double)));
+    L->rr = (double*)(L->R + 10 * align256(n * sizeof(double)));
+    // PF_MIXED_MG: multigrid-preconditioned inner passes when the grid
+    // coarsens (vectors in the region of the FP32 solver vectors)
+    L->mg = MgPlan();
+    if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
+        const int e = mg_setup(g, L->R, &L->mg);
+        if (e != PF_OK && e != PF_ERR_BAD_ARG) return e;
+        // the pseudo-inverse lives in the last slot of the workspace, outside
+        // the region the predictor overwrites, and is computed once here
+        if (L->mg.L && L->mg.pinv)
+            L->mg.pinv = (float*)((char*)ws + step_plan_ws_bytes(g, prec) - kPlanPinvBytes);
+    }
+    return PF_OK;
+}
+
+// Adds one request's step after the predictor (node `dep`) to graph G:
+// divergence and solver set-up, the solver's WHILE loop(s), then p += DP,
+// the projection and the monitor statistics.  *end gets the last node.
+static int add_solve_chain(cudaGraph_t G, cudaGraphNode_t dep, const pf_grid* g, int prec,
+                           PlanLayout& P, double* u, double* v, double* w, double* p,
+                           double* DP, double rho, double dt, double min_res, int max_it,
+                           double* stats, cudaStream_t cs, cudaGraphNode_t* end) {
+    const Dims d = P.d;
+    BicgScalars* sc = P.sc;
+    double* part = P.part;
     const int gp = pointwise_grid(d.n);
     const double vol = (g->dx * g->dy) * g->dz;
     const double c1 = rho / dt, c2 = -1.0 * vol;
     max_it = std::max(max_it, 1);
     dim3 blk2(32, 8);
-    // FP64 vectors, or FP32 vectors + correction followed by b and r (FP64)
-    char* vp = R;
-    BicgVecs<double> v64 = carve<double>(vp, n);
-    vp = R;
-    BicgVecs<float> v32 = carve<float>(vp, n);
-    float* e32 = (float*)vp;
-    double* bb = (double*)(R + 9 * align256(n * sizeof(double)));
-    double* rr = (double*)(R + 10 * align256(n * sizeof(double)));
-    // PF_MIXED_MG: multigrid-preconditioned inner passes when the grid
-    // coarsens (vectors in the region of the FP32 solver vectors)
-    MgPlan mg;
-    if (prec == PF_MIXED_MG && mg_region_bytes(g) <= 9 * align256(n * sizeof(double))) {
-        const int e = mg_setup(g, R, &mg);
-        if (e != PF_OK && e != PF_ERR_BAD_ARG) return e;
-        // the pseudo-inverse lives in the last slot of the workspace, outside
-        // the region the predictor overwrites, and is computed once here
-        if (mg.L && mg.pinv)
-            mg.pinv = (float*)((char*)ws + step_plan_ws_bytes(g, prec) - kPlanPinvBytes);
+    int rc = PF_OK;
+    // ---- divergence, solver set-up
+    cudaGraph_t seg1 = nullptr;
+    if ((rc = capture_begin(cs, nullptr))) return rc;
+    launch_div(g, u, v, w, P.div, cs);
+    if (prec == PF_FP64) {
+        const LapCoef<double> cf = lap_coef<double>(g);
+        const Tiling ta = make_tiling(d, 8 * PhaseCA<double>::R);
+        bicg_init<double, false><<<gp, kBlock, 0, cs>>>(d, sc, part, P.div, c1, c2, P.v64, DP,
+                                                       max_it, min_res);
+        bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v64, DP);
+    } else {
+        mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, P.div, c1, c2, P.bb, DP, P.rr);
     }
+    if ((rc = capture_end(cs, &seg1))) return rc;
+    cudaGraphNode_t n1, nw;
+    rc = add_child(G, dep, seg1, &n1);
+    cudaGraphDestroy(seg1);
+    if (rc) return rc;
+    cudaGraph_t body;
+    cudaGraphConditionalHandle h;
+    if ((rc = add_while(G, n1, &nw, &body, &h))) return rc;
+    if (prec == PF_FP64) {
+        const LapCoef<double> cf = lap_coef<double>(g);
+        const Tiling ta = make_tiling(d, 8 * PhaseCA<double>::R);
+        const Tiling tb = make_tiling(d, 8 * PhaseB<double>::R);
+        if ((rc = capture_begin(cs, body))) return rc;
+        bicg_b<double><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, P.v64, 1, h);
+        bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v64, DP, 1, h);
+        if ((rc = capture_end(cs, &body))) return rc;
+    } else {
+        const LapCoef<float> cf = lap_coef<float>(g);
+        const LapCoef<double> cfd = lap_coef<double>(g);
+        const Tiling ta = make_tiling(d, 8 * PhaseCA<float>::R);
+        const Tiling tb = make_tiling(d, 8 * PhaseB<float>::R);
+        const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
+        const double kInnerTol = 1e-4;
+        const MgPlan& mg = P.mg;
+        float* ecorr = mg.L ? mg.e : P.e32;
+        // outer body: inner set-up, inner WHILE, fold + residual + control
+        cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;
+        if ((rc = capture_begin(cs, nullptr))) return rc;
+        if (mg.L) {
+            mg_enqueue_init(mg, sc, part, P.rr, kInnerTol, max_it, cs, min_res);
+        } else {
+            bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, P.rr, 0.0, 0.0, P.v32,
+                                                         P.e32, max_it, kInnerTol);
+            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v32, P.e32);
+        }
+        if ((rc = capture_end(cs, &pre))) return rc;
+        cudaGraphNode_t b0, b1, bw, b3;
+        cudaGraphConditionalHandle hi;
+        if (cudaGraphConditionalHandleCreate(&hi, body, 1, cudaGraphCondAssignDefault) !=
+            cudaSuccess) return PF_ERR_CUDA;
+        {
+            // kernel node of the outer body (the graph that owns the inner
+            // loop) that re-arms the inner condition every pass
+            cudaKernelNodeParams kp;
+            std::memset(&kp, 0, sizeof(kp));
+            void* args[] = {&hi};
+            kp.func = (void*)arm_condition;
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(32);
+            kp.kernelParams = args;
+            if (cudaGraphAddKernelNode(&b0, body, nullptr, 0, &kp) != cudaSuccess)
+                return PF_ERR_CUDA;
+        }
+        rc = add_child(body, b0, pre, &b1);
+        cudaGraphDestroy(pre);
+        if (rc) return rc;
+        if ((rc = add_while(body, b1, &bw, &inner_body, &hi, false))) return rc;
+        if ((rc = capture_begin(cs, inner_body))) return rc;
+        if (mg.L) {
+            // two iterations per pass of the body: the p buffers alternate
+            mg_enqueue_iteration(mg, sc, part, 0, cs, 1, hi);
+            mg_enqueue_iteration(mg, sc, part, 1, cs, 1, hi);
+        } else {
+            bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, P.v32, 1, hi);
+            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v32, P.e32,
+                                                           1, hi);
+        }
+        if ((rc = capture_end(cs, &inner_body))) return rc;
+        if ((rc = capture_begin(cs, nullptr))) return rc;
+        fold_correction<float><<<gp, kBlock, 0, cs>>>(d, sc, ecorr, DP, 1);
+        mixed_residual<<<tiled_grid(tld), blk2, 0, cs>>>(d, tld, cfd, sc, part, P.bb, DP, P.rr);
+        mixed_control<<<1, 32, 0, cs>>>(sc, min_res, 40, max_it, h);
+        if ((rc = capture_end(cs, &post))) return rc;
+        rc = add_child(body, bw, post, &b3);
+        cudaGraphDestroy(post);
+        if (rc) return rc;
+    }
+    // ---- p += DP, projection, statistics
+    cudaGraph_t seg3 = nullptr;
+    if ((rc = capture_begin(cs, nullptr))) return rc;
+    step_info<<<1, 32, 0, cs>>>(sc, prec != PF_FP64 ? 1 : 0, stats + 5);
+    add_inplace<<<gp, kBlock, 0, cs>>>(d.n, DP, p);
+    launch_vel_corr(g, DP, dt / rho, u, v, w, cs);
+    launch_stats(g, u, v, w, stats, P.R, cs);
+    if ((rc = capture_end(cs, &seg3))) return rc;
+    rc = add_child(G, nw, seg3, end);
+    cudaGraphDestroy(seg3);
+    return rc;
+}
+
+// Captures the body of `enqueue(cs)` as a child node of G (no dependency).
+template <class F>
+static int add_captured(cudaGraph_t G, cudaStream_t cs, F enqueue, cudaGraphNode_t* node) {
+    cudaGraph_t seg = nullptr;
+    int rc = capture_begin(cs, nullptr);
+    if (rc) return rc;
+    const cudaError_t e = enqueue(cs);
+    rc = capture_end(cs, &seg);
+    if (rc) return rc;
+    if (e != cudaSuccess) { cudaGraphDestroy(seg); return PF_ERR_CUDA; }
+    rc = add_child(G, nullptr, seg, node);
+    cudaGraphDestroy(seg);
+    return rc;
+}
+
+static void plan_free(StepPlan* plan) {
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    delete plan;
+}
+
+int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
+                     double* w, double* p, double* DP, double mu, double rho,
+                     double dt, double min_res, int max_it, void* ws,
+                     double* stats, void** out) {
+    PlanLayout P;
+    int rc = plan_layout(g, prec, ws, &P);
+    if (rc != PF_OK) return rc;
     if (predictor_prepare(prec) != cudaSuccess) return PF_ERR_CUDA;
     cudaStream_t cs;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return PF_ERR_CUDA;
-    if (mg.L) {
-        if (mg_enqueue_setup(mg, cs) != PF_OK || cudaStreamSynchronize(cs) != cudaSuccess) {
+    if (P.mg.L) {
+        if (mg_enqueue_setup(P.mg, cs) != PF_OK || cudaStreamSynchronize(cs) != cudaSuccess) {
             cudaStreamDestroy(cs);
             return PF_ERR_CUDA;
         }
     }
     prof_suspend(true);
     StepPlan* plan = new StepPlan();
-    int rc = PF_OK;
     do {
         if (cudaGraphCreate(&plan->graph, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
         cudaGraph_t G = plan->graph;
-        // ---- segment 1: predictor, divergence, solver set-up
-        cudaGraph_t seg1 = nullptr;
-        if ((rc = capture_begin(cs, nullptr))) break;
-        launch_predictor(g, prec, rk4, u, v, w, nullptr, mu, rho, nullptr, dt, R, cs);
-        launch_div(g, u, v, w, div, cs);
-        if (prec == PF_FP64) {
-            const LapCoef<double> cf = lap_coef<double>(g);
-            const Tiling ta = make_tiling(d, 8 * PhaseCA<double>::R);
-            bicg_init<double, false><<<gp, kBlock, 0, cs>>>(d, sc, part, div, c1, c2, v64, DP,
-                                                           max_it, min_res);
-            bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v64, DP);
-        } else {
-            mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, div, c1, c2, bb, DP, rr);
-        }
-        if ((rc = capture_end(cs, &seg1))) break;
-        cudaGraphNode_t n1, nw;
-        if ((rc = add_child(G, nullptr, seg1, &n1))) break;
-        cudaGraphDestroy(seg1);
-        cudaGraph_t body;
-        cudaGraphConditionalHandle h;
-        if ((rc = add_while(G, n1, &nw, &body, &h))) break;
-        if (prec == PF_FP64) {
-            const LapCoef<double> cf = lap_coef<double>(g);
-            const Tiling ta = make_tiling(d, 8 * PhaseCA<double>::R);
-            const Tiling tb = make_tiling(d, 8 * PhaseB<double>::R);
-            if ((rc = capture_begin(cs, body))) break;
-            bicg_b<double><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, v64, 1, h);
-            bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v64, DP, 1, h);
-            if ((rc = capture_end(cs, &body))) break;
-        } else {
-            const LapCoef<float> cf = lap_coef<float>(g);
-            const LapCoef<double> cfd = lap_coef<double>(g);
-            const Tiling ta = make_tiling(d, 8 * PhaseCA<float>::R);
-            const Tiling tb = make_tiling(d, 8 * PhaseB<float>::R);
-            const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
-            const double kInnerTol = 1e-4;
-            float* ecorr = mg.L ? mg.e : e32;
-            // outer body: inner set-up, inner WHILE, fold + residual + control
-            cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;
-            if ((rc = capture_begin(cs, nullptr))) break;
-            if (mg.L) {
-                mg_enqueue_init(mg, sc, part, rr, kInnerTol, max_it, cs, min_res);
-            } else {
-                bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, rr, 0.0, 0.0, v32, e32,
-                                                             max_it, kInnerTol);
-                bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32);
-            }
-            if ((rc = capture_end(cs, &pre))) break;
-            cudaGraphNode_t b0, b1, bw, b3;
-            cudaGraphConditionalHandle hi;
-            if (cudaGraphConditionalHandleCreate(&hi, body, 1, cudaGraphCondAssignDefault) !=
-                cudaSuccess) { rc = PF_ERR_CUDA; break; }
-            {
-                // kernel node of the outer body (the graph that owns the
-                // inner loop) that re-arms the inner condition every pass
-                cudaKernelNodeParams kp;
-                std::memset(&kp, 0, sizeof(kp));
-                void* args[] = {&hi};
-                kp.func = (void*)arm_condition;
-                kp.gridDim = dim3(1);
-                kp.blockDim = dim3(32);
-                kp.kernelParams = args;
-                if (cudaGraphAddKernelNode(&b0, body, nullptr, 0, &kp) != cudaSuccess) {
-                    rc = PF_ERR_CUDA; break;
-                }
-            }
-            if ((rc = add_child(body, b0, pre, &b1))) break;
-            cudaGraphDestroy(pre);
-            if ((rc = add_while(body, b1, &bw, &inner_body, &hi, false))) break;
-            if ((rc = capture_begin(cs, inner_body))) break;
-            if (mg.L) {
-                // two iterations per pass of the body: the p buffers alternate
-                mg_enqueue_iteration(mg, sc, part, 0, cs, 1, hi);
-                mg_enqueue_iteration(mg, sc, part, 1, cs, 1, hi);
-            } else {
-                bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, v32, 1, hi);
-                bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, v32, e32, 1, hi);
-            }
-            if ((rc = capture_end(cs, &inner_body))) break;
-            if ((rc = capture_begin(cs, nullptr))) break;
-            fold_correction<float><<<gp, kBlock, 0, cs>>>(d, sc, ecorr, DP, 1);
-            mixed_residual<<<tiled_grid(tld), blk2, 0, cs>>>(d, tld, cfd, sc, part, bb, DP, rr);
-            mixed_control<<<1, 32, 0, cs>>>(sc, min_res, 40, max_it, h);
-            if ((rc = capture_end(cs, &post))) break;
-            if ((rc = add_child(body, bw, post, &b3))) break;
-            cudaGraphDestroy(post);
-        }
-        // ---- segment 3: p += DP, projection, statistics
-        cudaGraph_t seg3 = nullptr;
-        cudaGraphNode_t n3;
-        if ((rc = capture_begin(cs, nullptr))) break;
-        step_info<<<1, 32, 0, cs>>>(sc, prec != PF_FP64 ? 1 : 0, stats + 5);
-        add_inplace<<<gp, kBlock, 0, cs>>>(d.n, DP, p);
-        launch_vel_corr(g, DP, dt / rho, u, v, w, cs);
-        launch_stats(g, u, v, w, stats, R, cs);
-        if ((rc = capture_end(cs, &seg3))) break;
-        if ((rc = add_child(G, nw, seg3, &n3))) break;
-        cudaGraphDestroy(seg3);
+        cudaGraphNode_t n0, nend;
+        if ((rc = add_captured(G, cs, [&](cudaStream_t st) {
+                 return launch_predictor(g, prec, rk4, u, v, w, nullptr, mu, rho, nullptr, dt,
+                                         P.R, st);
+             }, &n0)))
+            break;
+        if ((rc = add_solve_chain(G, n0, g, prec, P, u, v, w, p, DP, rho, dt, min_res, max_it,
+                                  stats, cs, &nend)))
+            break;
         if (cudaGraphInstantiate(&plan->exec, G, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
     } while (0);
     prof_suspend(false);
     if (rc == PF_OK &&
-        (cudaMemsetAsync(sc, 0, sizeof(BicgScalars), cs) != cudaSuccess ||
+        (cudaMemsetAsync(P.sc, 0, sizeof(BicgScalars), cs) != cudaSuccess ||
          cudaStreamSynchronize(cs) != cudaSuccess))
         rc = PF_ERR_CUDA;
     cudaStreamDestroy(cs);
     if (rc != PF_OK) {
-        if (plan->exec) cudaGraphExecDestroy(plan->exec);
-        if (plan->graph) cudaGraphDestroy(plan->graph);
-        delete plan;
+        plan_free(plan);
+        cudaGetLastError();
+        return rc;
+    }
+    *out = plan;
+    return PF_OK;
+}
+
+size_t batch_table_bytes(int count) { return grouped_predictor_table_bytes(count); }
+
+int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
+                      size_t table_bytes, void** out) {
+    if (count < 1 || count > kMaxBatch || table_bytes < batch_table_bytes(count))
+        return PF_ERR_BAD_ARG;
+    PlanLayout* P = new PlanLayout[count];
+    int rc = PF_OK;
+    for (int r = 0; r < count && rc == PF_OK; ++r) rc = plan_layout(&m[r].grid, prec, m[r].ws, &P[r]);
+    if (rc != PF_OK) { delete[] P; return rc; }
+    if (predictor_prepare(prec) != cudaSuccess) { delete[] P; return PF_ERR_CUDA; }
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+        delete[] P;
+        return PF_ERR_CUDA;
+    }
+    // job tables of the grouped predictor, and each request's one-time set-up
+    GroupMember gm[kMaxBatch];
+    for (int r = 0; r < count; ++r)
+        gm[r] = GroupMember{m[r].grid, m[r].u, m[r].v, m[r].w, m[r].mu, m[r].rho, m[r].dt,
+                            P[r].R};
+    rc = grouped_predictor_tables(prec, rk4, gm, count, table, cs);
+    // one-time set-up of members that join a plan for the first time; a
+    // member carried over from an earlier plan may still be computing there
+    // and is not touched
+    for (int r = 0; r < count && rc == PF_OK; ++r)
+        if (m[r].fresh && P[r].mg.L && mg_enqueue_setup(P[r].mg, cs) != PF_OK) rc = PF_ERR_CUDA;
+    if (rc == PF_OK && cudaStreamSynchronize(cs) != cudaSuccess) rc = PF_ERR_CUDA;
+    StepPlan* plan = new StepPlan();
+    prof_suspend(true);
+    do {
+        if (rc != PF_OK) break;
+        if (cudaGraphCreate(&plan->graph, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
+        cudaGraph_t G = plan->graph;
+        cudaGraphNode_t n0;
+        if ((rc = add_captured(G, cs, [&](cudaStream_t st) {
+                 return launch_grouped_predictor(prec, rk4, gm, count, table, st);
+             }, &n0)))
+            break;
+        // the requests' solves run as independent branches of the graph
+        for (int r = 0; r < count && rc == PF_OK; ++r) {
+            cudaGraphNode_t nend;
+            rc = add_solve_chain(G, n0, &m[r].grid, prec, P[r], m[r].u, m[r].v, m[r].w, m[r].p,
+                                 m[r].DP, m[r].rho, m[r].dt, m[r].min_res, m[r].max_it,
+                                 m[r].stats, cs, &nend);
+        }
+        if (rc != PF_OK) break;
+        if (cudaGraphInstantiate(&plan->exec, G, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
+    } while (0);
+    prof_suspend(false);
+    for (int r = 0; r < count && rc == PF_OK; ++r)
+        if (m[r].fresh && cudaMemsetAsync(P[r].sc, 0, sizeof(BicgScalars), cs) != cudaSuccess)
+            rc = PF_ERR_CUDA;
+    if (rc == PF_OK && cudaStreamSynchronize(cs) != cudaSuccess) rc = PF_ERR_CUDA;
+    cudaStreamDestroy(cs);
+    delete[] P;
+    if (rc != PF_OK) {
+        plan_free(plan);
         cudaGetLastError();
         return rc;
     }
@@ -1118,11 +1247,7 @@ int step_plan_launch(void* plan, int nsteps, cudaStream_t s) {
 }
 
 int step_plan_destroy(void* plan) {
-    StepPlan* pl = (StepPlan*)plan;
-    if (!pl) return PF_OK;
-    if (pl->exec) cudaGraphExecDestroy(pl->exec);
-    if (pl->graph) cudaGraphDestroy(pl->graph);
-    delete pl;
+    if (plan) plan_free((StepPlan*)plan);
     return PF_OK;
 }
 

@@ -13,6 +13,8 @@
 // pf_common.cuh), including the edge-averaged viscosity one cell below the
 // off-diagonal flux (metric_staggered.py:127-144 vs :378-384).
 #include <algorithm>
+#include <cstring>
+#include <vector>
 
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
@@ -343,11 +345,11 @@ struct SmemSrc {
 // stage's FP64 u of the owned cells comes from plane i's stg slot.
 template <typename T, typename TI, typename TS, typename TA, int MODE>
 __device__ __forceinline__ void
-rhs_stage_tiled_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
-                     double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
-                     TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
-                     TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
-                     double hdt) {
+rhs_tile_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
+              double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+              TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
+              TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
+              double hdt, long long t) {
     static_assert(MODE == kModeFirst || MODE == kModeK, "FP64 input planes: first stage or k");
     using SM = RhsSmem<T, TI, TA, MODE>;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -358,7 +360,7 @@ rhs_stage_tiled_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
     const TI* fld[3] = {a.u, a.v, a.w};
     TA* A[3] = {au, av, aw};
     TS* S[3] = {su, sv, sw};
-    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+    {
         const int tz = (int)(t % tl.ntz);
         const long long rr = t / tl.ntz;
         const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
@@ -450,17 +452,13 @@ rhs_stage_tiled_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
 }
 
 template <typename T, typename TI, typename TS, typename TA, int MODE>
-__global__ void __launch_bounds__(256, 2)
-rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
-                double* __restrict__ v, double* __restrict__ w,
-                TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
-                TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
-                double hdt, double c6) {
+__device__ __forceinline__ void
+rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __restrict__ u,
+         double* __restrict__ v, double* __restrict__ w,
+         TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
+         TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
+         double hdt, double c6, long long t) {
     using SM = RhsSmem<T, TI, TA, MODE>;
-    if constexpr (SM::kConv) {
-        rhs_stage_tiled_conv<T, TI, TS, TA, MODE>(d, tl, a, u, v, w, su, sv, sw, au, av, aw, hdt);
-        return;
-    }
     extern __shared__ __align__(16) unsigned char smraw[];
     double* eu = reinterpret_cast<double*>(smraw);
     TI* ring = reinterpret_cast<TI*>(smraw + SM::kEu);
@@ -471,7 +469,7 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
     double* U[3] = {u, v, w};
     TA* A[3] = {au, av, aw};
     TS* S[3] = {su, sv, sw};
-    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x) {
+    {
         const int tz = (int)(t % tl.ntz);
         const long long rr = t / tl.ntz;
         const int tyy = (int)(rr % tl.nty), txx = (int)(rr / tl.nty);
@@ -567,6 +565,67 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
             cp_async_wait_all();
             __syncthreads();
         }
+    }
+}
+
+// One tile of a stage: the FP64-input form for an FP32 stage reading the
+// FP64 state, the direct form otherwise.
+template <typename T, typename TI, typename TS, typename TA, int MODE>
+__device__ __forceinline__ void
+stage_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* u, double* v,
+           double* w, TS* su, TS* sv, TS* sw, TA* au, TA* av, TA* aw, double hdt, double c6,
+           long long t) {
+    if constexpr (RhsSmem<T, TI, TA, MODE>::kConv)
+        rhs_tile_conv<T, TI, TS, TA, MODE>(d, tl, a, u, v, w, su, sv, sw, au, av, aw, hdt, t);
+    else
+        rhs_tile<T, TI, TS, TA, MODE>(d, tl, a, u, v, w, su, sv, sw, au, av, aw, hdt, c6, t);
+}
+
+template <typename T, typename TI, typename TS, typename TA, int MODE>
+__global__ void __launch_bounds__(256, 2)
+rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
+                double* __restrict__ v, double* __restrict__ w,
+                TS* __restrict__ su, TS* __restrict__ sv, TS* __restrict__ sw,
+                TA* __restrict__ au, TA* __restrict__ av, TA* __restrict__ aw,
+                double hdt, double c6) {
+    for (long long t = blockIdx.x; t < tl.ntiles; t += gridDim.x)
+        stage_tile<T, TI, TS, TA, MODE>(d, tl, a, u, v, w, su, sv, sw, au, av, aw, hdt, c6, t);
+}
+
+// Grouped stage: one launch advances the same RK4 stage of several
+// independent solves (a batch of requests, any grid sizes).  jobs[r] holds
+// request r's grid, tiling, stage arguments and the index of its first tile
+// in the batch's tile space; a block walks the batch's tiles (persistent
+// loop) and runs each with its request's arguments, so every tile computes
+// exactly what the single-request launch computes.
+template <typename T, typename TI>
+struct StageJob {
+    Dims d;
+    Tiling tl;
+    RhsArgs<T, TI> a;
+    double *u, *v, *w;
+    T *su, *sv, *sw, *au, *av, *aw;
+    double hdt, c6;
+    long long tile0;
+};
+
+constexpr int kMaxGroupJobs = kMaxBatch;
+
+template <typename T, typename TI, int MODE>
+__global__ void __launch_bounds__(256, 2)
+rhs_stage_grouped(const StageJob<T, TI>* __restrict__ jobs, int njobs, long long ntiles) {
+    __shared__ long long first[kMaxGroupJobs];
+    for (int r = threadIdx.y * 32 + threadIdx.x; r < njobs; r += 256) first[r] = jobs[r].tile0;
+    __syncthreads();
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int lo = 0, hi = njobs - 1;  // last job whose first tile is <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (first[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        const StageJob<T, TI>& J = jobs[lo];
+        stage_tile<T, TI, T, T, MODE>(J.d, J.tl, J.a, J.u, J.v, J.w, J.su, J.sv, J.sw, J.au,
+                                      J.av, J.aw, J.hdt, J.c6, t - J.tile0);
     }
 }
 
@@ -709,6 +768,168 @@ static cudaError_t predictor_impl(const pf_grid* g, int rk4, double* u,
                                acc, hdt, c6, s);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Grouped predictor: the RK4 stages of a batch of requests, one launch per
+// stage (rhs_stage_grouped over per-stage job tables in device memory).
+// ---------------------------------------------------------------------------
+template <typename T, typename TI, int MODE>
+static cudaError_t grouped_prepare() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+    const size_t sm = RhsSmem<T, TI, T, MODE>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(rhs_stage_grouped<T, TI, MODE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e == cudaSuccess) {
+        const size_t two = 2 * (sm + 1024 + kMaxGroupJobs * 8);
+        const int pct = (int)std::min<size_t>(100, (two * 100 + 228 * 1024 - 1) / (228 * 1024));
+        e = cudaFuncSetAttribute(rhs_stage_grouped<T, TI, MODE>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+    return e;
+}
+
+static size_t job_bytes() {
+    return std::max(std::max(sizeof(StageJob<double, double>), sizeof(StageJob<float, double>)),
+                    sizeof(StageJob<float, float>));
+}
+
+static size_t align256r(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t grouped_predictor_table_bytes(int count) {
+    return 4 * align256r((size_t)std::max(count, 1) * job_bytes());
+}
+
+// Job of one request for one stage (the arguments the single-request
+// predictor_impl passes to that stage).
+template <typename T, typename TI>
+static StageJob<T, TI> make_job(const GroupMember& m, const TI* in, T* st, T* acc,
+                                long long tile0) {
+    StageJob<T, TI> J;
+    const pf_grid* g = &m.grid;
+    J.d = Dims{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
+    J.tl = make_tiling(J.d, kRhsTY);
+    const long long n = J.d.n;
+    J.a = make_args<T, TI>(g, in, in + n, in + 2 * n, nullptr, nullptr, m.mu, m.rho);
+    J.u = m.u; J.v = m.v; J.w = m.w;
+    J.su = st; J.sv = st ? st + n : nullptr; J.sw = st ? st + 2 * n : nullptr;
+    J.au = acc; J.av = acc + n; J.aw = acc + 2 * n;
+    J.hdt = 0.5 * m.dt;
+    J.c6 = m.dt / 6.0;
+    J.tile0 = tile0;
+    return J;
+}
+
+// The four stage tables (or Euler's one) of type T, written into `table`.
+template <typename T>
+static int tables_impl(int rk4, const GroupMember* m, int count, void* table, cudaStream_t s,
+                       long long* ntiles) {
+    const size_t slot = align256r((size_t)count * job_bytes());
+    std::vector<unsigned char> host(4 * slot, 0);
+    long long tiles = 0;
+    for (int r = 0; r < count; ++r) {
+        const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
+        T* ws = (T*)m[r].R;
+        T *sa = ws, *sb = ws + 3 * n, *acc = ws + 6 * n;
+        const double* u = m[r].u;
+        if (!rk4) {
+            auto J = make_job<T, double>(m[r], u, nullptr, acc, tiles);
+            std::memcpy(host.data() + r * sizeof(J), &J, sizeof(J));
+        } else {
+            auto J0 = make_job<T, double>(m[r], u, sa, acc, tiles);
+            auto J1 = make_job<T, T>(m[r], sa, sb, acc, tiles);
+            auto J2 = make_job<T, T>(m[r], sb, sa, acc, tiles);
+            auto J3 = make_job<T, T>(m[r], sa, nullptr, acc, tiles);
+            std::memcpy(host.data() + 0 * slot + r * sizeof(J0), &J0, sizeof(J0));
+            std::memcpy(host.data() + 1 * slot + r * sizeof(J1), &J1, sizeof(J1));
+            std::memcpy(host.data() + 2 * slot + r * sizeof(J2), &J2, sizeof(J2));
+            std::memcpy(host.data() + 3 * slot + r * sizeof(J3), &J3, sizeof(J3));
+        }
+        Dims d{m[r].grid.nx, m[r].grid.ny, m[r].grid.nz, n};
+        tiles += make_tiling(d, kRhsTY).ntiles;
+    }
+    *ntiles = tiles;
+    if (cudaMemcpyAsync(table, host.data(), host.size(), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return PF_ERR_CUDA;
+    return PF_OK;
+}
+
+int grouped_predictor_tables(int prec, int rk4, const GroupMember* m, int count, void* table,
+                             cudaStream_t s) {
+    if (count < 1 || count > kMaxGroupJobs) return PF_ERR_BAD_ARG;
+    long long tiles = 0;
+    cudaError_t e = cudaSuccess;
+    if (prec == PF_FP64) {
+        if ((e = grouped_prepare<double, double, kModeK>()) ||
+            (e = grouped_prepare<double, double, kModeFirst>()) ||
+            (e = grouped_prepare<double, double, kModeMid>()) ||
+            (e = grouped_prepare<double, double, kModeLast>()))
+            return PF_ERR_CUDA;
+        return tables_impl<double>(rk4, m, count, table, s, &tiles);
+    }
+    if ((e = grouped_prepare<float, double, kModeK>()) ||
+        (e = grouped_prepare<float, double, kModeFirst>()) ||
+        (e = grouped_prepare<float, float, kModeMid>()) ||
+        (e = grouped_prepare<float, float, kModeLast>()))
+        return PF_ERR_CUDA;
+    return tables_impl<float>(rk4, m, count, table, s, &tiles);
+}
+
+template <typename T>
+static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, void* table,
+                                cudaStream_t s) {
+    const size_t slot = align256r((size_t)count * job_bytes());
+    long long tiles = 0;
+    for (int r = 0; r < count; ++r) {
+        Dims d{m[r].grid.nx, m[r].grid.ny, m[r].grid.nz,
+               (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz};
+        tiles += make_tiling(d, kRhsTY).ntiles;
+    }
+    const int grid = (int)std::min<long long>(tiles, num_sms() * 2);
+    const dim3 blk(32, 8);
+    const bool f64 = sizeof(T) == 8;
+    char* tb = (char*)table;
+    if (!rk4) {
+        PF_LAUNCH(f64 ? "grouped_euler_f64" : "grouped_euler_f32", s,
+                  (rhs_stage_grouped<T, double, kModeK><<<grid, blk,
+                      RhsSmem<T, double, T, kModeK>::bytes, s>>>(
+                      (const StageJob<T, double>*)tb, count, tiles)));
+        for (int r = 0; r < count; ++r) {
+            const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
+            const T* acc = (const T*)m[r].R + 6 * n;
+            const int gp = (int)std::min<long long>((n + 1023) / 1024, 4096);
+            PF_LAUNCH("euler_apply", s, euler_apply<T><<<gp, 256, 0, s>>>(
+                n, acc, acc + n, acc + 2 * n, m[r].dt, m[r].u, m[r].v, m[r].w));
+        }
+        return cudaGetLastError();
+    }
+    PF_LAUNCH(f64 ? "grouped_first_f64" : "grouped_first_f32", s,
+              (rhs_stage_grouped<T, double, kModeFirst><<<grid, blk,
+                  RhsSmem<T, double, T, kModeFirst>::bytes, s>>>(
+                  (const StageJob<T, double>*)tb, count, tiles)));
+    PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
+              (rhs_stage_grouped<T, T, kModeMid><<<grid, blk, RhsSmem<T, T, T, kModeMid>::bytes,
+                  s>>>((const StageJob<T, T>*)(tb + slot), count, tiles)));
+    PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
+              (rhs_stage_grouped<T, T, kModeMid><<<grid, blk, RhsSmem<T, T, T, kModeMid>::bytes,
+                  s>>>((const StageJob<T, T>*)(tb + 2 * slot), count, tiles)));
+    PF_LAUNCH(f64 ? "grouped_last_f64" : "grouped_last_f32", s,
+              (rhs_stage_grouped<T, T, kModeLast><<<grid, blk,
+                  RhsSmem<T, T, T, kModeLast>::bytes, s>>>(
+                  (const StageJob<T, T>*)(tb + 3 * slot), count, tiles)));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grouped_predictor(int prec, int rk4, const GroupMember* m, int count,
+                                     void* table, cudaStream_t s) {
+    return prec == PF_FP64 ? grouped_impl<double>(rk4, m, count, table, s)
+                           : grouped_impl<float>(rk4, m, count, table, s);
 }
 
 cudaError_t predictor_prepare(int prec) {

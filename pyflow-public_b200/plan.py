@@ -27,6 +27,22 @@ _lib.pf_step_plan_launch.restype = ctypes.c_int
 _lib.pf_step_plan_destroy.argtypes = [ctypes.c_void_p]
 _lib.pf_step_plan_destroy.restype = ctypes.c_int
 
+class BatchMember(ctypes.Structure):
+    _fields_ = [("grid", L.Grid)] + [(n, ctypes.c_void_p) for n in ("u", "v", "w", "p", "DP")] + [
+        ("mu", ctypes.c_double), ("rho", ctypes.c_double), ("dt", ctypes.c_double),
+        ("min_res", ctypes.c_double), ("max_it", ctypes.c_int), ("fresh", ctypes.c_int),
+        ("ws", ctypes.c_void_p),
+        ("ws_bytes", ctypes.c_size_t), ("stats", ctypes.c_void_p)]
+
+
+_lib.pf_batch_table_bytes.argtypes = [ctypes.c_int]
+_lib.pf_batch_table_bytes.restype = ctypes.c_size_t
+_lib.pf_batch_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BatchMember),
+                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.POINTER(ctypes.c_void_p)]
+_lib.pf_batch_plan_create.restype = ctypes.c_int
+MAX_BATCH = 64
+
 STAT_NAMES = ("max_u", "max_v", "max_w", "tke", "max_div", "max_res",
               "iterations", "status", "total_iterations", "steps")
 
@@ -62,6 +78,80 @@ class StepPlan:
 
     def stats(self):
         return dict(zip(STAT_NAMES, self.stats_dev.cpu().tolist()))
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.pf_step_plan_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Member:
+    """One request of a BatchPlan: its device fields u, v, w, p, DP (FP64,
+    one grid), constants, plan workspace and statistics buffer (the layout of
+    StepPlan.stats_dev).  The buffers stay owned by the member, so a member
+    can move from one batch to the next with its state and running totals."""
+
+    def __init__(self, u, v, w, p, DP, spacing, mu, rho, dt, min_res=1e-10, max_it=20000,
+                 prec="mixed_mg"):
+        for t, nm in ((u, "u"), (v, "v"), (w, "w"), (p, "p"), (DP, "DP")):
+            ops._check(t, u.shape, torch.float64, nm)
+        self.fields = (u, v, w, p, DP)
+        self.grid = ops.grid(u.shape, spacing)
+        self.prec = prec
+        need = _lib.pf_step_plan_workspace_bytes(ctypes.byref(self.grid), ops.PREC[prec])
+        self.ws = torch.empty(need, dtype=torch.uint8, device=u.device)
+        self.stats_dev = torch.zeros(10, dtype=torch.float64, device=u.device)
+        self.consts = (float(mu), float(rho), float(dt), float(min_res), int(max_it))
+        self.cells = u.numel()
+        self.fresh = True
+        # the fields must be ready before a plan first uses them
+        torch.cuda.current_stream(u.device).synchronize()
+
+    def stats(self):
+        return dict(zip(STAT_NAMES, self.stats_dev.cpu().tolist()))
+
+    def c_struct(self):
+        mu, rho, dt, min_res, max_it = self.consts
+        return BatchMember(self.grid, *(ops._p(t) for t in self.fields), mu, rho, dt, min_res,
+                           max_it, 1 if self.fresh else 0, ops._p(self.ws), self.ws.numel(),
+                           ops._p(self.stats_dev))
+
+
+class BatchPlan:
+    """One CUDA graph that advances every member by one time step per
+    replay (pf_batch_plan_create): the RK4 stages of all members as one
+    grouped launch per stage, then each member's divergence, pressure solve,
+    projection and statistics as independent graph branches.  Members keep
+    their results exactly as with their own StepPlan."""
+
+    def __init__(self, members, rk4=True):
+        if not members or len(members) > MAX_BATCH:
+            raise ValueError("a batch holds 1..%d members" % MAX_BATCH)
+        prec = members[0].prec
+        if any(m.prec != prec for m in members):
+            raise ValueError("all members of a batch use one precision form")
+        dev = members[0].ws.device
+        self.members = list(members)
+        need = _lib.pf_batch_table_bytes(len(members))
+        self.table = torch.empty(need, dtype=torch.uint8, device=dev)
+        arr = (BatchMember * len(members))(*(m.c_struct() for m in members))
+        self._h = ctypes.c_void_p(0)
+        L.check("pf_batch_plan_create", _lib.pf_batch_plan_create(
+            ops.PREC[prec], 1 if rk4 else 0, arr, len(members), ops._p(self.table),
+            self.table.numel(), ctypes.byref(self._h)))
+        for m in members:
+            m.fresh = False
+
+    def launch(self, nsteps=1, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream(self.table.device)
+        L.check("pf_step_plan_launch", _lib.pf_step_plan_launch(
+            self._h, int(nsteps), ctypes.c_void_p(s.cuda_stream)))
 
     def close(self):
         if self._h and self._h.value:

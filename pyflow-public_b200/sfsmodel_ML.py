@@ -150,9 +150,10 @@ class residual_stress:
             self.outParamsList = list(ck.get("outParamsList", []))
             self.sumParamsList = list(ck.get("sumParamsList", []))
         if hasattr(inputConfig, "LR"):
+            # the reference records the override but leaves the optimizer's
+            # learning rate as created (src/sfsmodel/sfsmodel_ML.py:214-216);
+            # the halving schedule then acts on both values separately
             self.LR = inputConfig.LR
-            for g in self.optimizer.param_groups:
-                g["lr"] = self.LR
         # training settings (src/sfsmodel/sfsmodel_ML.py:219-243)
         self.saveModel = hasattr(inputConfig, "modelDictSave")
         self.modelDictSave = getattr(inputConfig, "modelDictSave", None)

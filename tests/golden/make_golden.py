@@ -35,6 +35,11 @@ run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
 ml_16.npz          rhs_NavierStokes.evaluate with the reference's 'source' ML
                    closure (sfsmodel_ML, a seeded random network whose
                    weights are stored in the fixture) on a 16^3 box.
+finalize_8.npz     sfsmodel_ML.residual_stress.finalize over seven training
+                   windows with seeded gradients (gradient averaging over
+                   numSumDistr windows, RMSprop, learning-rate schedule).
+target_12x16x20.npz  Domain.TargetDataVelCorr: projection of a random target
+                   field (and the DP it adds to the simulation pressure).
 run_64.npz         PyFlow.run of the 64^3 plain-DNS workload (seed 0, k0 = 4,
                    nu = 0.01, dt = 0.005, 20 RK4 steps): final u, v, w, p on
                    every 4th cell of each axis, their sum / sum of squares /
@@ -315,6 +320,89 @@ def ml_case(out):
     print("ml: rhs max", np.abs(res["rhs_ml"]).max())
 
 
+def finalize_case(out):
+    """The reference's training update (residual_stress.finalize,
+    src/sfsmodel/sfsmodel_ML.py:284-349) over seven windows with seeded
+    gradients: numSumDistr = 2, LR_decay = 5 (halving once epoch >= 4 and
+    epoch % 5 == 0), an LR override in the configuration (which the reference
+    stores but does not pass to its optimizer)."""
+    import torch
+    n = 8
+    S = H.make_setup(n, n, n, 2 * np.pi, 2 * np.pi, 2 * np.pi)
+    ns, d = S.ns, S.decomp
+
+    class IC:
+        simDt = 0.004
+        modelDictSave = os.path.join(ns.tmp, "finalize_model.dict")
+        LR_decay = 5
+        numSumDistr = 2
+        LR = 0.003
+
+    class Comms:
+        size = 1
+
+        @staticmethod
+        def parallel_sum(a):
+            return a
+
+    # every operation of the update is elementwise: the fixture keeps the
+    # first K elements of every parameter (weights before and after each
+    # window, the window's gradient)
+    K = 96
+    torch.manual_seed(11)
+    ml = ns.sfsmodel_ML.residual_stress(IC(), d, S.geo)
+    names = [k for k, _ in ml.model.named_parameters()]
+    res = {"simDt": IC.simDt, "LR_decay": IC.LR_decay, "numSumDistr": IC.numSumDistr,
+           "LR_config": IC.LR, "names": np.array(names), "K": K}
+    for k, t in ml.model.named_parameters():
+        res["w0_" + k] = t.detach().numpy().ravel()[:K].copy()
+    rng = np.random.default_rng(77)
+    epochs = 7
+    for e in range(epochs):
+        for k, prm in ml.model.named_parameters():
+            g = (rng.standard_normal(tuple(prm.shape)) * 0.1).astype(np.float32)
+            res["g%d_%s" % (e, k)] = g.ravel()[:K].copy()
+            prm.grad = torch.tensor(g)
+        ml.finalize(Comms())
+        for k, prm in ml.model.named_parameters():
+            res["w%d_%s" % (e + 1, k)] = prm.detach().numpy().ravel()[:K].copy()
+        res["lr%d" % (e + 1)] = np.array([ml.LR, ml.optimizer.param_groups[0]["lr"]])
+    res["epochs"] = epochs
+    np.savez_compressed(os.path.join(out, "finalize_8.npz"), **res)
+    print("finalize: lr", [float(res["lr%d" % (e + 1)][1]) for e in range(epochs)])
+
+
+def target_case(out):
+    """Domain.TargetDataVelCorr (src/data/domain.py:445-468) on a random,
+    not divergence-free target field: divergence, BiCGStab solve (which also
+    adds DP to the simulation pressure p), target corrected by +dt/rho grad DP."""
+    import torch
+    nx, ny, nz = 12, 16, 20
+    lengths = (2 * np.pi, 2.1, 3.3)
+    S = H.make_setup(nx, ny, nz, *lengths)
+    ns, d = S.ns, S.decomp
+    rng = np.random.default_rng(4321)
+    uT, vT, wT = (rng.standard_normal((nx, ny, nz)) for _ in range(3))
+    p0 = 0.1 * rng.standard_normal((nx, ny, nz))
+    rho, dt = 1.3, 2.0e-3
+    D = types.SimpleNamespace(
+        targetDataVelCorr=True, metric=S.metric, rho=rho,
+        state_u_T=_state(ns, d, uT), state_v_T=_state(ns, d, vT), state_w_T=_state(ns, d, wT),
+        source_P=torch.zeros(nx, ny, nz, dtype=torch.float64),
+        state_DP_P=_state(ns, d, np.zeros((nx, ny, nz))), state_p_P=_state(ns, d, p0),
+        poisson=ns.pressure.solver_bicgstab(S.comms, d, S.metric, S.geo, rho, dt, 1e-10, 500))
+    ns.domain.Domain.TargetDataVelCorr(D, dt)
+    res = dict(shape=np.array([nx, ny, nz]), spacing=np.array([S.geo.dx, S.geo.dy, S.geo.dz]),
+               rho=rho, dt=dt, uT=uT, vT=vT, wT=wT, p0=p0,
+               u_out=D.state_u_T.interior().numpy().copy(),
+               v_out=D.state_v_T.interior().numpy().copy(),
+               w_out=D.state_w_T.interior().numpy().copy(),
+               DP=D.state_DP_P.interior().numpy().copy(),
+               p_out=D.state_p_P.interior().numpy().copy(), max_res=float(D.max_resP))
+    np.savez_compressed(os.path.join(out, "target_12x16x20.npz"), **res)
+    print("target: max_res", res["max_res"])
+
+
 def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005, stride=1):
     import torch
     ns = H.load_reference()
@@ -413,7 +501,8 @@ def run_case(out, n=32, steps=5, seed=0, nu=0.01, dt=0.005, stride=1):
 
 if __name__ == "__main__":
     out = HERE
-    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run", "run64", "ml"]
+    which = sys.argv[1:] or ["ops", "jacobi", "sgs", "adjoint", "run", "run64", "ml",
+                             "finalize", "target"]
     if "ops" in which:
         ops_case(out)
     if "jacobi" in which:
@@ -426,6 +515,10 @@ if __name__ == "__main__":
         run_case(out)
     if "ml" in which:
         ml_case(out)
+    if "finalize" in which:
+        finalize_case(out)
+    if "target" in which:
+        target_case(out)
     if "run64" in which:
         # the 64^3 plain-DNS workload: seed 0, k0 = 4, nu = 0.01, dt = 0.005,
         # 20 RK4 steps, BiCGStab to 1e-10

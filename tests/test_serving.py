@@ -23,26 +23,69 @@ def test_footprint_grows_with_grid():
 
 
 @pytest.mark.gpu
-def test_results_same_alone_and_in_mix():
+@pytest.mark.parametrize("prec", ["mixed_mg", "fp64"])
+def test_results_same_alone_and_in_mix(prec):
+    """Batched serving: each request's fields after its steps are bitwise the
+    same served alone, in a mix of sizes arriving over time (batch graphs
+    rebuilt as requests join and leave), and with one graph per request."""
     import pyflow_b200.serving as S
-    reqs = [S.Request(id=i, n=n, seed=1000 + i, nu=0.02 * 32 / n, dt=0.01, steps=5,
-                      arrival=0.002 * i) for i, n in enumerate([16, 24, 32, 16, 24, 20])]
+    sizes = [16, 24, 32, 16, 64, 20, 48]
+    reqs = [S.Request(id=i, n=n, seed=1000 + i, nu=0.02 * 32 / n, dt=0.01, steps=4 + i % 3,
+                      arrival=0.002 * i) for i, n in enumerate(sizes)]
     alone = {}
     for r in reqs:
-        srv = S.Server(max_slots=1, prec="mixed", keep_fields=True)
+        srv = S.Server(max_slots=1, prec=prec, keep_fields=True)
         res = srv.run([S.Request(**{**r.__dict__, "arrival": 0.0})])
         assert res[0].status == "ok", res[0]
         alone[r.id] = res[0]
-    srv = S.Server(max_slots=4, prec="mixed", keep_fields=True)
+    srv = S.Server(max_slots=4, prec=prec, keep_fields=True)
     mixed = srv.run(reqs)
-    assert srv.max_active > 1
-    assert len(mixed) == len(reqs)
+    assert srv.max_active > 1 and srv.rebuilds > 2
+    streams = S.Server(max_slots=4, prec=prec, keep_fields=True, batched=False).run(reqs)
+    assert len(mixed) == len(reqs) == len(streams)
+    by_stream = {r.id: r for r in streams}
     for m in mixed:
         a = alone[m.id]
         assert m.status == "ok"
-        for x, y in zip(m.fields, a.fields):
-            assert torch.equal(x, y)
+        for x, y, z in zip(m.fields, a.fields, by_stream[m.id].fields):
+            assert torch.equal(x, y) and torch.equal(x, z)
         assert m.stats["max_res"] <= 1e-10
+        assert m.stats["steps"] == m.steps
+
+
+@pytest.mark.gpu
+def test_batch_plan_matches_step_plans():
+    """One BatchPlan over requests of different sizes advances each exactly
+    like its own StepPlan (grouped RK4 stages, branch-parallel solves)."""
+    import pyflow_b200.initial as ic
+    from pyflow_b200.plan import BatchPlan, Member, StepPlan
+    shapes = [(32, 32, 32), (24, 20, 28), (64, 64, 64), (16, 48, 32)]
+    ref, members = [], []
+    for i, sh in enumerate(shapes):
+        sp = tuple(2 * np.pi / n for n in sh)
+        f0 = [torch.tensor(a, device="cuda") for a in ic.spectral_velocity(sh, seed=i)]
+        fa = [t.clone() for t in f0] + [torch.zeros_like(f0[0]) for _ in range(2)]
+        fb = [t.clone() for t in f0] + [torch.zeros_like(f0[0]) for _ in range(2)]
+        pl = StepPlan(*fa, sp, 0.01, 1.0, 0.004, prec="mixed_mg")
+        pl.launch(3)
+        torch.cuda.synchronize()
+        ref.append((fa, pl.stats()))
+        pl.close()
+        members.append(Member(*fb, sp, 0.01, 1.0, 0.004, prec="mixed_mg"))
+    bp = BatchPlan(members)
+    bp.launch(2)
+    bp2 = BatchPlan(members[::-1])      # a rebuilt batch carries the state over
+    bp2.launch(1)
+    torch.cuda.synchronize()
+    for (fa, st), m in zip(ref, members):
+        for x, y in zip(fa[:4], m.fields[:4]):
+            assert torch.equal(x, y)
+        got = m.stats()
+        for k in ("max_u", "tke", "max_div", "max_res", "iterations", "total_iterations",
+                  "steps"):
+            assert got[k] == st[k], k
+    bp.close()
+    bp2.close()
 
 
 @pytest.mark.gpu
