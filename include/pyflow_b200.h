@@ -229,6 +229,18 @@ int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u,
 int pf_step_plan_launch(pf_step_plan* plan, int nsteps, void* stream);
 int pf_step_plan_destroy(pf_step_plan* plan);
 
+/* NGA restart I/O from device memory (readNGArestart / writeNGArestart,
+ * src/data/dataReader.py:119-208, whose MPI-IO path is :215-390): a restart
+ * file stores each variable as an FP64 array in Fortran order (x fastest).
+ * pf_restart_pack writes a device field ([nx][ny][nz], z fastest) in the
+ * file's order into the device buffer file_order (nx*ny*nz doubles), ready
+ * for one contiguous copy to the file; pf_restart_unpack is the inverse.
+ * Asynchronous; the two buffers must not overlap; ny <= 65535. */
+int pf_restart_pack(const pf_grid* g, const double* field, double* file_order,
+                    void* stream);
+int pf_restart_unpack(const pf_grid* g, const double* file_order, double* field,
+                      void* stream);
+
 /* A batch of independent time steps (the serving loop's active requests,
  * any grid sizes, one precision form) captured as ONE CUDA graph: each
  * replay advances every member by one Domain.forwardStep

@@ -26,16 +26,34 @@ from . import ops
 from . import parallel
 
 
+class DeviceIC:
+    """The initial state as device fields, indexed like the reference's
+    data_IC[..., v]."""
+
+    def __init__(self, fields):
+        self.fields = fields
+        self.shape = tuple(fields[0].shape) + (len(fields),)
+
+    def __getitem__(self, key):
+        if isinstance(key, tuple) and len(key) == 2 and key[0] is Ellipsis:
+            return self.fields[key[1]]
+        raise IndexError("DeviceIC supports data_IC[..., v] only")
+
+
 def _initial_data(inputConfig, config, decomp):
     """names, startTime, data_IC[nx,ny,nz,4] (src/data/initial_conditions.py:39-77)."""
     name = getattr(inputConfig, "configName", "restart")
     if name == "restart":
-        names, t0, data = dr.readNGArestart(inputConfig.dataFileStr, headerOnly=False)
-        if data.shape[:3] != (config.Nx, config.Ny, config.Nz):
+        # straight into device memory (src/data/initial_conditions.py:57-77
+        # reads the restart into host arrays first)
+        (nx, ny, nz, nv), _, _ = dr.readNGArestart_dims(inputConfig.dataFileStr)
+        if (nx, ny, nz) != (config.Nx, config.Ny, config.Nz):
             raise ValueError("restart file and config grid sizes differ")
-        out = np.zeros(data.shape[:3] + (4,))
-        out[..., :min(4, data.shape[3])] = data[..., :4]
-        return ["U", "V", "W", "P"], t0, out
+        names, t0, fields = dr.readNGArestart_device(inputConfig.dataFileStr, decomp.device,
+                                                     nvar=4)
+        while len(fields) < 4:
+            fields.append(torch.zeros_like(fields[0]))
+        return ["U", "V", "W", "P"], t0, DeviceIC(fields)
     if name == "spectral":
         from . import initial
         L = (config.xGrid[-1] - config.xGrid[0], config.yGrid[-1] - config.yGrid[0],
@@ -84,9 +102,9 @@ def run(inputConfig):
     def write_restart(t):
         if fNameOut and rank0:
             D.data_all_CPU.time, D.data_all_CPU.dt = t, simDt
-            fields = [s.interior().cpu().numpy() for s in D.state_data_all]
-            dr.writeNGArestart(fNameOut + "_" + "{:12.7E}".format(t), fields,
-                               D.data_all_CPU.names, simDt, t)
+            dr.writeNGArestart_device(fNameOut + "_" + "{:12.7E}".format(t),
+                                      [s.interior() for s in D.state_data_all],
+                                      D.data_all_CPU.names, simDt, t)
 
     write_restart(simTime)
     if rank0:

@@ -62,6 +62,8 @@ def _load():
         "pf_flow_stats": ([G, P, P, P, D, P, P, S, P], I),
         "pf_sgs_closure": ([G, I, P, P, P, D, P, P], I),
         "pf_mlp_pack_bytes": ([], S),
+        "pf_restart_pack": ([G, P, P, P], I),
+        "pf_restart_unpack": ([G, P, P, P], I),
         "pf_mlp_closure": ([G, P, P, P, P, P, P, P, P], I),
     }
     for name, (args, res) in sigs.items():

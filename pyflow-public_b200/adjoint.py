@@ -296,9 +296,7 @@ def run_training(inputConfig, comms, decomp, geometry, metric, D, startTime):
             result = (float(L.detach()), float(u0[0].grad[nn, nn, nn]))
         else:
             fname = inputConfig.getTargetFileName(inputConfig.startFileIt + it)
-            _, _, data = dr.readNGArestart(fname, headerOnly=False)
-            tgt = [torch.tensor(data[..., c], dtype=torch.float64, device=state[0].device)
-                   for c in range(3)]
+            _, _, tgt = dr.readNGArestart_device(fname, state[0].device, nvar=3)
             if getattr(inputConfig, "targetDataVelCorr", False):
                 project(tgt, sp, rho, simDt, tol, max_it, p=D.state_p_P.interior())
             L = sum(torch.sum(torch.abs(c - g)) for c, g in zip(cur, tgt)) / n

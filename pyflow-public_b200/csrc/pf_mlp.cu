@@ -12,9 +12,9 @@
 //   1. each thread computes its cell's gradients and writes 16 BF16 features
 //      (9 + 7 zero pads) into the X tile in shared memory;
 //   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
-//   3. each thread reads its D1 row from TMEM (tcgen05.ld, 32 columns per
-//      wait), adds b1, applies tanh, and writes the BF16 row (pairs packed
-//      by one conversion) into the H tile;
+//   3. each thread reads its D1 row from TMEM (tcgen05.ld, 64 columns per
+//      wait), adds b1, rounds pairs of pre-activations to BF16, applies the
+//      packed BF16 tanh and writes the BF16 row into the H tile;
 //   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
 //   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
 //      its six stresses (FP64) to global memory.
@@ -151,15 +151,17 @@ __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// tanh of two FP32 values (hardware approximation), rounded to BF16 and
-// packed (a in the low half) by one conversion
+// tanh of two FP32 pre-activations as one packed BF16 pair (a in the low
+// half): both are rounded to BF16 by one conversion, then the hardware tanh
+// of the pair (tanh.approx.bf16x2) gives the two BF16 activations the next
+// layer reads.  One special-function instruction per pair: the epilogue's
+// limit is the special-function unit, so this halves it against two FP32
+// tanh and a conversion.
 __device__ __forceinline__ uint32_t tanh_pack_bf16x2(float a, float b) {
-    float ta, tb;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(ta) : "f"(a));
-    asm("tanh.approx.f32 %0, %1;" : "=f"(tb) : "f"(b));
-    uint32_t out;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(out) : "f"(tb), "f"(ta));
-    return out;
+    uint32_t x, y;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(x) : "f"(b), "f"(a));
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
+    return y;
 }
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) {

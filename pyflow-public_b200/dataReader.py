@@ -1,13 +1,25 @@
 """NGA config / restart files (format of src/data/dataReader.py:60-208).
 
-Serial numpy readers and writers: the restart format is a header
-``<4i nx,ny,nz,nvar><2d dt,time><8-char names>`` followed by each variable in
-Fortran order (float64).  Used by PyFlow.run for initial conditions and
-checkpoint/resume; device fields are copied in and out whole.
+The restart format is a header ``<4i nx,ny,nz,nvar><2d dt,time><8-char names>``
+followed by each variable in Fortran order (float64).
+
+* ``readNGArestart`` / ``writeNGArestart``: serial numpy, host arrays.
+* ``readNGArestart_device`` / ``writeNGArestart_device``: straight between
+  the file and device fields (the reference's checkpoint path is MPI-IO from
+  host copies, src/data/dataReader.py:215-390).  Each field is transposed to
+  or from the file's order on the device (pf_restart_pack / _unpack), then
+  moves in chunks through two pinned host buffers: the device-to-host copy
+  of chunk k+1 (a copy stream) overlaps the file write of chunk k (a writer
+  thread), and reading overlaps the same way.  No whole-field host copy.
+PyFlow.run reads its initial state and writes its checkpoints this way.
 """
+import ctypes
 import struct
+import threading
 
 import numpy as np
+
+CHUNK_BYTES = 1 << 26   # 64 MiB per pinned staging buffer
 
 
 def readNGAconfig(fName):
@@ -65,3 +77,102 @@ def writeNGArestart(fName, fields, names, dt, time):
             f.write(n.ljust(8)[:8].encode())
         for a in fields:
             f.write(np.asarray(a, dtype="<f8").reshape(-1, order="F").tobytes())
+
+
+def _header(nx, ny, nz, names, dt, time):
+    out = struct.pack("<4i", nx, ny, nz, len(names)) + struct.pack("<2d", dt, time)
+    for n in names:
+        out += n.ljust(8)[:8].encode()
+    return out
+
+
+def _lib():
+    from . import _lib as L
+    return L
+
+
+def writeNGArestart_device(fName, fields, names, dt, time, chunk_bytes=CHUNK_BYTES):
+    """Write device FP64 fields (each (nx, ny, nz), C order) as a restart
+    file, straight from device memory."""
+    import torch
+    from . import ops
+    L = _lib()
+    nx, ny, nz = fields[0].shape
+    dev = fields[0].device
+    g = ops.grid((nx, ny, nz), (1.0, 1.0, 1.0))
+    n = nx * ny * nz
+    scratch = torch.empty(n, dtype=torch.float64, device=dev)
+    per = max(1, min(n, chunk_bytes // 8))
+    pinned = [torch.empty(per, dtype=torch.float64).pin_memory() for _ in range(2)]
+    copy = torch.cuda.Stream(dev)
+    events = [torch.cuda.Event() for _ in range(2)]
+    main = torch.cuda.current_stream(dev)
+    with open(fName, "wb") as f:
+        f.write(_header(nx, ny, nz, names, dt, time))
+        for a in fields:
+            ops._check(a, (nx, ny, nz), torch.float64, "field")
+            L.check("pf_restart_pack", L.lib().pf_restart_pack(
+                ctypes.byref(g), ops._p(a), ops._p(scratch), ctypes.c_void_p(main.cuda_stream)))
+            copy.wait_stream(main)
+            writer, k = None, 0
+            for s0 in range(0, n, per):
+                m = min(per, n - s0)
+                buf = pinned[k & 1]
+                with torch.cuda.stream(copy):
+                    buf[:m].copy_(scratch[s0:s0 + m], non_blocking=True)
+                events[k & 1].record(copy)
+                if writer is not None:
+                    writer.join()
+                events[k & 1].synchronize()
+                view = buf[:m].numpy()
+                writer = threading.Thread(target=f.write, args=(memoryview(view).cast("B"),))
+                writer.start()
+                k += 1
+            if writer is not None:
+                writer.join()
+    # the scratch buffer is free once the copies have finished
+    copy.synchronize()
+
+
+def readNGArestart_device(fName, device, nvar=None, chunk_bytes=CHUNK_BYTES):
+    """(names, time, [fields]) of a restart file, each field a device FP64
+    tensor (nx, ny, nz) read straight into device memory."""
+    import torch
+    from . import ops
+    L = _lib()
+    (nx, ny, nz, nv), dt, time = readNGArestart_dims(fName)
+    names = readNGArestart(fName, headerOnly=True)[0]
+    nv = nv if nvar is None else min(nv, nvar)
+    dev = torch.device(device)
+    g = ops.grid((nx, ny, nz), (1.0, 1.0, 1.0))
+    n = nx * ny * nz
+    per = max(1, min(n, chunk_bytes // 8))
+    pinned = [torch.empty(per, dtype=torch.float64).pin_memory() for _ in range(2)]
+    done = [torch.cuda.Event() for _ in range(2)]
+    copy = torch.cuda.Stream(dev)
+    main = torch.cuda.current_stream(dev)
+    scratch = torch.empty(n, dtype=torch.float64, device=dev)
+    out = []
+    k = 0   # chunks so far (over all variables): buffer k & 1 was used by chunk k - 2
+    with open(fName, "rb") as f:
+        f.seek(32 + 8 * len(names))
+        for _ in range(nv):
+            copy.wait_stream(main)          # the scratch buffer is free
+            for s0 in range(0, n, per):
+                m = min(per, n - s0)
+                buf = pinned[k & 1]
+                if k >= 2:
+                    done[k & 1].synchronize()   # its previous copy has left
+                f.readinto(memoryview(buf[:m].numpy()).cast("B"))
+                with torch.cuda.stream(copy):
+                    scratch[s0:s0 + m].copy_(buf[:m], non_blocking=True)
+                done[k & 1].record(copy)
+                k += 1
+            main.wait_stream(copy)
+            field = torch.empty((nx, ny, nz), dtype=torch.float64, device=dev)
+            L.check("pf_restart_unpack", L.lib().pf_restart_unpack(
+                ctypes.byref(g), ops._p(scratch), ops._p(field),
+                ctypes.c_void_p(main.cuda_stream)))
+            out.append(field)
+    main.synchronize()
+    return names[:nv], time, out

@@ -18,7 +18,9 @@ class state_P:
             setattr(self, a, getattr(decomp, a))
         self.data = torch.zeros(decomp.nx_, decomp.ny_, decomp.nz_,
                                 dtype=torch.float64, device=decomp.device)
-        if IC is not None and np.any(IC):
+        if isinstance(IC, torch.Tensor):
+            self.data.copy_(IC)
+        elif IC is not None and np.any(IC):
             self.data.copy_(torch.as_tensor(np.asarray(IC, dtype=np.float64)))
         self.grad_x = self.grad_y = self.grad_z = None
 

@@ -99,8 +99,8 @@ def closure_torch(u, v, w, spacing, delta, W1, b1, W2, b2, W3, b3, rounding=True
         rnd, dt = (lambda t: t), torch.float64
     W1, b1, W2, b2, W3, b3 = (t.to(dt) for t in (W1, b1, W2, b2, W3, b3))
     x = rnd(x.to(dt))
-    h1 = rnd(torch.tanh(x @ rnd(W1).T + b1))
-    h2 = rnd(torch.tanh(h1 @ rnd(W2).T + b2))
+    h1 = rnd(torch.tanh(rnd(x @ rnd(W1).T + b1)))
+    h2 = rnd(torch.tanh(rnd(h1 @ rnd(W2).T + b2)))
     y = h2 @ rnd(W3).T + b3
     F = y.to(torch.float64) * ((delta * delta) * g2)
     return F.T.reshape((6,) + tuple(shape)).contiguous()

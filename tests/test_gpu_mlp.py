@@ -1,9 +1,14 @@
-"""The tensor-core SGS MLP closure (pf_mlp_closure) vs a torch model of the
-same arithmetic (BF16 inputs, weights and hidden activations; FP32
-accumulation).  Tolerance: 3e-2 of the output range -- the kernel's hardware
-tanh (tanh.approx.f32, relative error ~1e-3.5) and the tensor core's FP32
-summation order can flip the BF16 rounding of a hidden activation, which
-moves an output by a few BF16 ulps of its inputs."""
+"""The tensor-core SGS MLP closure (pf_mlp_closure) against two torch models:
+
+* a model of the same arithmetic (BF16 inputs and weights, FP32 accumulation,
+  BF16 pre-activations and activations).  Tolerance: 3e-2 of the output range
+  -- the kernel's hardware tanh (tanh.approx.bf16x2) and the tensor core's
+  FP32 summation order can flip the BF16 rounding of a hidden activation,
+  which moves an output by a few BF16 ulps of its inputs;
+* the FP64 model (the network with the same BF16-valued weights evaluated in
+  FP64 without roundings): the closure's error against exact arithmetic.
+  Tolerance: 5e-2 of the output range at any cell, 1.5e-2 in RMS.
+"""
 import numpy as np
 import pytest
 import torch
@@ -37,6 +42,37 @@ def test_mlp_closure_matches_bf16_model(shape):
     # most cells agree to FP32 accumulation order
     close = ((got - ref).abs() <= 1e-4 * scale).double().mean().item()
     assert close > 0.9, close
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 20, 36)])
+def test_mlp_closure_vs_fp64_model(shape):
+    import pyflow_b200.initial as ic
+    import pyflow_b200.sfsmodel_mlp as M
+    sp = tuple(2 * np.pi / n for n in shape)
+    u, v, w = (torch.tensor(a, device="cuda") for a in
+               ic.spectral_velocity(shape, k0=3.0, seed=5))
+    params = M.xavier_init(1)
+    rng = np.random.default_rng(8)
+    for k in ("b1", "b2", "b3"):
+        params[k] = (0.1 * rng.standard_normal(params[k].shape)).astype(np.float32)
+    wpack = torch.as_tensor(M.pack(params)).cuda()
+    out, g9, scales, err = M.closure(u, v, w, sp, wpack, delta=sp[0])
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    g2 = torch.mean(g9 * g9)
+    x = g9.reshape(9, -1).T / torch.sqrt(g2)
+    W = {k: M._bf16(torch.as_tensor(params[k], device="cuda")).double()
+         for k in ("W1", "W2", "W3")}
+    b = {k: torch.as_tensor(params[k], device="cuda").double() for k in ("b1", "b2", "b3")}
+    h1 = torch.tanh(x @ W["W1"].T + b["b1"])
+    h2 = torch.tanh(h1 @ W["W2"].T + b["b2"])
+    y = (h2 @ W["W3"].T + b["b3"]) * ((sp[0] * sp[0]) * g2)
+    ref = y.T.reshape(out.shape)
+    scale = ref.abs().max().item()
+    d = (out - ref).abs()
+    assert d.max().item() <= 5e-2 * scale, (d.max().item(), scale)
+    rms = torch.sqrt(torch.mean((out - ref) ** 2) / torch.mean(ref ** 2)).item()
+    assert rms <= 1.5e-2, rms
 
 
 def test_mlp_in_rhs_slot_runs():
