@@ -106,6 +106,8 @@ def parse(argv=None):
                     help="serve workload: number of requests")
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the request-stream measurement in the main run")
+    ap.add_argument("--no-les", action="store_true",
+                    help="skip the LES training measurement (64^3 LES, 256^3 DNS targets)")
     return ap.parse_args(argv)
 
 
@@ -479,6 +481,39 @@ def serve_measurement(a, torch, dev):
                     "admission by live free HBM"}
 
 
+def les_measurement(torch, dev, windows=3):
+    """LES training at its stated size: a 64^3 LES with the tensor-core MLP
+    closure (nu = 0.001, dt = 0.005), targets from a 256^3 FP64 DNS (seed 2)
+    box-filtered to 64^3, 20-step windows with the loss's gradient through
+    the hand-written adjoint (one checkpoint per step) and an RMSprop update
+    per window.  Times the target DNS and each window (forward + backward +
+    update) with CUDA events."""
+    import pyflow_b200.training as T
+    cfg = T.LESConfig()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    targets = T.dns_targets(cfg, device=dev)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    dns_s = e0.elapsed_time(e1) / 1e3
+    tr = T.Trainer(cfg, targets, device=dev)
+    times, losses = [], []
+    for _ in range(windows):
+        e0.record(st)
+        losses.append(tr.step())
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        times.append(e0.elapsed_time(e1) / 1e3)
+    del targets, tr
+    return {"les_grid": cfg.n, "dns_grid": cfg.n * cfg.factor, "window_steps": cfg.steps,
+            "nu": cfg.nu, "dt": cfg.dt, "dns_seed": cfg.dns_seed, "mlp_seed": cfg.mlp_seed,
+            "target_dns_s": dns_s, "window_s": times, "loss": losses,
+            "les_cell_steps_per_s_fwd_bwd": cfg.n ** 3 * cfg.steps / float(np.median(times)),
+            "note": "forward LES steps with the closure on the tensor cores, backward "
+                    "through the stage-exact RK4 adjoint with recomputed stages"}
+
+
 def run_serve(a, torch, dev):
     sv = serve_measurement(a, torch, dev)
     line = {"metric": "serve latency p50/p99 (s) and aggregate cell-steps/s",
@@ -549,7 +584,7 @@ def run_b200(a):
                         "included in both times" % acc_steps}
         torch.cuda.empty_cache()
 
-    roof, ktimes, e2e, mlp, cpu, serve = None, {}, None, None, None, None
+    roof, ktimes, e2e, mlp, cpu, serve, les = None, {}, None, None, None, None, None
     prof_steps = 2
     if not a.no_extras:
         # per-kernel device time: CUDA events around each launch of the
@@ -582,6 +617,9 @@ def run_b200(a):
             if not a.no_serve and world == 1:
                 serve = serve_measurement(a, torch, dev)
                 torch.cuda.empty_cache()
+            if not a.no_les and world == 1:
+                les = les_measurement(torch, dev)
+                torch.cuda.empty_cache()
     if rank == 0 and not a.no_cpu_baseline:
         its_ref = fp64["iterations_per_step"] if fp64 else wl["fp64_its"]
         val, desc, work = cpu_rate(wl, u0, v0, w0, a.cpu_budget, n >= 256, its_ref)
@@ -602,7 +640,7 @@ def run_b200(a):
                                                 "max_div")},
             "fp64_arm": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * a.steps)) if launches_per_step else None,
-            "clocks": clocks, "mlp_tensor_core": mlp, "serve": serve,
+            "clocks": clocks, "mlp_tensor_core": mlp, "serve": serve, "les_training": les,
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ktimes.items()},
         }
         print(json.dumps(line), flush=True)

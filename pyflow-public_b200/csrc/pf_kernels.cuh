@@ -29,16 +29,12 @@ struct GroupMember {
     void* R;
 };
 constexpr int kMaxBatch = 64;  // requests of one grouped launch
-// Device bytes of the per-stage job tables of `count` requests.
-size_t grouped_predictor_table_bytes(int count);
-// Writes the job tables (synchronous on s) and prepares the kernels; call
-// before any capture of launch_grouped_predictor with the same members.
-int grouped_predictor_tables(int prec, int rk4, const GroupMember* m, int count,
-                             void* table, cudaStream_t s);
+// Kernel attributes of the grouped stage kernels (before any capture).
+int grouped_predictor_prepare(int prec);
 // The predictor of every member, one launch per RK4 stage (constant
 // viscosity, no SFS stresses); same results as launch_predictor per member.
 cudaError_t launch_grouped_predictor(int prec, int rk4, const GroupMember* m, int count,
-                                     void* table, cudaStream_t s);
+                                     cudaStream_t s);
 
 size_t poisson_ws_bytes(const pf_grid* g, int prec);
 int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
@@ -69,9 +65,7 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
                      double dt, double min_res, int max_it, void* ws,
                      double* stats, void** out);
 int step_plan_launch(void* plan, int nsteps, cudaStream_t s);
-size_t batch_table_bytes(int count);
-int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
-                      size_t table_bytes, void** out);
+int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void** out);
 int step_plan_destroy(void* plan);
 
 }  // namespace pf

@@ -1174,12 +1174,8 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
     return PF_OK;
 }
 
-size_t batch_table_bytes(int count) { return grouped_predictor_table_bytes(count); }
-
-int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
-                      size_t table_bytes, void** out) {
-    if (count < 1 || count > kMaxBatch || table_bytes < batch_table_bytes(count))
-        return PF_ERR_BAD_ARG;
+int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void** out) {
+    if (count < 1 || count > kMaxBatch) return PF_ERR_BAD_ARG;
     PlanLayout* P = new PlanLayout[count];
     int rc = PF_OK;
     for (int r = 0; r < count && rc == PF_OK; ++r) rc = plan_layout(&m[r].grid, prec, m[r].ws, &P[r]);
@@ -1190,12 +1186,12 @@ int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, vo
         delete[] P;
         return PF_ERR_CUDA;
     }
-    // job tables of the grouped predictor, and each request's one-time set-up
+    // the grouped predictor's members, and each request's one-time set-up
     GroupMember gm[kMaxBatch];
     for (int r = 0; r < count; ++r)
         gm[r] = GroupMember{m[r].grid, m[r].u, m[r].v, m[r].w, m[r].mu, m[r].rho, m[r].dt,
                             P[r].R};
-    rc = grouped_predictor_tables(prec, rk4, gm, count, table, cs);
+    rc = grouped_predictor_prepare(prec);
     // one-time set-up of members that join a plan for the first time; a
     // member carried over from an earlier plan may still be computing there
     // and is not touched
@@ -1210,7 +1206,7 @@ int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, vo
         cudaGraph_t G = plan->graph;
         cudaGraphNode_t n0;
         if ((rc = add_captured(G, cs, [&](cudaStream_t st) {
-                 return launch_grouped_predictor(prec, rk4, gm, count, table, st);
+                 return launch_grouped_predictor(prec, rk4, gm, count, st);
              }, &n0)))
             break;
         // the requests' solves run as independent branches of the graph

@@ -69,25 +69,40 @@ struct GatherSrc {
     }
 };
 
+// The six x-face terms of a cell that the cell at i+1 reuses as its x-minus
+// terms: the viscous fluxes fxx (centre), fxy, fxz (x-edges) and the
+// convective products u u, v u, w u on the x-plus side.  Each is the same
+// expression, with the same operands in the same order, as the x-minus term
+// of the next cell, so reusing it changes no rounding.
+template <typename T>
+struct XFace {
+    T fxx, fxy, fxz, cuu, cvu, cwu;
+};
+
 // Computes (ru, rv, rw) of one cell from its neighbourhood S (velocity at
 // offsets -1..1, viscosity / SFS stresses at offsets -2..0 when present).
-template <typename T, class Src>
+// With CARRY, the x-minus terms come from *xin (the x-plus terms of the cell
+// at i-1: constant viscosity, no SFS stresses) and the velocity at i-1 is not
+// read; *xout, when given, receives this cell's x-plus terms.
+template <typename T, bool CARRY = false, class Src>
 __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
-                                bool has_visc, bool has_sfs, T& ru_o, T& rv_o, T& rw_o) {
+                                bool has_visc, bool has_sfs, T& ru_o, T& rv_o, T& rw_o,
+                                const XFace<T>* xin = nullptr, XFace<T>* xout = nullptr) {
     auto LV = [&](int di, int dj, int dk) -> T { return has_visc ? S.visc(di, dj, dk) : mu; };
     auto LS = [&](int c, int di, int dj, int dk) -> T { return S.sfs(c, di, dj, dk); };
     // velocity neighbourhood
-    const T u_c = S.u(0, 0, 0), u_xp = S.u(1, 0, 0), u_xm = S.u(-1, 0, 0);
+    // (the x-minus neighbours are read only without CARRY)
+    const T u_c = S.u(0, 0, 0), u_xp = S.u(1, 0, 0), u_xm = CARRY ? T(0) : S.u(-1, 0, 0);
     const T u_yp = S.u(0, 1, 0), u_ym = S.u(0, -1, 0), u_zp = S.u(0, 0, 1);
-    const T u_zm = S.u(0, 0, -1), u_xm_yp = S.u(-1, 1, 0), u_xp_ym = S.u(1, -1, 0);
-    const T u_xm_zp = S.u(-1, 0, 1), u_xp_zm = S.u(1, 0, -1);
-    const T v_c = S.v(0, 0, 0), v_xp = S.v(1, 0, 0), v_xm = S.v(-1, 0, 0);
+    const T u_zm = S.u(0, 0, -1), u_xm_yp = CARRY ? T(0) : S.u(-1, 1, 0), u_xp_ym = S.u(1, -1, 0);
+    const T u_xm_zp = CARRY ? T(0) : S.u(-1, 0, 1), u_xp_zm = S.u(1, 0, -1);
+    const T v_c = S.v(0, 0, 0), v_xp = S.v(1, 0, 0), v_xm = CARRY ? T(0) : S.v(-1, 0, 0);
     const T v_yp = S.v(0, 1, 0), v_ym = S.v(0, -1, 0), v_zp = S.v(0, 0, 1);
-    const T v_zm = S.v(0, 0, -1), v_xm_yp = S.v(-1, 1, 0), v_xp_ym = S.v(1, -1, 0);
+    const T v_zm = S.v(0, 0, -1), v_xm_yp = CARRY ? T(0) : S.v(-1, 1, 0), v_xp_ym = S.v(1, -1, 0);
     const T v_ym_zp = S.v(0, -1, 1), v_yp_zm = S.v(0, 1, -1);
-    const T w_c = S.w(0, 0, 0), w_xp = S.w(1, 0, 0), w_xm = S.w(-1, 0, 0);
+    const T w_c = S.w(0, 0, 0), w_xp = S.w(1, 0, 0), w_xm = CARRY ? T(0) : S.w(-1, 0, 0);
     const T w_yp = S.w(0, 1, 0), w_ym = S.w(0, -1, 0), w_zp = S.w(0, 0, 1);
-    const T w_zm = S.w(0, 0, -1), w_xm_zp = S.w(-1, 0, 1), w_xp_zm = S.w(1, 0, -1);
+    const T w_zm = S.w(0, 0, -1), w_xm_zp = CARRY ? T(0) : S.w(-1, 0, 1), w_xp_zm = S.w(1, 0, -1);
     const T w_ym_zp = S.w(0, -1, 1), w_yp_zm = S.w(0, 1, -1);
 
     // FP64 keeps the reference's divisions (bit-exact parity); the FP32 stage
@@ -102,14 +117,14 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
         if constexpr (f32) return s * T(1.0f / 3.0f); else return s / T(3.0);
     };
     const T D_c = div3(u_xp, u_c, v_yp, v_c, w_zp, w_c);
-    const T D_xm = div3(u_c, u_xm, v_xm_yp, v_xm, w_xm_zp, w_xm);
+    const T D_xm = CARRY ? T(0) : div3(u_c, u_xm, v_xm_yp, v_xm, w_xm_zp, w_xm);
     const T D_ym = div3(u_xp_ym, u_ym, v_c, v_ym, w_ym_zp, w_ym);
     const T D_zm = div3(u_xp_zm, u_zm, v_yp_zm, v_zm, w_c, w_zm);
 
     const T two = T(2.0);
     // diagonal viscous fluxes at centres
     const T fxx_c = ((u_xp - u_c) * dxi - D_c) * over_rho(two * LV(0, 0, 0));
-    const T fxx_m = ((u_c - u_xm) * dxi - D_xm) * over_rho(two * LV(-1, 0, 0));
+    const T fxx_m = CARRY ? xin->fxx : ((u_c - u_xm) * dxi - D_xm) * over_rho(two * LV(-1, 0, 0));
     const T fyy_c = ((v_yp - v_c) * dyi - D_c) * over_rho(two * LV(0, 0, 0));
     const T fyy_m = ((v_c - v_ym) * dyi - D_ym) * over_rho(two * LV(0, -1, 0));
     const T fzz_c = ((w_zp - w_c) * dzi - D_c) * over_rho(two * LV(0, 0, 0));
@@ -135,10 +150,12 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
     // off-diagonal viscous fluxes on edges: (grad_y u + grad_x v) * (Vxy / rho)
     const T fxy_c = (((u_yp - u_c) * dyi) + ((v_xp - v_c) * dxi)) * over_rho(vxy_c);
     const T fxy_ym = (((u_c - u_ym) * dyi) + ((v_xp_ym - v_ym) * dxi)) * over_rho(vxy_ym);
-    const T fxy_xm = (((u_xm_yp - u_xm) * dyi) + ((v_c - v_xm) * dxi)) * over_rho(vxy_xm);
+    const T fxy_xm = CARRY ? xin->fxy
+                           : (((u_xm_yp - u_xm) * dyi) + ((v_c - v_xm) * dxi)) * over_rho(vxy_xm);
     const T fxz_c = (((u_zp - u_c) * dzi) + ((w_xp - w_c) * dxi)) * over_rho(vxz_c);
     const T fxz_zm = (((u_c - u_zm) * dzi) + ((w_xp_zm - w_zm) * dxi)) * over_rho(vxz_zm);
-    const T fxz_xm = (((u_xm_zp - u_xm) * dzi) + ((w_c - w_xm) * dxi)) * over_rho(vxz_xm);
+    const T fxz_xm = CARRY ? xin->fxz
+                           : (((u_xm_zp - u_xm) * dzi) + ((w_c - w_xm) * dxi)) * over_rho(vxz_xm);
     const T fyz_c = (((v_zp - v_c) * dzi) + ((w_yp - w_c) * dyi)) * over_rho(vyz_c);
     const T fyz_zm = (((v_c - v_zm) * dzi) + ((w_yp_zm - w_zm) * dyi)) * over_rho(vyz_zm);
     const T fyz_ym = (((v_ym_zp - v_ym) * dzi) + ((w_c - w_ym) * dyi)) * over_rho(vyz_ym);
@@ -181,9 +198,14 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
 
     // convective fluxes (vel_conv_*, metric_staggered.py:458-526)
     const T h = T(0.5), one = T(1.0);
+    T cuu_p, cvu_p, cwu_p;  // this cell's x-plus convective products
     {
-        const T cp = h * (u_xp + u_c), cm = h * (u_c + u_xm);
-        ru -= (cp * cp - cm * cm) * dxi * one;
+        const T cp = h * (u_xp + u_c);
+        cuu_p = cp * cp;
+        T cmm;
+        if constexpr (CARRY) cmm = xin->cuu;
+        else { const T cm = h * (u_c + u_xm); cmm = cm * cm; }
+        ru -= (cuu_p - cmm) * dxi * one;
         const T uyp = h * (u_yp + u_c), uym = h * (u_c + u_ym);
         const T vxp = h * (v_yp + v_xm_yp), vxm = h * (v_c + v_xm);
         ru -= (uyp * vxp - uym * vxm) * dyi * one;
@@ -192,9 +214,13 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
         ru -= (uzp * wxp - uzm * wxm) * dzi * one;
     }
     {
-        const T vxp = h * (v_xp + v_c), vxm = h * (v_c + v_xm);
-        const T uyp = h * (u_xp + u_xp_ym), uym = h * (u_c + u_ym);
-        rv -= (vxp * uyp - vxm * uym) * dxi * one;
+        const T vxp = h * (v_xp + v_c);
+        const T uyp = h * (u_xp + u_xp_ym);
+        cvu_p = vxp * uyp;
+        T mm;
+        if constexpr (CARRY) mm = xin->cvu;
+        else { const T vxm = h * (v_c + v_xm), uym = h * (u_c + u_ym); mm = vxm * uym; }
+        rv -= (cvu_p - mm) * dxi * one;
         const T cp = h * (v_yp + v_c), cm = h * (v_c + v_ym);
         rv -= (cp * cp - cm * cm) * dyi * one;
         const T vzp = h * (v_zp + v_c), vzm = h * (v_c + v_zm);
@@ -202,9 +228,13 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
         rv -= (vzp * wyp - vzm * wym) * dzi * one;
     }
     {
-        const T wxp = h * (w_xp + w_c), wxm = h * (w_c + w_xm);
-        const T uzp = h * (u_xp + u_xp_zm), uzm = h * (u_c + u_zm);
-        rw -= (wxp * uzp - wxm * uzm) * dxi * one;
+        const T wxp = h * (w_xp + w_c);
+        const T uzp = h * (u_xp + u_xp_zm);
+        cwu_p = wxp * uzp;
+        T mm;
+        if constexpr (CARRY) mm = xin->cwu;
+        else { const T wxm = h * (w_c + w_xm), uzm = h * (u_c + u_zm); mm = wxm * uzm; }
+        rw -= (cwu_p - mm) * dxi * one;
         const T wyp = h * (w_yp + w_c), wym = h * (w_c + w_ym);
         const T vzp = h * (v_yp + v_yp_zm), vzm = h * (v_c + v_zm);
         rw -= (wyp * vzp - wym * vzm) * dyi * one;
@@ -212,6 +242,7 @@ __device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
         rw -= (cp * cp - cm * cm) * dzi * one;
     }
     ru_o = ru; rv_o = rv; rw_o = rw;
+    if (xout) *xout = XFace<T>{fxx_c, fxy_c, fxz_c, cuu_p, cvu_p, cwu_p};
 }
 
 template <typename T, typename TI>
@@ -416,6 +447,7 @@ rhs_tile_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
         convert(i0);
         convert(i0 + 1);
         __syncthreads();
+        XFace<T> xf[2];  // x-plus terms of this thread's two cells on the last plane
         for (int i = i0; i < i1; ++i) {
             const int c = i - i0;
             const int s0 = c & 3, s1 = (c + 1) & 3, s2 = (c + 2) & 3;
@@ -427,7 +459,13 @@ rhs_tile_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
                 const int jl = ty + 8 * r;
                 SmemSrc<T, T> src{ring, s0, s1, s2, jl + 1, tx + 1};
                 T k3[3];
-                rhs_core<T>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false, k3[0], k3[1], k3[2]);
+                // the x-minus terms of plane i are the x-plus terms of plane i-1
+                if (i == i0)
+                    rhs_core<T, false>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
+                                       k3[0], k3[1], k3[2], nullptr, &xf[r]);
+                else
+                    rhs_core<T, true>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
+                                      k3[0], k3[1], k3[2], &xf[r], &xf[r]);
                 const long long q = (long long)i * plane + coff[r];
                 const int pc = (jl + 1) * kRhsSZ + tx + 1;
 #pragma unroll
@@ -528,6 +566,7 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
+        XFace<T> xf[2];  // x-plus terms of this thread's two cells on the last plane
         for (int i = i0; i < i1; ++i) {
             const int c = i - i0;
             const int s0 = c & 3, s1 = (c + 1) & 3, s2 = (c + 2) & 3;
@@ -543,7 +582,13 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
                 const int jl = ty + 8 * r;
                 SmemSrc<T, TI> src{ring, s0, s1, s2, jl + 1, tx + 1};
                 T k3[3];
-                rhs_core<T>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false, k3[0], k3[1], k3[2]);
+                // the x-minus terms of plane i are the x-plus terms of plane i-1
+                if (i == i0)
+                    rhs_core<T, false>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
+                                       k3[0], k3[1], k3[2], nullptr, &xf[r]);
+                else
+                    rhs_core<T, true>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
+                                      k3[0], k3[1], k3[2], &xf[r], &xf[r]);
                 const long long q = (long long)i * plane + coff[r];
                 const int cc = jl * 32 + tx;
 #pragma unroll
@@ -593,11 +638,13 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
 }
 
 // Grouped stage: one launch advances the same RK4 stage of several
-// independent solves (a batch of requests, any grid sizes).  jobs[r] holds
+// independent solves (a batch of requests, any grid sizes).  jobs.j[r] holds
 // request r's grid, tiling, stage arguments and the index of its first tile
 // in the batch's tile space; a block walks the batch's tiles (persistent
 // loop) and runs each with its request's arguments, so every tile computes
-// exactly what the single-request launch computes.
+// exactly what the single-request launch computes.  The job table is a
+// by-value kernel parameter (it lives in the constant bank, read with a
+// block-uniform index like the single launch's parameters).
 template <typename T, typename TI>
 struct StageJob {
     Dims d;
@@ -611,19 +658,23 @@ struct StageJob {
 
 constexpr int kMaxGroupJobs = kMaxBatch;
 
+template <typename T, typename TI>
+struct StageJobs {
+    StageJob<T, TI> j[kMaxGroupJobs];
+};
+static_assert(sizeof(StageJobs<double, double>) + 16 <= 32764,
+              "the job table must fit the kernel parameter space");
+
 template <typename T, typename TI, int MODE>
 __global__ void __launch_bounds__(256, 2)
-rhs_stage_grouped(const StageJob<T, TI>* __restrict__ jobs, int njobs, long long ntiles) {
-    __shared__ long long first[kMaxGroupJobs];
-    for (int r = threadIdx.y * 32 + threadIdx.x; r < njobs; r += 256) first[r] = jobs[r].tile0;
-    __syncthreads();
+rhs_stage_grouped(const __grid_constant__ StageJobs<T, TI> jobs, int njobs, long long ntiles) {
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         int lo = 0, hi = njobs - 1;  // last job whose first tile is <= t
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (first[mid] <= t) lo = mid; else hi = mid - 1;
+            if (jobs.j[mid].tile0 <= t) lo = mid; else hi = mid - 1;
         }
-        const StageJob<T, TI>& J = jobs[lo];
+        const StageJob<T, TI>& J = jobs.j[lo];
         stage_tile<T, TI, T, T, MODE>(J.d, J.tl, J.a, J.u, J.v, J.w, J.su, J.sv, J.sw, J.au,
                                       J.av, J.aw, J.hdt, J.c6, t - J.tile0);
     }
@@ -784,24 +835,13 @@ static cudaError_t grouped_prepare() {
     cudaError_t e = cudaFuncSetAttribute(rhs_stage_grouped<T, TI, MODE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e == cudaSuccess) {
-        const size_t two = 2 * (sm + 1024 + kMaxGroupJobs * 8);
+        const size_t two = 2 * (sm + 1024);
         const int pct = (int)std::min<size_t>(100, (two * 100 + 228 * 1024 - 1) / (228 * 1024));
         e = cudaFuncSetAttribute(rhs_stage_grouped<T, TI, MODE>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     }
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
-}
-
-static size_t job_bytes() {
-    return std::max(std::max(sizeof(StageJob<double, double>), sizeof(StageJob<float, double>)),
-                    sizeof(StageJob<float, float>));
-}
-
-static size_t align256r(size_t b) { return (b + 255) & ~size_t(255); }
-
-size_t grouped_predictor_table_bytes(int count) {
-    return 4 * align256r((size_t)std::max(count, 1) * job_bytes());
 }
 
 // Job of one request for one stage (the arguments the single-request
@@ -824,46 +864,7 @@ static StageJob<T, TI> make_job(const GroupMember& m, const TI* in, T* st, T* ac
     return J;
 }
 
-// The four stage tables (or Euler's one) of type T, written into `table`.
-template <typename T>
-static int tables_impl(int rk4, const GroupMember* m, int count, void* table, cudaStream_t s,
-                       long long* ntiles) {
-    const size_t slot = align256r((size_t)count * job_bytes());
-    std::vector<unsigned char> host(4 * slot, 0);
-    long long tiles = 0;
-    for (int r = 0; r < count; ++r) {
-        const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
-        T* ws = (T*)m[r].R;
-        T *sa = ws, *sb = ws + 3 * n, *acc = ws + 6 * n;
-        const double* u = m[r].u;
-        if (!rk4) {
-            auto J = make_job<T, double>(m[r], u, nullptr, acc, tiles);
-            std::memcpy(host.data() + r * sizeof(J), &J, sizeof(J));
-        } else {
-            auto J0 = make_job<T, double>(m[r], u, sa, acc, tiles);
-            auto J1 = make_job<T, T>(m[r], sa, sb, acc, tiles);
-            auto J2 = make_job<T, T>(m[r], sb, sa, acc, tiles);
-            auto J3 = make_job<T, T>(m[r], sa, nullptr, acc, tiles);
-            std::memcpy(host.data() + 0 * slot + r * sizeof(J0), &J0, sizeof(J0));
-            std::memcpy(host.data() + 1 * slot + r * sizeof(J1), &J1, sizeof(J1));
-            std::memcpy(host.data() + 2 * slot + r * sizeof(J2), &J2, sizeof(J2));
-            std::memcpy(host.data() + 3 * slot + r * sizeof(J3), &J3, sizeof(J3));
-        }
-        Dims d{m[r].grid.nx, m[r].grid.ny, m[r].grid.nz, n};
-        tiles += make_tiling(d, kRhsTY).ntiles;
-    }
-    *ntiles = tiles;
-    if (cudaMemcpyAsync(table, host.data(), host.size(), cudaMemcpyHostToDevice, s) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-        return PF_ERR_CUDA;
-    return PF_OK;
-}
-
-int grouped_predictor_tables(int prec, int rk4, const GroupMember* m, int count, void* table,
-                             cudaStream_t s) {
-    if (count < 1 || count > kMaxGroupJobs) return PF_ERR_BAD_ARG;
-    long long tiles = 0;
+int grouped_predictor_prepare(int prec) {
     cudaError_t e = cudaSuccess;
     if (prec == PF_FP64) {
         if ((e = grouped_prepare<double, double, kModeK>()) ||
@@ -871,35 +872,46 @@ int grouped_predictor_tables(int prec, int rk4, const GroupMember* m, int count,
             (e = grouped_prepare<double, double, kModeMid>()) ||
             (e = grouped_prepare<double, double, kModeLast>()))
             return PF_ERR_CUDA;
-        return tables_impl<double>(rk4, m, count, table, s, &tiles);
+        return PF_OK;
     }
     if ((e = grouped_prepare<float, double, kModeK>()) ||
         (e = grouped_prepare<float, double, kModeFirst>()) ||
         (e = grouped_prepare<float, float, kModeMid>()) ||
         (e = grouped_prepare<float, float, kModeLast>()))
         return PF_ERR_CUDA;
-    return tables_impl<float>(rk4, m, count, table, s, &tiles);
+    return PF_OK;
 }
 
 template <typename T>
-static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, void* table,
-                                cudaStream_t s) {
-    const size_t slot = align256r((size_t)count * job_bytes());
+static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, cudaStream_t s) {
+    if (count < 1 || count > kMaxGroupJobs) return cudaErrorInvalidValue;
+    // the stage tables (built on the host, passed by value)
+    auto* J0 = new StageJobs<T, double>();
+    auto* J1 = new StageJobs<T, T>();
+    auto* J2 = new StageJobs<T, T>();
+    auto* J3 = new StageJobs<T, T>();
     long long tiles = 0;
     for (int r = 0; r < count; ++r) {
-        Dims d{m[r].grid.nx, m[r].grid.ny, m[r].grid.nz,
-               (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz};
-        tiles += make_tiling(d, kRhsTY).ntiles;
+        const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
+        T* ws = (T*)m[r].R;
+        T *sa = ws, *sb = ws + 3 * n, *acc = ws + 6 * n;
+        if (!rk4) {
+            J0->j[r] = make_job<T, double>(m[r], m[r].u, nullptr, acc, tiles);
+        } else {
+            J0->j[r] = make_job<T, double>(m[r], m[r].u, sa, acc, tiles);
+            J1->j[r] = make_job<T, T>(m[r], sa, sb, acc, tiles);
+            J2->j[r] = make_job<T, T>(m[r], sb, sa, acc, tiles);
+            J3->j[r] = make_job<T, T>(m[r], sa, nullptr, acc, tiles);
+        }
+        tiles += J0->j[r].tl.ntiles;
     }
     const int grid = (int)std::min<long long>(tiles, num_sms() * 2);
     const dim3 blk(32, 8);
     const bool f64 = sizeof(T) == 8;
-    char* tb = (char*)table;
     if (!rk4) {
         PF_LAUNCH(f64 ? "grouped_euler_f64" : "grouped_euler_f32", s,
                   (rhs_stage_grouped<T, double, kModeK><<<grid, blk,
-                      RhsSmem<T, double, T, kModeK>::bytes, s>>>(
-                      (const StageJob<T, double>*)tb, count, tiles)));
+                      RhsSmem<T, double, T, kModeK>::bytes, s>>>(*J0, count, tiles)));
         for (int r = 0; r < count; ++r) {
             const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
             const T* acc = (const T*)m[r].R + 6 * n;
@@ -907,29 +919,28 @@ static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, void* 
             PF_LAUNCH("euler_apply", s, euler_apply<T><<<gp, 256, 0, s>>>(
                 n, acc, acc + n, acc + 2 * n, m[r].dt, m[r].u, m[r].v, m[r].w));
         }
-        return cudaGetLastError();
+    } else {
+        PF_LAUNCH(f64 ? "grouped_first_f64" : "grouped_first_f32", s,
+                  (rhs_stage_grouped<T, double, kModeFirst><<<grid, blk,
+                      RhsSmem<T, double, T, kModeFirst>::bytes, s>>>(*J0, count, tiles)));
+        PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
+                  (rhs_stage_grouped<T, T, kModeMid><<<grid, blk,
+                      RhsSmem<T, T, T, kModeMid>::bytes, s>>>(*J1, count, tiles)));
+        PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
+                  (rhs_stage_grouped<T, T, kModeMid><<<grid, blk,
+                      RhsSmem<T, T, T, kModeMid>::bytes, s>>>(*J2, count, tiles)));
+        PF_LAUNCH(f64 ? "grouped_last_f64" : "grouped_last_f32", s,
+                  (rhs_stage_grouped<T, T, kModeLast><<<grid, blk,
+                      RhsSmem<T, T, T, kModeLast>::bytes, s>>>(*J3, count, tiles)));
     }
-    PF_LAUNCH(f64 ? "grouped_first_f64" : "grouped_first_f32", s,
-              (rhs_stage_grouped<T, double, kModeFirst><<<grid, blk,
-                  RhsSmem<T, double, T, kModeFirst>::bytes, s>>>(
-                  (const StageJob<T, double>*)tb, count, tiles)));
-    PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
-              (rhs_stage_grouped<T, T, kModeMid><<<grid, blk, RhsSmem<T, T, T, kModeMid>::bytes,
-                  s>>>((const StageJob<T, T>*)(tb + slot), count, tiles)));
-    PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
-              (rhs_stage_grouped<T, T, kModeMid><<<grid, blk, RhsSmem<T, T, T, kModeMid>::bytes,
-                  s>>>((const StageJob<T, T>*)(tb + 2 * slot), count, tiles)));
-    PF_LAUNCH(f64 ? "grouped_last_f64" : "grouped_last_f32", s,
-              (rhs_stage_grouped<T, T, kModeLast><<<grid, blk,
-                  RhsSmem<T, T, T, kModeLast>::bytes, s>>>(
-                  (const StageJob<T, T>*)(tb + 3 * slot), count, tiles)));
+    delete J0; delete J1; delete J2; delete J3;
     return cudaGetLastError();
 }
 
 cudaError_t launch_grouped_predictor(int prec, int rk4, const GroupMember* m, int count,
-                                     void* table, cudaStream_t s) {
-    return prec == PF_FP64 ? grouped_impl<double>(rk4, m, count, table, s)
-                           : grouped_impl<float>(rk4, m, count, table, s);
+                                     cudaStream_t s) {
+    return prec == PF_FP64 ? grouped_impl<double>(rk4, m, count, s)
+                           : grouped_impl<float>(rk4, m, count, s);
 }
 
 cudaError_t predictor_prepare(int prec) {

@@ -35,11 +35,8 @@ class BatchMember(ctypes.Structure):
         ("ws_bytes", ctypes.c_size_t), ("stats", ctypes.c_void_p)]
 
 
-_lib.pf_batch_table_bytes.argtypes = [ctypes.c_int]
-_lib.pf_batch_table_bytes.restype = ctypes.c_size_t
 _lib.pf_batch_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BatchMember),
-                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
-                                      ctypes.POINTER(ctypes.c_void_p)]
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
 _lib.pf_batch_plan_create.restype = ctypes.c_int
 MAX_BATCH = 64
 
@@ -136,20 +133,17 @@ class BatchPlan:
         prec = members[0].prec
         if any(m.prec != prec for m in members):
             raise ValueError("all members of a batch use one precision form")
-        dev = members[0].ws.device
+        self.device = members[0].ws.device
         self.members = list(members)
-        need = _lib.pf_batch_table_bytes(len(members))
-        self.table = torch.empty(need, dtype=torch.uint8, device=dev)
         arr = (BatchMember * len(members))(*(m.c_struct() for m in members))
         self._h = ctypes.c_void_p(0)
         L.check("pf_batch_plan_create", _lib.pf_batch_plan_create(
-            ops.PREC[prec], 1 if rk4 else 0, arr, len(members), ops._p(self.table),
-            self.table.numel(), ctypes.byref(self._h)))
+            ops.PREC[prec], 1 if rk4 else 0, arr, len(members), ctypes.byref(self._h)))
         for m in members:
             m.fresh = False
 
     def launch(self, nsteps=1, stream=None):
-        s = stream if stream is not None else torch.cuda.current_stream(self.table.device)
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
         L.check("pf_step_plan_launch", _lib.pf_step_plan_launch(
             self._h, int(nsteps), ctypes.c_void_p(s.cuda_stream)))
 
