@@ -305,6 +305,7 @@ mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
         if (threadIdx.x == 0) {
             sc->max_b = mx; sc->scale = mx; sc->true_res = mx;
             sc->outer = 0; sc->total = 0; sc->counter = 0u;
+            sc->use64 = 0; sc->prev_ratio = 2.0;
         }
     }
 }
@@ -846,7 +847,10 @@ cudaError_t launch_vel_corr(const pf_grid* g, const double* DP, double scale,
 // ============================================================================
 
 // Refinement control (one thread): after the FP64 residual of a pass, count the
-// pass and its inner iterations and decide whether another pass runs.
+// pass and its inner iterations and decide whether another pass runs, with
+// the host-driven solve's rules: an FP32 pass that ended non-finite or in
+// breakdown was discarded (its fold skipped) and the solve continues with
+// FP64 passes, as it does once two FP32 passes in a row gain less than 2x.
 __global__ void mixed_control(BicgScalars* sc, double min_res, int max_outer,
                               int max_it, cudaGraphConditionalHandle cond) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -855,14 +859,47 @@ __global__ void mixed_control(BicgScalars* sc, double min_res, int max_outer,
     // max|b| == 0: nothing to solve; a NaN max|b| gives a NaN ratio
     const double ratio = sc->max_b == 0.0 ? 0.0 : sc->true_res / sc->max_b;
     const int pass = sc->status;  // status of the inner pass just run
+    const bool failed32 = !sc->use64 && (pass == PF_NONFINITE || pass == PF_BREAKDOWN);
     bool stop = true;
-    if (!(ratio == ratio) || isinf(ratio)) sc->status = PF_NONFINITE;
+    if (sc->use64 && pass == PF_NONFINITE) sc->status = PF_NONFINITE;
+    else if (!(ratio == ratio) || isinf(ratio)) sc->status = PF_NONFINITE;
     else if (ratio <= min_res) sc->status = PF_OK;
-    else if (pass == PF_NONFINITE || pass == PF_BREAKDOWN) sc->status = pass;
     else if (sc->outer >= max_outer || sc->total >= max_it) sc->status = PF_MAXIT;
     else stop = false;
+    if (!stop) {
+        if (failed32 || (!sc->use64 && sc->outer > 1 && ratio > 0.5 * sc->prev_ratio))
+            sc->use64 = 1;
+        sc->prev_ratio = ratio;
+    }
     sc->max_res = ratio;
     if (stop) cudaGraphSetConditional(cond, 0);
+}
+
+// Start of a refinement pass: choose the FP64 or the FP32 pass.
+__global__ void pass_branch(const BicgScalars* sc, cudaGraphConditionalHandle if64) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    cudaGraphSetConditional(if64, sc->use64 ? 1u : 0u);
+}
+
+// An FP64 pass finishes the solve: its inner tolerance is the remaining
+// reduction (set after bicg_init, before the first kernel CA reads it).
+__global__ void pass_tol64(BicgScalars* sc, double min_res) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double ratio = sc->max_b == 0.0 ? 0.0 : sc->true_res / sc->max_b;
+    sc->min_res = ratio > 0.0 ? fmin(0.5, 0.5 * min_res / ratio) : 0.5;
+}
+
+// x += scale * e of the pass just run (its precision is sc->use64); an FP32
+// pass that ended non-finite or in breakdown is discarded.
+__global__ void __launch_bounds__(kBlock)
+fold_mixed(Dims d, const BicgScalars* sc, const float* e32, const double* e64, double* x) {
+    const bool f64 = sc->use64 != 0;
+    if (!f64 && (sc->status == PF_NONFINITE || sc->status == PF_BREAKDOWN)) return;
+    if (f64 && sc->status == PF_NONFINITE) return;
+    const double s = sc->scale;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
+         q += (long long)gridDim.x * blockDim.x)
+        x[q] = x[q] + s * (f64 ? e64[q] : double(e32[q]));
 }
 
 // copy the solve's result next to the monitor statistics:
@@ -1041,55 +1078,115 @@ static int add_solve_chain(cudaGraph_t G, cudaGraphNode_t dep, const pf_grid* g,
         const double kInnerTol = 1e-4;
         const MgPlan& mg = P.mg;
         float* ecorr = mg.L ? mg.e : P.e32;
-        // outer body: inner set-up, inner WHILE, fold + residual + control
-        cudaGraph_t pre = nullptr, post = nullptr, inner_body = nullptr;
-        if ((rc = capture_begin(cs, nullptr))) return rc;
-        if (mg.L) {
-            mg_enqueue_init(mg, sc, part, P.rr, kInnerTol, max_it, cs, min_res);
-        } else {
-            bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, P.rr, 0.0, 0.0, P.v32,
-                                                         P.e32, max_it, kInnerTol);
-            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v32, P.e32);
-        }
-        if ((rc = capture_end(cs, &pre))) return rc;
-        cudaGraphNode_t b0, b1, bw, b3;
-        cudaGraphConditionalHandle hi;
-        if (cudaGraphConditionalHandleCreate(&hi, body, 1, cudaGraphCondAssignDefault) !=
-            cudaSuccess) return PF_ERR_CUDA;
-        {
-            // kernel node of the outer body (the graph that owns the inner
-            // loop) that re-arms the inner condition every pass
+        // FP64 inner vectors (the same region: a pass uses one set)
+        char* r64 = P.R;
+        BicgVecs<double> v64 = carve<double>(r64, (size_t)d.n);
+        double* e64 = (double*)r64;
+        const LapCoef<double> cf64 = lap_coef<double>(g);
+        const Tiling ta64 = make_tiling(d, 8 * PhaseCA<double>::R);
+        const Tiling tb64 = make_tiling(d, 8 * PhaseB<double>::R);
+        // outer body: branch kernel, IF(use64) {FP64 pass} ELSE {FP32 pass},
+        // then fold + residual + control
+        cudaGraphConditionalHandle h32, h64, hif;
+        if (cudaGraphConditionalHandleCreate(&hif, body, 0, cudaGraphCondAssignDefault) !=
+                cudaSuccess)
+            return PF_ERR_CUDA;
+        // a one-thread kernel node: func(args...) with the given argument list
+        auto add_tiny = [](cudaGraph_t gr, void* func, void** args, cudaGraphNode_t* node) {
             cudaKernelNodeParams kp;
             std::memset(&kp, 0, sizeof(kp));
-            void* args[] = {&hi};
-            kp.func = (void*)arm_condition;
+            kp.func = func;
             kp.gridDim = dim3(1);
             kp.blockDim = dim3(32);
             kp.kernelParams = args;
-            if (cudaGraphAddKernelNode(&b0, body, nullptr, 0, &kp) != cudaSuccess)
+            return cudaGraphAddKernelNode(node, gr, nullptr, 0, &kp) == cudaSuccess ? PF_OK
+                                                                                     : PF_ERR_CUDA;
+        };
+        cudaGraphNode_t b0, bif, b3;
+        {
+            BicgScalars* scp = sc;
+            void* args[] = {&scp, &hif};
+            if ((rc = add_tiny(body, (void*)pass_branch, args, &b0))) return rc;
+        }
+        cudaGraph_t br64, br32;
+        {
+            cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
+            prm.conditional.handle = hif;
+            prm.conditional.type = cudaGraphCondTypeIf;
+            prm.conditional.size = 2;
+            if (cudaGraphAddNode(&bif, body, &b0, 1, &prm) != cudaSuccess) return PF_ERR_CUDA;
+            br64 = prm.conditional.phGraph_out[0];
+            br32 = prm.conditional.phGraph_out[1];
+        }
+        // FP32 branch: re-arm its loop, set-up, then the inner WHILE (the
+        // handle belongs to the branch graph that holds the loop)
+        {
+            cudaGraph_t pre = nullptr, inner_body = nullptr;
+            cudaGraphNode_t a0, c1n, cw;
+            if (cudaGraphConditionalHandleCreate(&h32, br32, 1, cudaGraphCondAssignDefault) !=
+                cudaSuccess)
                 return PF_ERR_CUDA;
+            void* args[] = {&h32};
+            if ((rc = add_tiny(br32, (void*)arm_condition, args, &a0))) return rc;
+            if ((rc = capture_begin(cs, nullptr))) return rc;
+            if (mg.L) {
+                mg_enqueue_init(mg, sc, part, P.rr, kInnerTol, max_it, cs, min_res);
+            } else {
+                bicg_init<float, true><<<gp, kBlock, 0, cs>>>(d, sc, part, P.rr, 0.0, 0.0, P.v32,
+                                                             P.e32, max_it, kInnerTol);
+                bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v32,
+                                                               P.e32);
+            }
+            if ((rc = capture_end(cs, &pre))) return rc;
+            rc = add_child(br32, a0, pre, &c1n);
+            cudaGraphDestroy(pre);
+            if (rc) return rc;
+            if ((rc = add_while(br32, c1n, &cw, &inner_body, &h32, false))) return rc;
+            if ((rc = capture_begin(cs, inner_body))) return rc;
+            if (mg.L) {
+                // two iterations per pass of the body: the p buffers alternate
+                mg_enqueue_iteration(mg, sc, part, 0, cs, 1, h32);
+                mg_enqueue_iteration(mg, sc, part, 1, cs, 1, h32);
+            } else {
+                bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, P.v32, 1,
+                                                              h32);
+                bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v32,
+                                                               P.e32, 1, h32);
+            }
+            if ((rc = capture_end(cs, &inner_body))) return rc;
         }
-        rc = add_child(body, b0, pre, &b1);
-        cudaGraphDestroy(pre);
-        if (rc) return rc;
-        if ((rc = add_while(body, b1, &bw, &inner_body, &hi, false))) return rc;
-        if ((rc = capture_begin(cs, inner_body))) return rc;
-        if (mg.L) {
-            // two iterations per pass of the body: the p buffers alternate
-            mg_enqueue_iteration(mg, sc, part, 0, cs, 1, hi);
-            mg_enqueue_iteration(mg, sc, part, 1, cs, 1, hi);
-        } else {
-            bicg_b<float><<<tiled_grid(tb), blk2, 0, cs>>>(d, tb, cf, sc, part, P.v32, 1, hi);
-            bicg_ca<float><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v32, P.e32,
-                                                           1, hi);
+        // FP64 branch: re-arm, set-up with the remaining tolerance, its WHILE
+        {
+            cudaGraph_t pre = nullptr, inner_body = nullptr;
+            cudaGraphNode_t a0, c1n, cw;
+            if (cudaGraphConditionalHandleCreate(&h64, br64, 1, cudaGraphCondAssignDefault) !=
+                cudaSuccess)
+                return PF_ERR_CUDA;
+            void* args[] = {&h64};
+            if ((rc = add_tiny(br64, (void*)arm_condition, args, &a0))) return rc;
+            if ((rc = capture_begin(cs, nullptr))) return rc;
+            bicg_init<double, true><<<gp, kBlock, 0, cs>>>(d, sc, part, P.rr, 0.0, 0.0, v64, e64,
+                                                          max_it, 0.5);
+            pass_tol64<<<1, 32, 0, cs>>>(sc, min_res);
+            bicg_ca<double><<<tiled_grid(ta64), blk2, 0, cs>>>(d, ta64, cf64, sc, part, v64, e64);
+            if ((rc = capture_end(cs, &pre))) return rc;
+            rc = add_child(br64, a0, pre, &c1n);
+            cudaGraphDestroy(pre);
+            if (rc) return rc;
+            if ((rc = add_while(br64, c1n, &cw, &inner_body, &h64, false))) return rc;
+            if ((rc = capture_begin(cs, inner_body))) return rc;
+            bicg_b<double><<<tiled_grid(tb64), blk2, 0, cs>>>(d, tb64, cf64, sc, part, v64, 1, h64);
+            bicg_ca<double><<<tiled_grid(ta64), blk2, 0, cs>>>(d, ta64, cf64, sc, part, v64, e64,
+                                                              1, h64);
+            if ((rc = capture_end(cs, &inner_body))) return rc;
         }
-        if ((rc = capture_end(cs, &inner_body))) return rc;
+        cudaGraph_t post = nullptr;
         if ((rc = capture_begin(cs, nullptr))) return rc;
-        fold_correction<float><<<gp, kBlock, 0, cs>>>(d, sc, ecorr, DP, 1);
+        fold_mixed<<<gp, kBlock, 0, cs>>>(d, sc, ecorr, e64, DP);
         mixed_residual<<<tiled_grid(tld), blk2, 0, cs>>>(d, tld, cfd, sc, part, P.bb, DP, P.rr);
         mixed_control<<<1, 32, 0, cs>>>(sc, min_res, 40, max_it, h);
         if ((rc = capture_end(cs, &post))) return rc;
-        rc = add_child(body, bw, post, &b3);
+        rc = add_child(body, bif, post, &b3);
         cudaGraphDestroy(post);
         if (rc) return rc;
     }

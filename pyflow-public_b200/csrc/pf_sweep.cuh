@@ -20,7 +20,8 @@ struct BicgScalars {
     int done;          // 0 running, 1 stopped, 2 stop after DP += alpha pp
     int status, max_it;
     unsigned int counter;
-    int pad[2];
+    int use64;          // mixed graph mode: the next refinement pass runs in FP64
+    double prev_ratio;  // mixed graph mode: true residual ratio after the previous pass
 };
 
 template <typename T>

@@ -42,6 +42,35 @@ def test_plan_matches_forward_step(prec, shape):
                                ref, rtol=1e-14, atol=1e-18)
 
 
+def test_plan_mixed_fp64_fallback_matches_host_solve():
+    """Unpreconditioned FP32 passes stall at 256^3 (their matvec's relative
+    rounding error on the smoothest modes reaches the inner tolerance); the
+    host-driven solve then switches to FP64 passes, and the captured step
+    takes the same branch (an IF node on a device flag): both converge to the
+    reference's tolerance with the same iteration count and the same
+    velocity."""
+    import pyflow_b200.initial as ic
+    import pyflow_b200.ops as ops
+    from pyflow_b200.plan import StepPlan
+    shape = (256, 256, 256)
+    sp = tuple(2 * np.pi / n for n in shape)
+    f0 = [t.contiguous() for t in ic.spectral_velocity_device(shape, k0=4.0, seed=6)]
+    a = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    info = ops.forward_step(*a, sp, 0.0025, 1.0, 0.00125, min_res=1e-10, max_it=20000,
+                            prec="mixed")
+    b = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    plan = StepPlan(*b, sp, 0.0025, 1.0, 0.00125, min_res=1e-10, max_it=20000, prec="mixed")
+    plan.launch(1)
+    torch.cuda.synchronize()
+    st = plan.stats()
+    plan.close()
+    assert info.status == 0 and info.max_res <= 1e-10
+    assert st["status"] == 0 and st["max_res"] <= 1e-10, st
+    assert int(st["iterations"]) == info.iterations
+    for x, y in zip(a[:3], b[:3]):
+        assert (x - y).abs().max().item() <= 1e-12 * y.abs().max().item()
+
+
 def test_plans_run_concurrently_on_streams():
     """Several plans on their own streams give the same results as alone."""
     import pyflow_b200.initial as ic
