@@ -88,10 +88,12 @@ int pf_laplace_apply(const pf_grid* g, const double* A, double* B,
 
 /* RK4.step (src/solver/advancer.py:75-113) including the reference's stage-4
  * state u + dt/2 k3; u, v, w (FP64) updated in place.  Euler.step
- * (src/solver/advancer.py:49-57) when rk4 == 0. */
+ * (src/solver/advancer.py:49-57) when rk4 == 0.  visc / sfs (NULL or as for
+ * pf_rhs_ns) are in the stage type: double for PF_FP64, float for the mixed
+ * forms. */
 int pf_predictor_step(const pf_grid* g, int prec, int rk4, double* u,
-                      double* v, double* w, const double* visc, double mu,
-                      double rho, const double* sfs, double dt, void* ws,
+                      double* v, double* w, const void* visc, double mu,
+                      double rho, const void* sfs, double dt, void* ws,
                       size_t ws_bytes, void* stream);
 
 /* solver_bicgstab.solve (src/solver/pressure.py:196-297) on
@@ -116,14 +118,15 @@ int pf_jacobi_solve(const pf_grid* g, double rho, double dt, int n_it,
 int pf_vel_corr(const pf_grid* g, const double* DP, double scale, double* u,
                 double* v, double* w, void* stream);
 
-/* Domain.forwardStep with the SFS model off or 'tensor'
- * (src/data/domain.py:342-402): predictor, divergence, Poisson solve
- * (solver 0 = BiCGStab, 1 = Jacobi with max_it sweeps), projection.
- * Synchronous; *info gets the solve result. */
+/* Domain.forwardStep with the SFS model off, 'eddyVisc' (visc = mu + mu_t)
+ * or 'tensor' (src/data/domain.py:342-402): predictor, divergence, Poisson
+ * solve (solver 0 = BiCGStab, 1 = Jacobi with max_it sweeps), projection.
+ * visc / sfs as for pf_predictor_step (stage type).  Synchronous; *info gets
+ * the solve result. */
 int pf_forward_step(const pf_grid* g, int prec, int rk4, int solver,
                     double* u, double* v, double* w, double* p, double* DP,
-                    const double* visc, double mu, double rho,
-                    const double* sfs, double dt, double min_res, int max_it,
+                    const void* visc, double mu, double rho,
+                    const void* sfs, double dt, double min_res, int max_it,
                     void* ws, size_t ws_bytes, void* stream,
                     pf_solve_info* info);
 

@@ -55,11 +55,16 @@ class RK4:
 
     def step(self, simDt):
         a = _fused_args(self.rhsClass)
-        if a is not None and (self.prec == "fp64" or (a["visc"] is None and a["sfs"] is None)):
+        if a is not None:
+            visc, sfs = a["visc"], a["sfs"]
+            if self.prec != "fp64":
+                # the mixed forms' stages read the closure fields in FP32
+                visc = None if visc is None else visc.float()
+                sfs = None if sfs is None else sfs.float()
             ops.predictor_step(self.state_u.interior(), self.state_v.interior(),
                                self.state_w.interior(), a["spacing"], a["mu"],
                                a["rho"], simDt, rk4=True, prec=self.prec,
-                               visc=a["visc"], sfs=a["sfs"])
+                               visc=visc, sfs=sfs)
             return
         rc = self.rhsClass
         u, v, w = self.state_u, self.state_v, self.state_w

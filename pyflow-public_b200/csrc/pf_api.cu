@@ -78,8 +78,8 @@ int pf_laplace_apply(const pf_grid* g, const double* A, double* B, void* stream)
 }
 
 int pf_predictor_step(const pf_grid* g, int prec, int rk4, double* u,
-                      double* v, double* w, const double* visc, double mu,
-                      double rho, const double* sfs, double dt, void* ws,
+                      double* v, double* w, const void* visc, double mu,
+                      double rho, const void* sfs, double dt, void* ws,
                       size_t ws_bytes, void* stream) {
     if (!grid_ok(g) || !prec_ok(prec) || !u || !v || !w || !(rho != 0.0)) return PF_ERR_BAD_ARG;
     if (!ws || ws_bytes < predictor_ws_bytes(g, prec)) return PF_ERR_BAD_ARG;
@@ -112,8 +112,8 @@ int pf_vel_corr(const pf_grid* g, const double* DP, double scale, double* u,
 
 int pf_forward_step(const pf_grid* g, int prec, int rk4, int solver,
                     double* u, double* v, double* w, double* p, double* DP,
-                    const double* visc, double mu, double rho,
-                    const double* sfs, double dt, double min_res, int max_it,
+                    const void* visc, double mu, double rho,
+                    const void* sfs, double dt, double min_res, int max_it,
                     void* ws, size_t ws_bytes, void* stream,
                     pf_solve_info* info) {
     if (!grid_ok(g) || !prec_ok(prec) || !u || !v || !w || !p || !DP || !(rho != 0.0) ||

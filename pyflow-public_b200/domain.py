@@ -140,11 +140,14 @@ class Domain:
                 self.sfsmodel.update(self.state_u_P, self.state_v_P,
                                      self.state_w_P, self.metric)
         fused = (self.doPressure and isinstance(self.forwardRHS, velocity.ForwardRHS)
-                 and (self.precision == "fp64" or not self.use_SFSmodel)
                  and self.sfsmodel.modelType != "source")
         if fused:
             mu, visc = velocity.visc_args(self.VISC_P)
             sfs = velocity.sfs_args(self.sfsmodel) if self.use_SFSmodel else None
+            if self.precision != "fp64":
+                # the mixed forms' stages read the closure fields in FP32
+                visc = None if visc is None else visc.float()
+                sfs = None if sfs is None else sfs.float()
             solver = "bicgstab" if self.pSolverMode == "bicgstab" else "jacobi"
             p = self.poisson
             max_it = (p.max_iterations if solver == "bicgstab"
