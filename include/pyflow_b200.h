@@ -256,8 +256,11 @@ int pf_restart_unpack(const pf_grid* g, const double* file_order, double* field,
  * what its own pf_step_plan would: results are the same alone and in any
  * batch.  A member's fields, workspace (pf_step_plan_workspace_bytes) and
  * stats (10 doubles, the layout of pf_step_plan_create) belong to the plan
- * while it exists; the grouped launches carry the members' arguments as
- * kernel parameters (no device table).  At most 64 members.  A member
+ * while it exists.  table is a caller device buffer of
+ * pf_batch_table_bytes(count) bytes, 256-byte aligned, that holds the grouped
+ * launches' per-member arguments (written at creation) and, in its first int,
+ * an error flag that a grouped launch sets to 1 if it finds a tile outside
+ * every member's range (it then skips the tile).  At most 64 members.  A member
  * with fresh != 0 joins a plan for the first time: creation initialises its
  * solver state (synchronously, on a stream of its own).  A member with
  * fresh == 0 is carried over from an earlier plan, whose launches may still
@@ -273,8 +276,10 @@ typedef struct pf_batch_member {
     size_t ws_bytes;
     double* stats;
 } pf_batch_member;
+size_t pf_batch_table_bytes(int count);
 int pf_batch_plan_create(int prec, int rk4, const pf_batch_member* members,
-                         int count, pf_step_plan** plan);
+                         int count, void* table, size_t table_bytes,
+                         pf_step_plan** plan);
 
 /* Optional per-kernel device-time accounting: when enabled, each kernel launch
  * of the library is bracketed by CUDA events on its stream.  pf_profile_read

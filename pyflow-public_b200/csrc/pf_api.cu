@@ -180,9 +180,16 @@ int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* 
     return rc;
 }
 
-int pf_batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count,
-                         pf_step_plan** plan) {
-    if (!prec_ok(prec) || !m || count < 1 || count > kMaxBatch || !plan) return PF_ERR_BAD_ARG;
+size_t pf_batch_table_bytes(int count) {
+    if (count < 1 || count > kMaxBatch) return 0;
+    return grouped_predictor_table_bytes(count);
+}
+
+int pf_batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
+                         size_t table_bytes, pf_step_plan** plan) {
+    if (!prec_ok(prec) || !m || count < 1 || count > kMaxBatch || !plan || !table ||
+        ((uintptr_t)table & 255) || table_bytes < grouped_predictor_table_bytes(count))
+        return PF_ERR_BAD_ARG;
     for (int r = 0; r < count; ++r) {
         const pf_batch_member& b = m[r];
         if (!grid_ok(&b.grid) || !b.u || !b.v || !b.w || !b.p || !b.DP || !b.stats || !b.ws ||
@@ -191,7 +198,7 @@ int pf_batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count,
             return PF_ERR_BAD_ARG;
     }
     void* p = nullptr;
-    const int rc = batch_plan_create(prec, rk4 ? 1 : 0, m, count, &p);
+    const int rc = batch_plan_create(prec, rk4 ? 1 : 0, m, count, table, &p);
     if (rc == PF_OK) *plan = (pf_step_plan*)p;
     return rc;
 }

@@ -31,10 +31,17 @@ struct GroupMember {
 constexpr int kMaxBatch = 64;  // requests of one grouped launch
 // Kernel attributes of the grouped stage kernels (before any capture).
 int grouped_predictor_prepare(int prec);
+// Device bytes of the grouped stages' job tables for `count` members.
+size_t grouped_predictor_table_bytes(int count);
+// Writes the job tables into `table` (synchronous on s, clears the error
+// flag in its first word) and prepares the kernels; before any capture of
+// launch_grouped_predictor with the same members and table.
+int grouped_predictor_tables(int prec, int rk4, const GroupMember* m, int count,
+                             void* table, cudaStream_t s);
 // The predictor of every member, one launch per RK4 stage (constant
 // viscosity, no SFS stresses); same results as launch_predictor per member.
 cudaError_t launch_grouped_predictor(int prec, int rk4, const GroupMember* m, int count,
-                                     cudaStream_t s);
+                                     void* table, cudaStream_t s);
 
 size_t poisson_ws_bytes(const pf_grid* g, int prec);
 int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
@@ -65,7 +72,8 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
                      double dt, double min_res, int max_it, void* ws,
                      double* stats, void** out);
 int step_plan_launch(void* plan, int nsteps, cudaStream_t s);
-int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void** out);
+int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
+                      void** out);
 int step_plan_destroy(void* plan);
 
 }  // namespace pf

@@ -1271,7 +1271,8 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
     return PF_OK;
 }
 
-int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void** out) {
+int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
+                      void** out) {
     if (count < 1 || count > kMaxBatch) return PF_ERR_BAD_ARG;
     PlanLayout* P = new PlanLayout[count];
     int rc = PF_OK;
@@ -1288,7 +1289,7 @@ int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, vo
     for (int r = 0; r < count; ++r)
         gm[r] = GroupMember{m[r].grid, m[r].u, m[r].v, m[r].w, m[r].mu, m[r].rho, m[r].dt,
                             P[r].R};
-    rc = grouped_predictor_prepare(prec);
+    rc = grouped_predictor_tables(prec, rk4, gm, count, table, cs);
     // one-time set-up of members that join a plan for the first time; a
     // member carried over from an earlier plan may still be computing there
     // and is not touched
@@ -1303,7 +1304,7 @@ int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, vo
         cudaGraph_t G = plan->graph;
         cudaGraphNode_t n0;
         if ((rc = add_captured(G, cs, [&](cudaStream_t st) {
-                 return launch_grouped_predictor(prec, rk4, gm, count, st);
+                 return launch_grouped_predictor(prec, rk4, gm, count, table, st);
              }, &n0)))
             break;
         // the requests' solves run as independent branches of the graph

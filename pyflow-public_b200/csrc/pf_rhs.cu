@@ -20,6 +20,7 @@
 #include "pf_kernels.cuh"
 #include "pf_profile.cuh"
 #include "pf_sweep.cuh"
+#include "pf_flux.cuh"
 
 namespace pf {
 
@@ -33,10 +34,6 @@ struct RhsArgs {
     T mu, rho, dxi, dyi, dzi;
 };
 
-template <typename T>
-__device__ inline T edge4(T a, T b, T c, T d) {
-    return T(0.25) * (((a + b) + c) + d);
-}
 
 // Neighbourhood of cell (i, j, k) read from global memory (any viscosity /
 // SFS configuration): wrapped plane / row / column offsets of the neighbours
@@ -68,182 +65,6 @@ struct GatherSrc {
         return __ldg(a->sfs + (long long)c * n + off(di, dj, dk));
     }
 };
-
-// The six x-face terms of a cell that the cell at i+1 reuses as its x-minus
-// terms: the viscous fluxes fxx (centre), fxy, fxz (x-edges) and the
-// convective products u u, v u, w u on the x-plus side.  Each is the same
-// expression, with the same operands in the same order, as the x-minus term
-// of the next cell, so reusing it changes no rounding.
-template <typename T>
-struct XFace {
-    T fxx, fxy, fxz, cuu, cvu, cwu;
-};
-
-// Computes (ru, rv, rw) of one cell from its neighbourhood S (velocity at
-// offsets -1..1, viscosity / SFS stresses at offsets -2..0 when present).
-// With CARRY, the x-minus terms come from *xin (the x-plus terms of the cell
-// at i-1: constant viscosity, no SFS stresses) and the velocity at i-1 is not
-// read; *xout, when given, receives this cell's x-plus terms.
-template <typename T, bool CARRY = false, class Src>
-__device__ inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
-                                bool has_visc, bool has_sfs, T& ru_o, T& rv_o, T& rw_o,
-                                const XFace<T>* xin = nullptr, XFace<T>* xout = nullptr) {
-    auto LV = [&](int di, int dj, int dk) -> T { return has_visc ? S.visc(di, dj, dk) : mu; };
-    auto LS = [&](int c, int di, int dj, int dk) -> T { return S.sfs(c, di, dj, dk); };
-    // velocity neighbourhood
-    // (the x-minus neighbours are read only without CARRY)
-    const T u_c = S.u(0, 0, 0), u_xp = S.u(1, 0, 0), u_xm = CARRY ? T(0) : S.u(-1, 0, 0);
-    const T u_yp = S.u(0, 1, 0), u_ym = S.u(0, -1, 0), u_zp = S.u(0, 0, 1);
-    const T u_zm = S.u(0, 0, -1), u_xm_yp = CARRY ? T(0) : S.u(-1, 1, 0), u_xp_ym = S.u(1, -1, 0);
-    const T u_xm_zp = CARRY ? T(0) : S.u(-1, 0, 1), u_xp_zm = S.u(1, 0, -1);
-    const T v_c = S.v(0, 0, 0), v_xp = S.v(1, 0, 0), v_xm = CARRY ? T(0) : S.v(-1, 0, 0);
-    const T v_yp = S.v(0, 1, 0), v_ym = S.v(0, -1, 0), v_zp = S.v(0, 0, 1);
-    const T v_zm = S.v(0, 0, -1), v_xm_yp = CARRY ? T(0) : S.v(-1, 1, 0), v_xp_ym = S.v(1, -1, 0);
-    const T v_ym_zp = S.v(0, -1, 1), v_yp_zm = S.v(0, 1, -1);
-    const T w_c = S.w(0, 0, 0), w_xp = S.w(1, 0, 0), w_xm = CARRY ? T(0) : S.w(-1, 0, 0);
-    const T w_yp = S.w(0, 1, 0), w_ym = S.w(0, -1, 0), w_zp = S.w(0, 0, 1);
-    const T w_zm = S.w(0, 0, -1), w_xm_zp = CARRY ? T(0) : S.w(-1, 0, 1), w_xp_zm = S.w(1, 0, -1);
-    const T w_ym_zp = S.w(0, -1, 1), w_yp_zm = S.w(0, 1, -1);
-
-    // FP64 keeps the reference's divisions (bit-exact parity); the FP32 stage
-    // of the mixed forms multiplies by the reciprocals instead (one rounding
-    // more, no IEEE division sequence per use)
-    constexpr bool f32 = sizeof(T) == 4;
-    const T irho = T(1) / rho;
-    auto over_rho = [&](T a) -> T { if constexpr (f32) return a * irho; else return a / rho; };
-    // divergence / 3 at centres (div_vel_over, metric_staggered.py:424-433)
-    auto div3 = [&](T ue, T uw, T vn, T vs, T wt, T wb) -> T {
-        const T s = (((ue - uw) * dxi) + ((vn - vs) * dyi)) + ((wt - wb) * dzi);
-        if constexpr (f32) return s * T(1.0f / 3.0f); else return s / T(3.0);
-    };
-    const T D_c = div3(u_xp, u_c, v_yp, v_c, w_zp, w_c);
-    const T D_xm = CARRY ? T(0) : div3(u_c, u_xm, v_xm_yp, v_xm, w_xm_zp, w_xm);
-    const T D_ym = div3(u_xp_ym, u_ym, v_c, v_ym, w_ym_zp, w_ym);
-    const T D_zm = div3(u_xp_zm, u_zm, v_yp_zm, v_zm, w_c, w_zm);
-
-    const T two = T(2.0);
-    // diagonal viscous fluxes at centres
-    const T fxx_c = ((u_xp - u_c) * dxi - D_c) * over_rho(two * LV(0, 0, 0));
-    const T fxx_m = CARRY ? xin->fxx : ((u_c - u_xm) * dxi - D_xm) * over_rho(two * LV(-1, 0, 0));
-    const T fyy_c = ((v_yp - v_c) * dyi - D_c) * over_rho(two * LV(0, 0, 0));
-    const T fyy_m = ((v_c - v_ym) * dyi - D_ym) * over_rho(two * LV(0, -1, 0));
-    const T fzz_c = ((w_zp - w_c) * dzi - D_c) * over_rho(two * LV(0, 0, 0));
-    const T fzz_m = ((w_c - w_zm) * dzi - D_zm) * over_rho(two * LV(0, 0, -1));
-
-    // edge viscosities (one cell below the flux, as in the reference)
-    T vxy_c, vxy_ym, vxy_xm, vxz_c, vxz_zm, vxz_xm, vyz_c, vyz_zm, vyz_ym;
-    if (has_visc) {
-        vxy_c = edge4(LV(0, 0, 0), LV(-1, 0, 0), LV(0, -1, 0), LV(-1, -1, 0));
-        vxy_ym = edge4(LV(0, -1, 0), LV(-1, -1, 0), LV(0, -2, 0), LV(-1, -2, 0));
-        vxy_xm = edge4(LV(-1, 0, 0), LV(-2, 0, 0), LV(-1, -1, 0), LV(-2, -1, 0));
-        vxz_c = edge4(LV(0, 0, 0), LV(-1, 0, 0), LV(0, 0, -1), LV(-1, 0, -1));
-        vxz_zm = edge4(LV(0, 0, -1), LV(-1, 0, -1), LV(0, 0, -2), LV(-1, 0, -2));
-        vxz_xm = edge4(LV(-1, 0, 0), LV(-2, 0, 0), LV(-1, 0, -1), LV(-2, 0, -1));
-        vyz_c = edge4(LV(0, 0, 0), LV(0, -1, 0), LV(0, 0, -1), LV(0, -1, -1));
-        vyz_zm = edge4(LV(0, 0, -1), LV(0, -1, -1), LV(0, 0, -2), LV(0, -1, -2));
-        vyz_ym = edge4(LV(0, -1, 0), LV(0, -2, 0), LV(0, -1, -1), LV(0, -2, -1));
-    } else {
-        const T m = mu;
-        const T e = edge4(m, m, m, m);
-        vxy_c = vxy_ym = vxy_xm = vxz_c = vxz_zm = vxz_xm = vyz_c = vyz_zm = vyz_ym = e;
-    }
-    // off-diagonal viscous fluxes on edges: (grad_y u + grad_x v) * (Vxy / rho)
-    const T fxy_c = (((u_yp - u_c) * dyi) + ((v_xp - v_c) * dxi)) * over_rho(vxy_c);
-    const T fxy_ym = (((u_c - u_ym) * dyi) + ((v_xp_ym - v_ym) * dxi)) * over_rho(vxy_ym);
-    const T fxy_xm = CARRY ? xin->fxy
-                           : (((u_xm_yp - u_xm) * dyi) + ((v_c - v_xm) * dxi)) * over_rho(vxy_xm);
-    const T fxz_c = (((u_zp - u_c) * dzi) + ((w_xp - w_c) * dxi)) * over_rho(vxz_c);
-    const T fxz_zm = (((u_c - u_zm) * dzi) + ((w_xp_zm - w_zm) * dxi)) * over_rho(vxz_zm);
-    const T fxz_xm = CARRY ? xin->fxz
-                           : (((u_xm_zp - u_xm) * dzi) + ((w_c - w_xm) * dxi)) * over_rho(vxz_xm);
-    const T fyz_c = (((v_zp - v_c) * dzi) + ((w_yp - w_c) * dyi)) * over_rho(vyz_c);
-    const T fyz_zm = (((v_c - v_zm) * dzi) + ((w_yp_zm - w_zm) * dyi)) * over_rho(vyz_zm);
-    const T fyz_ym = (((v_ym_zp - v_ym) * dzi) + ((w_c - w_ym) * dyi)) * over_rho(vyz_ym);
-
-    T ux_p = fxx_c, ux_m = fxx_m, uy_p = fxy_c, uy_m = fxy_ym, uz_p = fxz_c, uz_m = fxz_zm;
-    T vx_p = fxy_c, vx_m = fxy_xm, vy_p = fyy_c, vy_m = fyy_m, vz_p = fyz_c, vz_m = fyz_zm;
-    T wx_p = fxz_c, wx_m = fxz_xm, wy_p = fyz_c, wy_m = fyz_ym, wz_p = fzz_c, wz_m = fzz_m;
-    if (has_sfs) {
-        // 'tensor' SFS stresses, off-diagonals edge-averaged (interp_sc_xy/xz/yz)
-        const T sxy_c = edge4(LS(3, 0, 0, 0), LS(3, -1, 0, 0), LS(3, 0, -1, 0), LS(3, -1, -1, 0));
-        const T sxy_ym = edge4(LS(3, 0, -1, 0), LS(3, -1, -1, 0), LS(3, 0, -2, 0), LS(3, -1, -2, 0));
-        const T sxy_xm = edge4(LS(3, -1, 0, 0), LS(3, -2, 0, 0), LS(3, -1, -1, 0), LS(3, -2, -1, 0));
-        const T sxz_c = edge4(LS(4, 0, 0, 0), LS(4, -1, 0, 0), LS(4, 0, 0, -1), LS(4, -1, 0, -1));
-        const T sxz_zm = edge4(LS(4, 0, 0, -1), LS(4, -1, 0, -1), LS(4, 0, 0, -2), LS(4, -1, 0, -2));
-        const T sxz_xm = edge4(LS(4, -1, 0, 0), LS(4, -2, 0, 0), LS(4, -1, 0, -1), LS(4, -2, 0, -1));
-        const T syz_c = edge4(LS(5, 0, 0, 0), LS(5, 0, -1, 0), LS(5, 0, 0, -1), LS(5, 0, -1, -1));
-        const T syz_zm = edge4(LS(5, 0, 0, -1), LS(5, 0, -1, -1), LS(5, 0, 0, -2), LS(5, 0, -1, -2));
-        const T syz_ym = edge4(LS(5, 0, -1, 0), LS(5, 0, -2, 0), LS(5, 0, -1, -1), LS(5, 0, -2, -1));
-        ux_p += LS(0, 0, 0, 0); ux_m += LS(0, -1, 0, 0);
-        uy_p += sxy_c;          uy_m += sxy_ym;
-        uz_p += sxz_c;          uz_m += sxz_zm;
-        vx_p += sxy_c;          vx_m += sxy_xm;
-        vy_p += LS(1, 0, 0, 0); vy_m += LS(1, 0, -1, 0);
-        vz_p += syz_c;          vz_m += syz_zm;
-        wx_p += sxz_c;          wx_m += sxz_xm;
-        wy_p += syz_c;          wy_m += syz_ym;
-        wz_p += LS(2, 0, 0, 0); wz_m += LS(2, 0, 0, -1);
-    }
-    // div_visc (metric_staggered.py:406-418): rhs.add_(dxi, F) is one fma
-    T ru = T(0), rv = T(0), rw = T(0);
-    ru = fma(dxi, ux_p, ru); ru = fma(-dxi, ux_m, ru);
-    ru = fma(dyi, uy_p, ru); ru = fma(-dyi, uy_m, ru);
-    ru = fma(dzi, uz_p, ru); ru = fma(-dzi, uz_m, ru);
-    rv = fma(dxi, vx_p, rv); rv = fma(-dxi, vx_m, rv);
-    rv = fma(dyi, vy_p, rv); rv = fma(-dyi, vy_m, rv);
-    rv = fma(dzi, vz_p, rv); rv = fma(-dzi, vz_m, rv);
-    rw = fma(dxi, wx_p, rw); rw = fma(-dxi, wx_m, rw);
-    rw = fma(dyi, wy_p, rw); rw = fma(-dyi, wy_m, rw);
-    rw = fma(dzi, wz_p, rw); rw = fma(-dzi, wz_m, rw);
-
-    // convective fluxes (vel_conv_*, metric_staggered.py:458-526)
-    const T h = T(0.5), one = T(1.0);
-    T cuu_p, cvu_p, cwu_p;  // this cell's x-plus convective products
-    {
-        const T cp = h * (u_xp + u_c);
-        cuu_p = cp * cp;
-        T cmm;
-        if constexpr (CARRY) cmm = xin->cuu;
-        else { const T cm = h * (u_c + u_xm); cmm = cm * cm; }
-        ru -= (cuu_p - cmm) * dxi * one;
-        const T uyp = h * (u_yp + u_c), uym = h * (u_c + u_ym);
-        const T vxp = h * (v_yp + v_xm_yp), vxm = h * (v_c + v_xm);
-        ru -= (uyp * vxp - uym * vxm) * dyi * one;
-        const T uzp = h * (u_zp + u_c), uzm = h * (u_c + u_zm);
-        const T wxp = h * (w_zp + w_xm_zp), wxm = h * (w_c + w_xm);
-        ru -= (uzp * wxp - uzm * wxm) * dzi * one;
-    }
-    {
-        const T vxp = h * (v_xp + v_c);
-        const T uyp = h * (u_xp + u_xp_ym);
-        cvu_p = vxp * uyp;
-        T mm;
-        if constexpr (CARRY) mm = xin->cvu;
-        else { const T vxm = h * (v_c + v_xm), uym = h * (u_c + u_ym); mm = vxm * uym; }
-        rv -= (cvu_p - mm) * dxi * one;
-        const T cp = h * (v_yp + v_c), cm = h * (v_c + v_ym);
-        rv -= (cp * cp - cm * cm) * dyi * one;
-        const T vzp = h * (v_zp + v_c), vzm = h * (v_c + v_zm);
-        const T wyp = h * (w_zp + w_ym_zp), wym = h * (w_c + w_ym);
-        rv -= (vzp * wyp - vzm * wym) * dzi * one;
-    }
-    {
-        const T wxp = h * (w_xp + w_c);
-        const T uzp = h * (u_xp + u_xp_zm);
-        cwu_p = wxp * uzp;
-        T mm;
-        if constexpr (CARRY) mm = xin->cwu;
-        else { const T wxm = h * (w_c + w_xm), uzm = h * (u_c + u_zm); mm = wxm * uzm; }
-        rw -= (cwu_p - mm) * dxi * one;
-        const T wyp = h * (w_yp + w_c), wym = h * (w_c + w_ym);
-        const T vzp = h * (v_yp + v_yp_zm), vzm = h * (v_c + v_zm);
-        rw -= (wyp * vzp - wym * vzm) * dyi * one;
-        const T cp = h * (w_zp + w_c), cm = h * (w_c + w_zm);
-        rw -= (cp * cp - cm * cm) * dzi * one;
-    }
-    ru_o = ru; rv_o = rv; rw_o = rw;
-    if (xout) *xout = XFace<T>{fxx_c, fxy_c, fxz_c, cuu_p, cvu_p, cwu_p};
-}
 
 template <typename T, typename TI>
 __device__ inline void rhs_cell(const Dims& d, const RhsArgs<T, TI>& a, int i, int j, int k,
@@ -638,13 +459,13 @@ rhs_stage_tiled(Dims d, Tiling tl, RhsArgs<T, TI> a, double* __restrict__ u,
 }
 
 // Grouped stage: one launch advances the same RK4 stage of several
-// independent solves (a batch of requests, any grid sizes).  jobs.j[r] holds
-// request r's grid, tiling, stage arguments and the index of its first tile
-// in the batch's tile space; a block walks the batch's tiles (persistent
-// loop) and runs each with its request's arguments, so every tile computes
-// exactly what the single-request launch computes.  The job table is a
-// by-value kernel parameter (it lives in the constant bank, read with a
-// block-uniform index like the single launch's parameters).
+// independent solves (a batch of requests, any grid sizes).  jobs[r] (device
+// memory) holds request r's grid, tiling, stage arguments and the index of
+// its first tile in the batch's tile space; a block walks the batch's tiles
+// (persistent loop), stages the tile's job in shared memory and runs the
+// tile with it, so every tile computes exactly what the single-request
+// launch computes.  A tile index outside every job's range (a table that does
+// not match the launch) is skipped and recorded in *err.
 template <typename T, typename TI>
 struct StageJob {
     Dims d;
@@ -658,25 +479,38 @@ struct StageJob {
 
 constexpr int kMaxGroupJobs = kMaxBatch;
 
-template <typename T, typename TI>
-struct StageJobs {
-    StageJob<T, TI> j[kMaxGroupJobs];
-};
-static_assert(sizeof(StageJobs<double, double>) + 16 <= 32764,
-              "the job table must fit the kernel parameter space");
-
 template <typename T, typename TI, int MODE>
 __global__ void __launch_bounds__(256, 2)
-rhs_stage_grouped(const __grid_constant__ StageJobs<T, TI> jobs, int njobs, long long ntiles) {
+rhs_stage_grouped(const StageJob<T, TI>* __restrict__ jobs, int njobs, long long ntiles,
+                  int* __restrict__ err) {
+    __shared__ long long first[kMaxGroupJobs];
+    __shared__ StageJob<T, TI> J;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    njobs = min(njobs, kMaxGroupJobs);
+    for (int r = tid; r < njobs; r += 256) first[r] = jobs[r].tile0;
+    __syncthreads();
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         int lo = 0, hi = njobs - 1;  // last job whose first tile is <= t
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (jobs.j[mid].tile0 <= t) lo = mid; else hi = mid - 1;
+            if (first[mid] <= t) lo = mid; else hi = mid - 1;
         }
-        const StageJob<T, TI>& J = jobs.j[lo];
+        // the previous tile is done with J (each tile ends at a barrier)
+        __syncthreads();
+        {
+            static_assert(sizeof(StageJob<T, TI>) % 8 == 0, "job copied in 8-byte words");
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(jobs + lo);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&J);
+            for (int q = tid; q < (int)(sizeof(StageJob<T, TI>) / 8); q += 256) dst[q] = src[q];
+        }
+        __syncthreads();
+        const long long local = t - J.tile0;
+        if (local < 0 || local >= J.tl.ntiles) {
+            if (tid == 0) atomicExch(err, 1);
+            continue;
+        }
         stage_tile<T, TI, T, T, MODE>(J.d, J.tl, J.a, J.u, J.v, J.w, J.su, J.sv, J.sw, J.au,
-                                      J.av, J.aw, J.hdt, J.c6, t - J.tile0);
+                                      J.av, J.aw, J.hdt, J.c6, local);
     }
 }
 
@@ -882,36 +716,88 @@ int grouped_predictor_prepare(int prec) {
     return PF_OK;
 }
 
+// Table layout: [error flag, 256 B][stage 0 jobs][stage 1][stage 2][stage 3],
+// each stage's slot of `count` jobs 256-byte aligned.
+static size_t job_slot_bytes(int count) {
+    const size_t j = std::max(std::max(sizeof(StageJob<double, double>),
+                                       sizeof(StageJob<float, double>)),
+                              sizeof(StageJob<float, float>));
+    return ((size_t)std::max(count, 1) * j + 255) & ~size_t(255);
+}
+
+size_t grouped_predictor_table_bytes(int count) { return 256 + 4 * job_slot_bytes(count); }
+
 template <typename T>
-static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, cudaStream_t s) {
-    if (count < 1 || count > kMaxGroupJobs) return cudaErrorInvalidValue;
-    // the stage tables (built on the host, passed by value)
-    auto* J0 = new StageJobs<T, double>();
-    auto* J1 = new StageJobs<T, T>();
-    auto* J2 = new StageJobs<T, T>();
-    auto* J3 = new StageJobs<T, T>();
+static long long group_tiles(const GroupMember* m, int count) {
+    long long tiles = 0;
+    for (int r = 0; r < count; ++r) {
+        Dims d{m[r].grid.nx, m[r].grid.ny, m[r].grid.nz,
+               (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz};
+        tiles += make_tiling(d, kRhsTY).ntiles;
+    }
+    return tiles;
+}
+
+template <typename T>
+static int tables_impl(int rk4, const GroupMember* m, int count, void* table, cudaStream_t s) {
+    const size_t slot = job_slot_bytes(count);
+    std::vector<unsigned char> host(grouped_predictor_table_bytes(count), 0);
+    unsigned char* st0 = host.data() + 256;
     long long tiles = 0;
     for (int r = 0; r < count; ++r) {
         const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
         T* ws = (T*)m[r].R;
         T *sa = ws, *sb = ws + 3 * n, *acc = ws + 6 * n;
         if (!rk4) {
-            J0->j[r] = make_job<T, double>(m[r], m[r].u, nullptr, acc, tiles);
+            auto J = make_job<T, double>(m[r], m[r].u, nullptr, acc, tiles);
+            std::memcpy(st0 + r * sizeof(J), &J, sizeof(J));
+            tiles += J.tl.ntiles;
         } else {
-            J0->j[r] = make_job<T, double>(m[r], m[r].u, sa, acc, tiles);
-            J1->j[r] = make_job<T, T>(m[r], sa, sb, acc, tiles);
-            J2->j[r] = make_job<T, T>(m[r], sb, sa, acc, tiles);
-            J3->j[r] = make_job<T, T>(m[r], sa, nullptr, acc, tiles);
+            auto J0 = make_job<T, double>(m[r], m[r].u, sa, acc, tiles);
+            auto J1 = make_job<T, T>(m[r], sa, sb, acc, tiles);
+            auto J2 = make_job<T, T>(m[r], sb, sa, acc, tiles);
+            auto J3 = make_job<T, T>(m[r], sa, nullptr, acc, tiles);
+            std::memcpy(st0 + 0 * slot + r * sizeof(J0), &J0, sizeof(J0));
+            std::memcpy(st0 + 1 * slot + r * sizeof(J1), &J1, sizeof(J1));
+            std::memcpy(st0 + 2 * slot + r * sizeof(J2), &J2, sizeof(J2));
+            std::memcpy(st0 + 3 * slot + r * sizeof(J3), &J3, sizeof(J3));
+            tiles += J0.tl.ntiles;
         }
-        tiles += J0->j[r].tl.ntiles;
     }
+    if (tiles != group_tiles<T>(m, count)) return PF_ERR_BAD_ARG;
+    if (cudaMemcpyAsync(table, host.data(), host.size(), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return PF_ERR_CUDA;
+    return PF_OK;
+}
+
+int grouped_predictor_tables(int prec, int rk4, const GroupMember* m, int count, void* table,
+                             cudaStream_t s) {
+    if (count < 1 || count > kMaxGroupJobs || !table) return PF_ERR_BAD_ARG;
+    int rc = grouped_predictor_prepare(prec);
+    if (rc != PF_OK) return rc;
+    return prec == PF_FP64 ? tables_impl<double>(rk4, m, count, table, s)
+                           : tables_impl<float>(rk4, m, count, table, s);
+}
+
+template <typename T>
+static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, void* table,
+                                cudaStream_t s) {
+    if (count < 1 || count > kMaxGroupJobs) return cudaErrorInvalidValue;
+    const size_t slot = job_slot_bytes(count);
+    char* tb = (char*)table;
+    int* err = (int*)tb;
+    char* st0 = tb + 256;
+    const long long tiles = group_tiles<T>(m, count);
     const int grid = (int)std::min<long long>(tiles, num_sms() * 2);
     const dim3 blk(32, 8);
     const bool f64 = sizeof(T) == 8;
     if (!rk4) {
         PF_LAUNCH(f64 ? "grouped_euler_f64" : "grouped_euler_f32", s,
                   (rhs_stage_grouped<T, double, kModeK><<<grid, blk,
-                      RhsSmem<T, double, T, kModeK>::bytes, s>>>(*J0, count, tiles)));
+                      RhsSmem<T, double, T, kModeK>::bytes, s>>>(
+                      (const StageJob<T, double>*)st0, count, tiles, err)));
         for (int r = 0; r < count; ++r) {
             const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
             const T* acc = (const T*)m[r].R + 6 * n;
@@ -919,28 +805,29 @@ static cudaError_t grouped_impl(int rk4, const GroupMember* m, int count, cudaSt
             PF_LAUNCH("euler_apply", s, euler_apply<T><<<gp, 256, 0, s>>>(
                 n, acc, acc + n, acc + 2 * n, m[r].dt, m[r].u, m[r].v, m[r].w));
         }
-    } else {
-        PF_LAUNCH(f64 ? "grouped_first_f64" : "grouped_first_f32", s,
-                  (rhs_stage_grouped<T, double, kModeFirst><<<grid, blk,
-                      RhsSmem<T, double, T, kModeFirst>::bytes, s>>>(*J0, count, tiles)));
-        PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
-                  (rhs_stage_grouped<T, T, kModeMid><<<grid, blk,
-                      RhsSmem<T, T, T, kModeMid>::bytes, s>>>(*J1, count, tiles)));
-        PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
-                  (rhs_stage_grouped<T, T, kModeMid><<<grid, blk,
-                      RhsSmem<T, T, T, kModeMid>::bytes, s>>>(*J2, count, tiles)));
-        PF_LAUNCH(f64 ? "grouped_last_f64" : "grouped_last_f32", s,
-                  (rhs_stage_grouped<T, T, kModeLast><<<grid, blk,
-                      RhsSmem<T, T, T, kModeLast>::bytes, s>>>(*J3, count, tiles)));
+        return cudaGetLastError();
     }
-    delete J0; delete J1; delete J2; delete J3;
+    PF_LAUNCH(f64 ? "grouped_first_f64" : "grouped_first_f32", s,
+              (rhs_stage_grouped<T, double, kModeFirst><<<grid, blk,
+                  RhsSmem<T, double, T, kModeFirst>::bytes, s>>>(
+                  (const StageJob<T, double>*)st0, count, tiles, err)));
+    PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
+              (rhs_stage_grouped<T, T, kModeMid><<<grid, blk, RhsSmem<T, T, T, kModeMid>::bytes,
+                  s>>>((const StageJob<T, T>*)(st0 + slot), count, tiles, err)));
+    PF_LAUNCH(f64 ? "grouped_mid_f64" : "grouped_mid_f32", s,
+              (rhs_stage_grouped<T, T, kModeMid><<<grid, blk, RhsSmem<T, T, T, kModeMid>::bytes,
+                  s>>>((const StageJob<T, T>*)(st0 + 2 * slot), count, tiles, err)));
+    PF_LAUNCH(f64 ? "grouped_last_f64" : "grouped_last_f32", s,
+              (rhs_stage_grouped<T, T, kModeLast><<<grid, blk,
+                  RhsSmem<T, T, T, kModeLast>::bytes, s>>>(
+                  (const StageJob<T, T>*)(st0 + 3 * slot), count, tiles, err)));
     return cudaGetLastError();
 }
 
 cudaError_t launch_grouped_predictor(int prec, int rk4, const GroupMember* m, int count,
-                                     cudaStream_t s) {
-    return prec == PF_FP64 ? grouped_impl<double>(rk4, m, count, s)
-                           : grouped_impl<float>(rk4, m, count, s);
+                                     void* table, cudaStream_t s) {
+    return prec == PF_FP64 ? grouped_impl<double>(rk4, m, count, table, s)
+                           : grouped_impl<float>(rk4, m, count, table, s);
 }
 
 cudaError_t predictor_prepare(int prec) {

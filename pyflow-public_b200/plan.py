@@ -35,8 +35,11 @@ class BatchMember(ctypes.Structure):
         ("ws_bytes", ctypes.c_size_t), ("stats", ctypes.c_void_p)]
 
 
+_lib.pf_batch_table_bytes.argtypes = [ctypes.c_int]
+_lib.pf_batch_table_bytes.restype = ctypes.c_size_t
 _lib.pf_batch_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(BatchMember),
-                                      ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.POINTER(ctypes.c_void_p)]
 _lib.pf_batch_plan_create.restype = ctypes.c_int
 MAX_BATCH = 64
 
@@ -135,10 +138,14 @@ class BatchPlan:
             raise ValueError("all members of a batch use one precision form")
         self.device = members[0].ws.device
         self.members = list(members)
+        # per-member arguments of the grouped launches (first int: error flag)
+        self.table = torch.empty(_lib.pf_batch_table_bytes(len(members)), dtype=torch.uint8,
+                                 device=self.device)
         arr = (BatchMember * len(members))(*(m.c_struct() for m in members))
         self._h = ctypes.c_void_p(0)
         L.check("pf_batch_plan_create", _lib.pf_batch_plan_create(
-            ops.PREC[prec], 1 if rk4 else 0, arr, len(members), ctypes.byref(self._h)))
+            ops.PREC[prec], 1 if rk4 else 0, arr, len(members), ops._p(self.table),
+            self.table.numel(), ctypes.byref(self._h)))
         for m in members:
             m.fresh = False
 
@@ -146,6 +153,10 @@ class BatchPlan:
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         L.check("pf_step_plan_launch", _lib.pf_step_plan_launch(
             self._h, int(nsteps), ctypes.c_void_p(s.cuda_stream)))
+
+    def error(self):
+        """True if a grouped launch found a tile outside every member's range."""
+        return bool(self.table[:4].view(torch.int32).item())
 
     def close(self):
         if self._h and self._h.value:

@@ -2,9 +2,10 @@
 
 * a model of the same arithmetic (BF16 inputs and weights, FP32 accumulation,
   BF16 pre-activations and activations).  Tolerance: 3e-2 of the output range
-  -- the kernel's hardware tanh (tanh.approx.bf16x2) and the tensor core's
-  FP32 summation order can flip the BF16 rounding of a hidden activation,
-  which moves an output by a few BF16 ulps of its inputs;
+  at any cell and 1e-2 at 90 % of the cells -- the kernel's hardware tanh
+  (tanh.approx.bf16x2) and the tensor core's FP32 summation order can flip
+  the BF16 rounding of a hidden activation, which moves an output by a few
+  BF16 ulps of its inputs;
 * the FP64 model (the network with the same BF16-valued weights evaluated in
   FP64 without roundings): the closure's error against exact arithmetic.
   Tolerance: 5e-2 of the output range at any cell, 1.5e-2 in RMS.
@@ -39,8 +40,10 @@ def test_mlp_closure_matches_bf16_model(shape):
     assert scale > 0
     err_max = (got - ref).abs().max().item()
     assert err_max <= 3e-2 * scale, (err_max, scale)
-    # most cells agree to FP32 accumulation order
-    close = ((got - ref).abs() <= 1e-4 * scale).double().mean().item()
+    # most cells agree to about one BF16 ulp of the hidden activations: the
+    # hardware's packed BF16 tanh and torch's tanh rounded to BF16 differ by
+    # one ulp on a fraction of the activations
+    close = ((got - ref).abs() <= 1e-2 * scale).double().mean().item()
     assert close > 0.9, close
 
 
