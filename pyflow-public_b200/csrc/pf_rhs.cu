@@ -681,14 +681,14 @@ static cudaError_t grouped_prepare() {
 // Job of one request for one stage (the arguments the single-request
 // predictor_impl passes to that stage).
 template <typename T, typename TI>
-static StageJob<T, TI> make_job(const GroupMember& m, const TI* in, T* st, T* acc,
-                                long long tile0) {
+static StageJob<T, TI> make_job(const GroupMember& m, const TI* in_u, const TI* in_v,
+                                const TI* in_w, T* st, T* acc, long long tile0) {
     StageJob<T, TI> J;
     const pf_grid* g = &m.grid;
     J.d = Dims{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     J.tl = make_tiling(J.d, kRhsTY);
     const long long n = J.d.n;
-    J.a = make_args<T, TI>(g, in, in + n, in + 2 * n, nullptr, nullptr, m.mu, m.rho);
+    J.a = make_args<T, TI>(g, in_u, in_v, in_w, nullptr, nullptr, m.mu, m.rho);
     J.u = m.u; J.v = m.v; J.w = m.w;
     J.su = st; J.sv = st ? st + n : nullptr; J.sw = st ? st + 2 * n : nullptr;
     J.au = acc; J.av = acc + n; J.aw = acc + 2 * n;
@@ -748,15 +748,17 @@ static int tables_impl(int rk4, const GroupMember* m, int count, void* table, cu
         const long long n = (long long)m[r].grid.nx * m[r].grid.ny * m[r].grid.nz;
         T* ws = (T*)m[r].R;
         T *sa = ws, *sb = ws + 3 * n, *acc = ws + 6 * n;
+        // the first stage (and Euler's k) reads the FP64 state u, v, w -- three
+        // separate fields; later stages read a stage state, 3 consecutive fields
         if (!rk4) {
-            auto J = make_job<T, double>(m[r], m[r].u, nullptr, acc, tiles);
+            auto J = make_job<T, double>(m[r], m[r].u, m[r].v, m[r].w, nullptr, acc, tiles);
             std::memcpy(st0 + r * sizeof(J), &J, sizeof(J));
             tiles += J.tl.ntiles;
         } else {
-            auto J0 = make_job<T, double>(m[r], m[r].u, sa, acc, tiles);
-            auto J1 = make_job<T, T>(m[r], sa, sb, acc, tiles);
-            auto J2 = make_job<T, T>(m[r], sb, sa, acc, tiles);
-            auto J3 = make_job<T, T>(m[r], sa, nullptr, acc, tiles);
+            auto J0 = make_job<T, double>(m[r], m[r].u, m[r].v, m[r].w, sa, acc, tiles);
+            auto J1 = make_job<T, T>(m[r], sa, sa + n, sa + 2 * n, sb, acc, tiles);
+            auto J2 = make_job<T, T>(m[r], sb, sb + n, sb + 2 * n, sa, acc, tiles);
+            auto J3 = make_job<T, T>(m[r], sa, sa + n, sa + 2 * n, nullptr, acc, tiles);
             std::memcpy(st0 + 0 * slot + r * sizeof(J0), &J0, sizeof(J0));
             std::memcpy(st0 + 1 * slot + r * sizeof(J1), &J1, sizeof(J1));
             std::memcpy(st0 + 2 * slot + r * sizeof(J2), &J2, sizeof(J2));
