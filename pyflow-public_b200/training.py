@@ -151,7 +151,10 @@ class LESConfig:
     urms: float = 1.0
     dns_seed: int = 2
     mlp_seed: int = 1
-    lr: float = 1e-3
+    # RMSprop's first steps move every weight by about 10 lr: 1e-4 keeps the
+    # closure's stresses (scaled by Delta^2 <|grad u|^2>) small against the
+    # viscous terms at nu = 0.001
+    lr: float = 1e-4
     tol: float = 1e-12
     dns_prec: str = "fp64"
 
@@ -214,12 +217,16 @@ class Trainer:
         return total / cfg.steps
 
     def step(self):
+        """One window: forward, backward, update.  A window whose loss is not
+        finite (an LES that blew up) updates nothing and reports its loss."""
         self.opt.zero_grad(set_to_none=True)
         L = self.loss()
-        L.backward()
-        self.opt.step()
-        self.history.append(float(L.detach()))
-        return self.history[-1]
+        val = float(L.detach())
+        if math.isfinite(val):
+            L.backward()
+            self.opt.step()
+        self.history.append(val)
+        return val
 
     def state_dict(self):
         return {k: t.detach().cpu().numpy() for k, t in zip(PARAM_NAMES, self.params)}
