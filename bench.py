@@ -74,9 +74,10 @@ TOL = 1e-10
 MAX_IT = 20000
 SOLVER = {
     "mixed_mg": "bicgstab right-preconditioned by an fp32 multigrid V(2,2) cycle, "
-                "inside fp64 iterative refinement",
-    "mixed": "fp32 bicgstab inside fp64 iterative refinement",
-    "fp64": "bicgstab (fp64, the reference's algorithm)",
+                "inside fp64 iterative refinement started from the previous step's DP",
+    "mixed": "fp32 bicgstab inside fp64 iterative refinement started from the previous "
+             "step's DP",
+    "fp64": "bicgstab (fp64, the reference's algorithm, DP = 0 at every solve)",
 }
 
 

@@ -221,7 +221,11 @@ int pf_bicgstab_solve_noalloc(const pf_grid* g, double rho, double dt,
  * every step, and accumulates the iterations and the step count in
  * stats[8], stats[9].  The workspace (pf_step_plan_workspace_bytes, 256-byte aligned)
  * belongs to the plan.  Plans of different fields may run concurrently on
- * different streams. */
+ * different streams.  PF_FP64 solves from DP = 0 like the reference
+ * (src/solver/pressure.py:202); the mixed forms start each solve from the DP
+ * that the previous step left (so DP must hold finite values -- zeros --
+ * before the first launch) and stop on the reference's criterion applied to
+ * the true residual, max|b - A DP| <= min_res max|b|. */
 typedef struct pf_step_plan pf_step_plan;
 size_t pf_step_plan_workspace_bytes(const pf_grid* g, int prec);
 int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u,

@@ -284,7 +284,8 @@ bicg_b(Dims d, Tiling tl, LapCoef<T> cf, BicgScalars* sc, double* part,
 }
 
 // ------------------------------------------------ mixed-precision refinement
-// b = (source*rho/dt)*(-vol) in FP64, DP = 0, max|b|.
+// b = (source*rho/dt)*(-vol) in FP64, max|b|; DP = 0 unless x is null (a
+// solve that starts from the DP it is given).
 __global__ void __launch_bounds__(kBlock)
 mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
              double c1, double c2, double* b, double* x, double* r_copy) {
@@ -294,7 +295,7 @@ mixed_b_init(Dims d, BicgScalars* sc, double* part, const double* src,
          q += (long long)gridDim.x * blockDim.x) {
         const double r = (src[q] * c1) * c2;
         b[q] = r;
-        x[q] = 0.0;
+        if (x) x[q] = 0.0;
         if (r_copy) r_copy[q] = r;
         m = nanmax(m, fabs(r));
     }
@@ -1051,7 +1052,13 @@ static int add_solve_chain(cudaGraph_t G, cudaGraphNode_t dep, const pf_grid* g,
                                                        max_it, min_res);
         bicg_ca<double><<<tiled_grid(ta), blk2, 0, cs>>>(d, ta, cf, sc, part, P.v64, DP);
     } else {
-        mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, P.div, c1, c2, P.bb, DP, P.rr);
+        // the refinement starts from the previous step's DP (zero before the
+        // first step): its first residual is r = b - A DP, and the stop test
+        // stays the reference's, max|b - A DP| <= min_res max|b|
+        const Tiling tld = make_tiling(d, 8 * PhaseResidual::R);
+        mixed_b_init<<<gp, kBlock, 0, cs>>>(d, sc, part, P.div, c1, c2, P.bb, nullptr, nullptr);
+        mixed_residual<<<tiled_grid(tld), blk2, 0, cs>>>(d, tld, lap_coef<double>(g), sc, part,
+                                                        P.bb, DP, P.rr);
     }
     if ((rc = capture_end(cs, &seg1))) return rc;
     cudaGraphNode_t n1, nw;
