@@ -6,18 +6,19 @@
 // accumulation; its six outputs times out_scale are the stresses FXX, FYY, FZZ,
 // FXY, FXZ, FYZ of the 'tensor' SFS slot (src/solver/velocity.py:262-267,...).
 //
-// CTAs of 128 threads (4 warps, two per SM) walk tiles of 128 consecutive
-// cells; cell m of a tile is accumulator row / TMEM lane m and belongs to
-// thread m:
-//   1. each thread computes its cell's gradients and writes 16 BF16 features
-//      (9 + 7 zero pads) into the X tile in shared memory;
+// CTAs of 256 threads (8 warps, two CTAs per SM) walk tiles of 128
+// consecutive cells; cell m of a tile is accumulator row / TMEM lane m and
+// belongs to threads m and m + 128 (the second warpgroup reads the same TMEM
+// lanes, columns 64..127):
+//   1. threads 0..127 compute their cell's gradients and write 16 BF16
+//      features (9 + 7 zero pads) into the X tile in shared memory;
 //   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
-//   3. each thread reads its D1 row from TMEM (tcgen05.ld, 64 columns per
-//      wait), adds b1, rounds pairs of pre-activations to BF16, applies the
-//      packed BF16 tanh and writes the BF16 row into the H tile;
+//   3. each thread reads its 64 columns of its D1 row from TMEM (tcgen05.ld,
+//      one wait), adds b1, rounds pairs of pre-activations to BF16, applies
+//      the packed BF16 tanh and writes them into the H tile;
 //   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
-//   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
-//      its six stresses (FP64) to global memory.
+//   5. 8 tcgen05.mma with N=16: D3 = H W3^T; threads 0..127 add b3 and
+//      write their six stresses (FP64) to global memory.
 // Completion of each MMA group is signalled by tcgen05.commit to an mbarrier;
 // every wait on it is bounded and reports a timeout through an error flag.
 //
@@ -41,6 +42,7 @@ namespace mlp {
 
 constexpr int kHidden = 128;
 constexpr int kTile = 128;
+constexpr int kThreads = 256;      // two threads per accumulator row
 constexpr int kW1Bytes = 4096;      // 128 x 16 bf16
 constexpr int kW2Bytes = 32768;     // 128 x 128 bf16
 constexpr int kW3Bytes = 4096;      // 16 x 128 bf16
@@ -252,26 +254,25 @@ __device__ inline void nb_gradients(const CellNb& nb, double dxi, double dyi, do
     }
 }
 
-// Writes 128 hidden values of this thread's row: tanh(acc + bias) as BF16.
+// Writes 64 hidden values (columns c_begin .. c_begin + 63) of this thread's
+// row: tanh(acc + bias) as BF16.
 __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bias,
-                                                uint8_t* H, int row) {
+                                                uint8_t* H, int row, int c_begin) {
+    // 32 columns per TMEM load and wait (the second warpgroup's loads and the
+    // other CTA's work cover the wait)
 #pragma unroll 1
-    for (int c0 = 0; c0 < kHidden; c0 += 64) {
-        // two 32-column loads in flight, one wait
-        uint32_t r[64];
+    for (int c0 = c_begin; c0 < c_begin + 64; c0 += 32) {
+        uint32_t r[32];
         tmem_ld32_issue(taddr + c0, r);
-        tmem_ld32_issue(taddr + c0 + 32, r + 32);
         tmem_wait_ld();
-        float v[64];
 #pragma unroll
-        for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
-#pragma unroll
-        for (int q = 0; q < 64; q += 8) {
+        for (int q = 0; q < 32; q += 8) {
             uint32_t packed[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e)
-                packed[e] = tanh_pack_bf16x2(v[q + 2 * e] + bias[c0 + q + 2 * e],
-                                             v[q + 2 * e + 1] + bias[c0 + q + 2 * e + 1]);
+                packed[e] = tanh_pack_bf16x2(__uint_as_float(r[q + 2 * e]) + bias[c0 + q + 2 * e],
+                                             __uint_as_float(r[q + 2 * e + 1]) +
+                                                 bias[c0 + q + 2 * e + 1]);
             // 8 consecutive k of one row are one 16-byte chunk
             *reinterpret_cast<uint4*>(H + kmajor_off(row, c0 + q, 4096)) =
                 make_uint4(packed[0], packed[1], packed[2], packed[3]);
@@ -282,7 +283,7 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bia
 }  // namespace mlp
 
 // scales[0] = 1/g_rms (input normalisation), scales[1] = output scale
-__global__ void __launch_bounds__(128, 2)
+__global__ void __launch_bounds__(mlp::kThreads, 2)
 mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restrict__ v,
                    const double* __restrict__ w, double dxi, double dyi, double dzi,
                    const uint8_t* __restrict__ wpack, const float* __restrict__ scales,
@@ -298,7 +299,12 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     uint64_t* bar = reinterpret_cast<uint64_t*>(sH + kHBytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
 
+    // 256 threads: thread (half, row) with row = tid % 128 owns accumulator
+    // row / TMEM lane `row` and, in the epilogues, its 64 columns
+    // half*64 .. half*64+63; the first half also computes the features and
+    // writes the outputs.  Warp w reads TMEM lanes 32 (w % 4) .. +31.
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int row = tid & (kTile - 1), half = tid >> 7;
     // weights: a straight copy of the packed image
     {
         const uint4* src = reinterpret_cast<const uint4*>(wpack);
@@ -320,22 +326,22 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     const uint32_t d1 = tmem, d2 = tmem + 128, d3 = tmem;  // column offsets
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     const float in_scale = scales[0], out_scale = scales[1];
     const uint32_t id128 = instr_desc(128, 128), id16 = instr_desc(128, 16);
     uint32_t phase = 0;
     bool ok = true;
     const long long ntiles = (d.n + kTile - 1) / kTile;
     CellNb nb;
-    {
-        const long long c0 = (long long)blockIdx.x * kTile + tid;
+    if (half == 0) {
+        const long long c0 = (long long)blockIdx.x * kTile + row;
         if (blockIdx.x < ntiles && c0 < d.n) load_nb(d, u, v, w, c0, nb);
     }
     for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const long long cell = t * kTile + tid;
+        const long long cell = t * kTile + row;
         const bool valid = cell < d.n;
-        // ---- features -> X (row tid)
-        {
+        // ---- features -> X (row `row`, first half)
+        if (half == 0) {
             double g[9];
             if (valid) nb_gradients(nb, dxi, dyi, dzi, g);
             uint32_t p[8];
@@ -346,8 +352,8 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
                 const float b = (valid && k1 < 9) ? float(g[k1]) * in_scale : 0.f;
                 p[e] = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
             }
-            *reinterpret_cast<uint4*>(sX + kmajor_off(tid, 0, 4096)) = make_uint4(p[0], p[1], p[2], p[3]);
-            *reinterpret_cast<uint4*>(sX + kmajor_off(tid, 8, 4096)) = make_uint4(p[4], p[5], p[6], p[7]);
+            *reinterpret_cast<uint4*>(sX + kmajor_off(row, 0, 4096)) = make_uint4(p[0], p[1], p[2], p[3]);
+            *reinterpret_cast<uint4*>(sX + kmajor_off(row, 8, 4096)) = make_uint4(p[4], p[5], p[6], p[7]);
         }
         fence_async_smem();
         tc_fence_before();
@@ -359,15 +365,15 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
             commit(bar);
         }
         // the next tile's neighbourhood loads run under this tile's layers
-        {
-            const long long cn = (t + gridDim.x) * kTile + tid;
+        if (half == 0) {
+            const long long cn = (t + gridDim.x) * kTile + row;
             if (t + gridDim.x < ntiles && cn < d.n) load_nb(d, u, v, w, cn, nb);
         }
         ok = __syncthreads_and(wait_phase(bar, phase));
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
-        hidden_epilogue(lane_base + d1, sB, sH, tid);
+        hidden_epilogue(lane_base + d1, sB, sH, row, half * 64);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -384,7 +390,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
-        hidden_epilogue(lane_base + d2, sB + 128, sH, tid);
+        hidden_epilogue(lane_base + d2, sB + 128, sH, row, half * 64);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -401,7 +407,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
-        {
+        if (half == 0) {
             float y[16];
             mlp::tmem_ld16(lane_base + d3, y);
             if (valid) {
@@ -461,7 +467,7 @@ cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
     // shared memory (a third would not fit in shared memory, so a TMEM
     // allocation never has to wait for another CTA of this kernel)
     const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
-    PF_LAUNCH("mlp_closure", s, mlp_closure_kernel<<<grid, 128, smem, s>>>(
+    PF_LAUNCH("mlp_closure", s, mlp_closure_kernel<<<grid, mlp::kThreads, smem, s>>>(
         d, u, v, w, 1.0 / g->dx, 1.0 / g->dy, 1.0 / g->dz, (const uint8_t*)wpack, scales,
         out, err));
     return cudaGetLastError();
