@@ -343,15 +343,16 @@ def timed_plan(torch, dev, u0, v0, w0, wl, prec, steps, warmup, barrier, world, 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if path == "host":
         import pyflow_b200.ops as ops
+        warm = prec != "fp64"   # the mixed plans' initial guess: the previous DP
         for _ in range(warmup):
             ops.forward_step(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
-                             prec=prec)
+                             prec=prec, warm=warm)
         barrier()
         its, info = 0, None
         e0.record(st)
         for _ in range(steps):
             info = ops.forward_step(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL,
-                                    max_it=MAX_IT, prec=prec)
+                                    max_it=MAX_IT, prec=prec, warm=warm)
             its += info.iterations
         e1.record(st)
         barrier()
@@ -589,13 +590,14 @@ def run_b200(a):
     prof_steps = 2
     if not a.no_extras:
         # per-kernel device time: CUDA events around each launch of the
-        # host-driven path, which runs the kernels of the captured step
+        # host-driven path, which runs the kernels of the captured step (in
+        # the mixed forms from the previous step's DP, as the plans do)
         prof.enable(True)
         f = [torch.tensor(x, device=dev) for x in (u0, v0, w0)]
         f += [torch.zeros_like(f[0]), torch.zeros_like(f[0])]
         for _ in range(prof_steps):
             ops.forward_step(*f, sp, wl["nu"], 1.0, wl["dt"], min_res=TOL, max_it=MAX_IT,
-                             prec=a.prec)
+                             prec=a.prec, warm=a.prec != "fp64")
         torch.cuda.synchronize(dev)
         ktimes = prof.read()
         prof.enable(False)

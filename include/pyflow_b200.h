@@ -51,6 +51,13 @@ enum pf_status {
 
 enum pf_prec { PF_FP64 = 0, PF_MIXED = 1, PF_MIXED_MG = 2 };
 
+/* Flag OR-ed into prec of pf_bicgstab_solve / pf_forward_step: in the mixed
+ * forms the solve starts from the DP it is given (for example the previous
+ * step's) instead of zero, as the mixed step plans do; the stop criterion is
+ * unchanged (max|b - A DP| <= min_res max|b|).  Ignored for PF_FP64, which
+ * always starts from DP = 0 like the reference. */
+enum pf_flags { PF_WARM_START = 0x100 };
+
 /* Result of a Poisson solve (host struct, filled by the synchronous calls). */
 typedef struct pf_solve_info {
     double max_res;      /* max|r| / max|r0|, the reference's return value */

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_PKG, "libpyflow_b200.so")
 PF_OK, PF_ERR_BAD_ARG, PF_ERR_CUDA, PF_BREAKDOWN, PF_MAXIT, PF_NONFINITE, \
     PF_STAGNATION, PF_ERR_TOO_LARGE = range(8)
 PF_FP64, PF_MIXED, PF_MIXED_MG = 0, 1, 2
+PF_WARM_START = 0x100   # flag in prec: mixed solves start from the DP given
 
 
 class Grid(ctypes.Structure):

@@ -70,7 +70,15 @@ def project(vel, spacing, rho, dt, tol=1e-12, max_it=20000, p=None, DP=None):
     src = ops.div_vel(u, v, w, spacing)
     DP = torch.zeros_like(u) if DP is None else DP.zero_()
     p = torch.zeros_like(u) if p is None else p
+    # a field that is already divergence free to round-off (the adjoint of a
+    # loss between two projected fields) needs no correction: a solve on a
+    # round-off right-hand side would only iterate on noise
+    vmax = max(float(t.abs().max()) for t in vel)
+    if float(src.abs().max()) <= 1e-13 * vmax / min(spacing):
+        return None
     info = ops.bicgstab_solve(src, DP, p, spacing, rho, dt, tol, max_it)
+    if info.status in (L.PF_NONFINITE, L.PF_BREAKDOWN):
+        raise RuntimeError("projection solve failed (status %d)" % info.status)
     ops.vel_corr(DP, dt / rho, u, v, w, spacing)
     return info
 
@@ -203,8 +211,10 @@ class ForwardStep(torch.autograd.Function):
         uo, vo, wo = u.detach().clone(), v.detach().clone(), w.detach().clone()
         p = torch.zeros_like(uo)
         DP = torch.zeros_like(uo)
-        ops.forward_step(uo, vo, wo, p, DP, spacing, mu, rho, dt, rk4=rk4,
-                         min_res=tol, max_it=max_it, sfs=sd)
+        info = ops.forward_step(uo, vo, wo, p, DP, spacing, mu, rho, dt, rk4=rk4,
+                                min_res=tol, max_it=max_it, sfs=sd)
+        if info.status in (L.PF_NONFINITE, L.PF_BREAKDOWN):
+            raise RuntimeError("forward step: pressure solve failed (status %d)" % info.status)
         return uo, vo, wo
 
     @staticmethod

@@ -22,6 +22,9 @@ bool grid_ok(const pf_grid* g) {
 
 bool prec_ok(int p) { return p == PF_FP64 || p == PF_MIXED || p == PF_MIXED_MG; }
 
+// prec with the optional PF_WARM_START flag of the solving entry points
+bool prec_flags_ok(int p) { return prec_ok(p & 0xFF) && (p & ~0xFF & ~PF_WARM_START) == 0; }
+
 cudaStream_t S(void* s) { return (cudaStream_t)s; }
 
 int cuda_rc(cudaError_t e) { return e == cudaSuccess ? PF_OK : PF_ERR_CUDA; }
@@ -91,8 +94,9 @@ int pf_bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
                       double min_res, int max_it, const double* source,
                       double* DP, double* p, void* ws, size_t ws_bytes,
                       void* stream, pf_solve_info* info) {
-    if (!grid_ok(g) || !prec_ok(prec) || !source || !DP || !p || !(dt != 0.0)) return PF_ERR_BAD_ARG;
-    if (!ws || ws_bytes < poisson_ws_bytes(g, prec)) return PF_ERR_BAD_ARG;
+    if (!grid_ok(g) || !prec_flags_ok(prec) || !source || !DP || !p || !(dt != 0.0))
+        return PF_ERR_BAD_ARG;
+    if (!ws || ws_bytes < poisson_ws_bytes(g, prec & 0xFF)) return PF_ERR_BAD_ARG;
     return bicgstab_solve(g, prec, rho, dt, min_res, max_it, source, DP, p, ws, S(stream), info);
 }
 
@@ -116,9 +120,11 @@ int pf_forward_step(const pf_grid* g, int prec, int rk4, int solver,
                     const void* sfs, double dt, double min_res, int max_it,
                     void* ws, size_t ws_bytes, void* stream,
                     pf_solve_info* info) {
-    if (!grid_ok(g) || !prec_ok(prec) || !u || !v || !w || !p || !DP || !(rho != 0.0) ||
+    if (!grid_ok(g) || !prec_flags_ok(prec) || !u || !v || !w || !p || !DP || !(rho != 0.0) ||
         !(dt != 0.0) || (solver != 0 && solver != 1))
         return PF_ERR_BAD_ARG;
+    const int flags = prec & ~0xFF;
+    prec &= 0xFF;
     if (!ws || ws_bytes < pf_workspace_bytes(g, prec)) return PF_ERR_BAD_ARG;
     const size_t n = (size_t)g->nx * g->ny * g->nz;
     double* div = (double*)ws;
@@ -130,7 +136,7 @@ int pf_forward_step(const pf_grid* g, int prec, int rk4, int solver,
     if (rc) return rc;
     pf_solve_info si{0.0, 0, 1, PF_OK};
     if (solver == 0) {
-        rc = bicgstab_solve(g, prec, rho, dt, min_res, max_it, div, DP, p, rest, s, &si);
+        rc = bicgstab_solve(g, prec | flags, rho, dt, min_res, max_it, div, DP, p, rest, s, &si);
     } else {
         // the Jacobi solver zeroes and overwrites p (src/solver/pressure.py:121)
         rc = jacobi_solve(g, rho, dt, max_it, div, DP, p, rest, s, &si.max_res);

@@ -438,6 +438,9 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
                    double min_res, int max_it, const double* source,
                    double* DP, double* p, void* ws, cudaStream_t s,
                    pf_solve_info* info) {
+    // PF_WARM_START (mixed forms): the refinement starts from the DP given
+    const bool warm = (prec & PF_WARM_START) != 0 && (prec & 0xFF) != PF_FP64;
+    prec &= 0xFF;
     Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     const size_t n = (size_t)d.n;
     char* ptr = (char*)ws;
@@ -490,7 +493,8 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
             if (rc != PF_OK && rc != PF_ERR_BAD_ARG) return rc;
             if (mg.L && mg_enqueue_setup(mg, s) != PF_OK) return PF_ERR_CUDA;
         }
-        PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b, DP, nullptr));
+        PF_LAUNCH("mixed_b_init", s, mixed_b_init<<<gp, kBlock, 0, s>>>(d, sc, part, source, c1, c2, b,
+                                                                       warm ? nullptr : DP, nullptr));
         if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
         const double max_b = hs.max_b;
         int status = PF_OK, outer = 0, total = 0;
@@ -498,7 +502,7 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
         double ratio = max_b > 0 ? 1.0 : 0.0, prev_ratio = 2.0;
         if (!(max_b == max_b)) status = PF_NONFINITE;
         while (status == PF_OK && max_b > 0.0) {
-            if (outer > 0) {
+            if (outer > 0 || warm) {
                 PF_LAUNCH("mixed_residual", s, mixed_residual<<<tiled_grid(tld), dim3(32, 8), 0, s>>>(
                     d, tld, cfd, sc, part, b, DP, r));
                 if (read_scalars(sc, &hs, s)) return PF_ERR_CUDA;
@@ -509,7 +513,7 @@ int bicgstab_solve(const pf_grid* g, int prec, double rho, double dt,
             if (outer >= kMaxOuter || total >= max_it) { status = PF_MAXIT; break; }
             if (!use64 && outer > 1 && ratio > 0.5 * prev_ratio) use64 = true;
             prev_ratio = ratio;
-            const double* rhs = outer == 0 ? b : r;
+            const double* rhs = (outer == 0 && !warm) ? b : r;
             ++outer;
             if (!use64) {
                 float* e = e32;

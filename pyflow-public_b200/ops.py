@@ -119,18 +119,20 @@ def predictor_step(u, v, w, spacing, mu, rho, dt, rk4=True, prec="fp64",
 
 
 def bicgstab_solve(source, DP, p, spacing, rho, dt, min_res, max_it,
-                   prec="fp64"):
+                   prec="fp64", warm=False):
     """solver_bicgstab.solve (src/solver/pressure.py:196-297): DP solves the
-    pressure Poisson equation for the divergence ``source``; p += DP.
+    pressure Poisson equation for the divergence ``source``; p += DP.  With
+    ``warm`` (mixed forms) the solve starts from the DP given.
     Returns a SolveInfo (max_res, iterations, outer, status)."""
     for t, nm in ((source, "source"), (DP, "DP"), (p, "p")):
         _check(t, source.shape, torch.float64, nm)
     pr = PREC[prec]
+    flag = L.PF_WARM_START if warm else 0
     g = grid(source.shape, spacing)
     ws = workspace(g, pr, source.device)
     info = L.SolveInfo()
     L.check("pf_bicgstab_solve", L.lib().pf_bicgstab_solve(
-        ctypes.byref(g), pr, float(rho), float(dt), float(min_res),
+        ctypes.byref(g), pr | flag, float(rho), float(dt), float(min_res),
         int(max_it), _p(source), _p(DP), _p(p), _p(ws), ws.numel(),
         _stream(source), ctypes.byref(info)))
     return info
@@ -162,8 +164,10 @@ def vel_corr(DP, scale, u, v, w, spacing):
 
 def forward_step(u, v, w, p, DP, spacing, mu, rho, dt, rk4=True,
                  solver="bicgstab", min_res=1e-10, max_it=300, prec="fp64",
-                 visc=None, sfs=None):
-    """Domain.forwardStep + velCorr (src/data/domain.py:342-402)."""
+                 visc=None, sfs=None, warm=False):
+    """Domain.forwardStep + velCorr (src/data/domain.py:342-402).  With
+    ``warm`` (mixed forms) the pressure solve starts from the DP given (the
+    previous step's), as the mixed step plans do."""
     for t, nm in ((u, "u"), (v, "v"), (w, "w"), (p, "p"), (DP, "DP")):
         _check(t, u.shape, torch.float64, nm)
     pr = PREC[prec]
@@ -176,7 +180,7 @@ def forward_step(u, v, w, p, DP, spacing, mu, rho, dt, rk4=True,
     ws = workspace(g, pr, u.device)
     info = L.SolveInfo()
     L.check("pf_forward_step", L.lib().pf_forward_step(
-        ctypes.byref(g), pr, 1 if rk4 else 0,
+        ctypes.byref(g), pr | (L.PF_WARM_START if warm else 0), 1 if rk4 else 0,
         0 if solver == "bicgstab" else 1, _p(u), _p(v), _p(w), _p(p), _p(DP),
         _p(visc), float(mu), float(rho), _p(sfs), float(dt), float(min_res),
         int(max_it), _p(ws), ws.numel(), _stream(u), ctypes.byref(info)))

@@ -200,6 +200,7 @@ class Trainer:
                                     requires_grad=True) for k in PARAM_NAMES]
         self.opt = torch.optim.RMSprop(self.params, lr=cfg.lr)
         self.history = []
+        self.skipped = 0   # windows whose gradient was not finite (no update)
 
     def loss(self):
         cfg = self.cfg
@@ -217,14 +218,18 @@ class Trainer:
         return total / cfg.steps
 
     def step(self):
-        """One window: forward, backward, update.  A window whose loss is not
-        finite (an LES that blew up) updates nothing and reports its loss."""
+        """One window: forward, backward, update.  A window whose loss or
+        gradient is not finite updates nothing (counted in ``skipped``) and
+        reports its loss."""
         self.opt.zero_grad(set_to_none=True)
         L = self.loss()
         val = float(L.detach())
         if math.isfinite(val):
             L.backward()
-            self.opt.step()
+            if all(bool(torch.isfinite(p.grad).all()) for p in self.params if p.grad is not None):
+                self.opt.step()
+            else:
+                self.skipped += 1
         self.history.append(val)
         return val
 
