@@ -265,14 +265,17 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bia
         uint32_t r[32];
         tmem_ld32_issue(taddr + c0, r);
         tmem_wait_ld();
+        // the bias of these 32 columns as 16-byte shared-memory loads
+        const float4* b4 = reinterpret_cast<const float4*>(bias + c0);
 #pragma unroll
         for (int q = 0; q < 32; q += 8) {
+            const float4 ba = b4[q / 4], bb = b4[q / 4 + 1];
+            const float bq[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
             uint32_t packed[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e)
-                packed[e] = tanh_pack_bf16x2(__uint_as_float(r[q + 2 * e]) + bias[c0 + q + 2 * e],
-                                             __uint_as_float(r[q + 2 * e + 1]) +
-                                                 bias[c0 + q + 2 * e + 1]);
+                packed[e] = tanh_pack_bf16x2(__uint_as_float(r[q + 2 * e]) + bq[2 * e],
+                                             __uint_as_float(r[q + 2 * e + 1]) + bq[2 * e + 1]);
             // 8 consecutive k of one row are one 16-byte chunk
             *reinterpret_cast<uint4*>(H + kmajor_off(row, c0 + q, 4096)) =
                 make_uint4(packed[0], packed[1], packed[2], packed[3]);
