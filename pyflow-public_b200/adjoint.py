@@ -77,8 +77,8 @@ def project(vel, spacing, rho, dt, tol=1e-12, max_it=20000, p=None, DP=None):
     if float(src.abs().max()) <= 1e-13 * vmax / min(spacing):
         return None
     info = ops.bicgstab_solve(src, DP, p, spacing, rho, dt, tol, max_it)
-    if info.status in (L.PF_NONFINITE, L.PF_BREAKDOWN):
-        raise RuntimeError("projection solve failed (status %d)" % info.status)
+    if info.status == L.PF_NONFINITE:
+        raise RuntimeError("projection solve: non-finite residual")
     ops.vel_corr(DP, dt / rho, u, v, w, spacing)
     return info
 
@@ -213,8 +213,8 @@ class ForwardStep(torch.autograd.Function):
         DP = torch.zeros_like(uo)
         info = ops.forward_step(uo, vo, wo, p, DP, spacing, mu, rho, dt, rk4=rk4,
                                 min_res=tol, max_it=max_it, sfs=sd)
-        if info.status in (L.PF_NONFINITE, L.PF_BREAKDOWN):
-            raise RuntimeError("forward step: pressure solve failed (status %d)" % info.status)
+        if info.status == L.PF_NONFINITE:
+            raise RuntimeError("forward step: non-finite pressure residual")
         return uo, vo, wo
 
     @staticmethod
