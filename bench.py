@@ -507,8 +507,10 @@ def les_measurement(torch, dev, windows=3):
         e1.record(st)
         torch.cuda.synchronize(dev)
         times.append(e0.elapsed_time(e1) / 1e3)
+    tr_skipped = tr.skipped
     del targets, tr
     return {"les_grid": cfg.n, "dns_grid": cfg.n * cfg.factor, "window_steps": cfg.steps,
+            "windows_without_update": tr_skipped,
             "nu": cfg.nu, "dt": cfg.dt, "dns_seed": cfg.dns_seed, "mlp_seed": cfg.mlp_seed,
             "target_dns_s": dns_s, "window_s": times, "loss": losses,
             "les_cell_steps_per_s_fwd_bwd": cfg.n ** 3 * cfg.steps / float(np.median(times)),
@@ -621,7 +623,10 @@ def run_b200(a):
                 serve = serve_measurement(a, torch, dev)
                 torch.cuda.empty_cache()
             if not a.no_les and world == 1:
-                les = les_measurement(torch, dev)
+                try:
+                    les = les_measurement(torch, dev)
+                except RuntimeError as e:   # reported, the rest of the line stands
+                    les = {"error": str(e)}
                 torch.cuda.empty_cache()
     if rank == 0 and not a.no_cpu_baseline:
         its_ref = fp64["iterations_per_step"] if fp64 else wl["fp64_its"]

@@ -225,8 +225,13 @@ class Trainer:
         L = self.loss()
         val = float(L.detach())
         if math.isfinite(val):
-            L.backward()
-            if all(bool(torch.isfinite(p.grad).all()) for p in self.params if p.grad is not None):
+            try:
+                L.backward()
+                finite = all(bool(torch.isfinite(p.grad).all())
+                             for p in self.params if p.grad is not None)
+            except RuntimeError:
+                finite = False   # a non-finite adjoint field stopped the backward pass
+            if finite:
                 self.opt.step()
             else:
                 self.skipped += 1
