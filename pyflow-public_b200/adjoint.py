@@ -70,11 +70,13 @@ def project(vel, spacing, rho, dt, tol=1e-12, max_it=20000, p=None, DP=None):
     src = ops.div_vel(u, v, w, spacing)
     DP = torch.zeros_like(u) if DP is None else DP.zero_()
     p = torch.zeros_like(u) if p is None else p
-    # a field that is already divergence free to round-off (the adjoint of a
-    # loss between two projected fields) needs no correction: a solve on a
-    # round-off right-hand side would only iterate on noise
+    # a field that is already divergence free to the solver's precision (the
+    # adjoint of a loss between two projected fields: its divergence is
+    # round-off of the field) needs no correction: BiCGStab on a round-off
+    # right-hand side only iterates on noise, stagnates at the relative
+    # tolerance and can end non-finite
     vmax = max(float(t.abs().max()) for t in vel)
-    if float(src.abs().max()) <= 1e-13 * vmax / min(spacing):
+    if float(src.abs().max()) <= 1e-9 * vmax / min(spacing):
         return None
     info = ops.bicgstab_solve(src, DP, p, spacing, rho, dt, tol, max_it)
     if info.status == L.PF_NONFINITE:

@@ -6,19 +6,22 @@
 // accumulation; its six outputs times out_scale are the stresses FXX, FYY, FZZ,
 // FXY, FXZ, FYZ of the 'tensor' SFS slot (src/solver/velocity.py:262-267,...).
 //
-// CTAs of 256 threads (8 warps, two CTAs per SM) walk tiles of 128
+// CTAs of 128 threads (4 warps, three CTAs per SM) walk tiles of 128
 // consecutive cells; cell m of a tile is accumulator row / TMEM lane m and
-// belongs to threads m and m + 128 (the second warpgroup reads the same TMEM
-// lanes, columns 64..127):
-//   1. threads 0..127 compute their cell's gradients and write 16 BF16
-//      features (9 + 7 zero pads) into the X tile in shared memory;
+// belongs to thread m:
+//   1. each thread computes its cell's gradients and writes 16 BF16 features
+//      (9 + 7 zero pads) into the X tile in shared memory (the first 4 KB of
+//      the H tile);
 //   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
-//   3. each thread reads its 64 columns of its D1 row from TMEM (tcgen05.ld,
-//      one wait), adds b1, rounds pairs of pre-activations to BF16, applies
-//      the packed BF16 tanh and writes them into the H tile;
+//   3. each thread reads its D1 row from TMEM (tcgen05.ld, 32 columns per
+//      wait), adds b1, rounds pairs of pre-activations to BF16, applies the
+//      packed BF16 tanh and writes them into the H tile;
 //   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
-//   5. 8 tcgen05.mma with N=16: D3 = H W3^T; threads 0..127 add b3 and
-//      write their six stresses (FP64) to global memory.
+//   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
+//      its six stresses (FP64) to global memory.
+// The three layers accumulate one after another into the same 128 TMEM
+// columns (each epilogue has read its accumulator before the next layer is
+// issued).
 // Completion of each MMA group is signalled by tcgen05.commit to an mbarrier;
 // every wait on it is bounded and reports a timeout through an error flag.
 //
@@ -42,15 +45,16 @@ namespace mlp {
 
 constexpr int kHidden = 128;
 constexpr int kTile = 128;
-constexpr int kThreads = 256;      // two threads per accumulator row
+constexpr int kThreads = 128;      // one thread per accumulator row
+constexpr int kCtasPerSm = 3;      // three tiles in flight per SM
 constexpr int kW1Bytes = 4096;      // 128 x 16 bf16
 constexpr int kW2Bytes = 32768;     // 128 x 128 bf16
 constexpr int kW3Bytes = 4096;      // 16 x 128 bf16
 constexpr int kBiasBytes = (128 + 128 + 16) * 4;
 constexpr int kPackBytes = kW1Bytes + kW2Bytes + kW3Bytes + kBiasBytes;
-constexpr int kXBytes = 4096;       // 128 x 16 bf16
+constexpr int kXBytes = 4096;       // 128 x 16 bf16 (shares the H tile's first bytes)
 constexpr int kHBytes = 32768;      // 128 x 128 bf16
-constexpr unsigned kTmemCols = 256;
+constexpr unsigned kTmemCols = 128; // the three layers' accumulators, one after another
 constexpr long long kSpinLimit = 1LL << 22;
 
 // byte offset of element (row r, col k) in a K-major no-swizzle tile whose
@@ -254,14 +258,14 @@ __device__ inline void nb_gradients(const CellNb& nb, double dxi, double dyi, do
     }
 }
 
-// Writes 64 hidden values (columns c_begin .. c_begin + 63) of this thread's
-// row: tanh(acc + bias) as BF16.
+// Writes the 128 hidden values of this thread's row: tanh(acc + bias) as
+// BF16 (c_begin = 0).
 __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bias,
                                                 uint8_t* H, int row, int c_begin) {
     // 32 columns per TMEM load and wait (the second warpgroup's loads and the
     // other CTA's work cover the wait)
 #pragma unroll 1
-    for (int c0 = c_begin; c0 < c_begin + 64; c0 += 32) {
+    for (int c0 = c_begin; c0 < c_begin + kHidden; c0 += 32) {
         uint32_t r[32];
         tmem_ld32_issue(taddr + c0, r);
         tmem_wait_ld();
@@ -286,7 +290,7 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* bia
 }  // namespace mlp
 
 // scales[0] = 1/g_rms (input normalisation), scales[1] = output scale
-__global__ void __launch_bounds__(mlp::kThreads, 2)
+__global__ void __launch_bounds__(mlp::kThreads, mlp::kCtasPerSm)
 mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restrict__ v,
                    const double* __restrict__ w, double dxi, double dyi, double dzi,
                    const uint8_t* __restrict__ wpack, const float* __restrict__ scales,
@@ -297,17 +301,19 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     uint8_t* sW2 = sW1 + kW1Bytes;
     uint8_t* sW3 = sW2 + kW2Bytes;
     float* sB = reinterpret_cast<float*>(sW3 + kW3Bytes);  // b1[128] b2[128] b3[16]
-    uint8_t* sX = reinterpret_cast<uint8_t*>(sB) + kBiasBytes;
-    uint8_t* sH = sX + kXBytes;
+    // X shares the first 4 KB of the H tile: layer 1 reads X before the
+    // epilogue that writes H, and the next tile writes X after layer 3 has
+    // read H
+    uint8_t* sH = reinterpret_cast<uint8_t*>(sB) + kBiasBytes;
+    uint8_t* sX = sH;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sH + kHBytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
 
-    // 256 threads: thread (half, row) with row = tid % 128 owns accumulator
-    // row / TMEM lane `row` and, in the epilogues, its 64 columns
-    // half*64 .. half*64+63; the first half also computes the features and
-    // writes the outputs.  Warp w reads TMEM lanes 32 (w % 4) .. +31.
+    // thread `row` owns accumulator row / TMEM lane `row`: its features, its
+    // 128 hidden columns in the epilogues and its outputs.  Warp w reads TMEM
+    // lanes 32 w .. 32 w + 31.
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int row = tid & (kTile - 1), half = tid >> 7;
+    const int row = tid, half = 0;
     // weights: a straight copy of the packed image
     {
         const uint4* src = reinterpret_cast<const uint4*>(wpack);
@@ -328,7 +334,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t d1 = tmem, d2 = tmem + 128, d3 = tmem;  // column offsets
+    const uint32_t d1 = tmem, d2 = tmem, d3 = tmem;  // one 128-column accumulator
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     const float in_scale = scales[0], out_scale = scales[1];
     const uint32_t id128 = instr_desc(128, 128), id16 = instr_desc(128, 16);
@@ -376,7 +382,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
-        hidden_epilogue(lane_base + d1, sB, sH, row, half * 64);
+        hidden_epilogue(lane_base + d1, sB, sH, row, 0);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -393,7 +399,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
-        hidden_epilogue(lane_base + d2, sB + 128, sH, row, half * 64);
+        hidden_epilogue(lane_base + d2, sB + 128, sH, row, 0);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -439,7 +445,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
 }
 
 size_t mlp_smem_bytes() {
-    return (size_t)mlp::kPackBytes + mlp::kXBytes + mlp::kHBytes + 64;
+    return (size_t)mlp::kPackBytes + mlp::kHBytes + 64;
 }
 
 cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
@@ -454,7 +460,7 @@ cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
         cudaError_t e = cudaFuncSetAttribute(mlp_closure_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        // the largest shared-memory carveout, so two CTAs fit on an SM
+        // the largest shared-memory carveout, so three CTAs fit on an SM
         e = cudaFuncSetAttribute(mlp_closure_kernel,
                                  cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
@@ -465,11 +471,11 @@ cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long ntiles = (d.n + mlp::kTile - 1) / mlp::kTile;
-    // two CTAs per SM, so one's tensor-core layer overlaps the other's
-    // epilogue: each holds 256 of the SM's 512 TMEM columns and ~79 KB of
-    // shared memory (a third would not fit in shared memory, so a TMEM
-    // allocation never has to wait for another CTA of this kernel)
-    const int grid = (int)std::min<long long>(ntiles, 2LL * sms);
+    // three CTAs per SM, so the tensor-core layers of some overlap the
+    // epilogues of the others: each holds 128 of the SM's 512 TMEM columns
+    // and ~73 KB of shared memory (a fourth would not fit in shared memory,
+    // so a TMEM allocation never has to wait for another CTA of this kernel)
+    const int grid = (int)std::min<long long>(ntiles, (long long)mlp::kCtasPerSm * sms);
     PF_LAUNCH("mlp_closure", s, mlp_closure_kernel<<<grid, mlp::kThreads, smem, s>>>(
         d, u, v, w, 1.0 / g->dx, 1.0 / g->dy, 1.0 / g->dz, (const uint8_t*)wpack, scales,
         out, err));
