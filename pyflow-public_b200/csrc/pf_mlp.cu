@@ -14,8 +14,8 @@
 //      the H tile);
 //   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
 //   3. each thread reads its D1 row from TMEM (tcgen05.ld, 32 columns per
-//      wait), adds b1, rounds pairs of pre-activations to BF16, applies the
-//      packed BF16 tanh and writes them into the H tile;
+//      wait), adds b1, truncates pairs of pre-activations to BF16, applies
+//      the packed BF16 tanh and writes them into the H tile;
 //   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
 //   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
 //      its six stresses (FP64) to global memory.
@@ -52,8 +52,7 @@ constexpr int kW2Bytes = 32768;     // 128 x 128 bf16
 constexpr int kW3Bytes = 4096;      // 16 x 128 bf16
 constexpr int kBiasBytes = (128 + 128 + 16) * 4;
 constexpr int kPackBytes = kW1Bytes + kW2Bytes + kW3Bytes + kBiasBytes;
-constexpr int kXBytes = 4096;       // 128 x 16 bf16 (shares the H tile's first bytes)
-constexpr int kHBytes = 32768;      // 128 x 128 bf16
+constexpr int kHBytes = 32768;      // 128 x 128 bf16; its first 4 KB hold the 128 x 16 X tile
 constexpr unsigned kTmemCols = 128; // the three layers' accumulators, one after another
 constexpr long long kSpinLimit = 1LL << 22;
 
@@ -158,14 +157,14 @@ __device__ __forceinline__ void tmem_wait_ld() {
 }
 
 // tanh of two FP32 pre-activations as one packed BF16 pair (a in the low
-// half): both are rounded to BF16 by one conversion, then the hardware tanh
-// of the pair (tanh.approx.bf16x2) gives the two BF16 activations the next
-// layer reads.  One special-function instruction per pair: the epilogue's
-// limit is the special-function unit, so this halves it against two FP32
-// tanh and a conversion.
+// half): both are truncated to BF16 by one byte permutation (their high
+// halves), then the hardware tanh of the pair (tanh.approx.bf16x2) gives the
+// two BF16 activations the next layer reads.  The epilogue is bound by the
+// special-function unit; the permutation runs on the integer pipe, so a
+// pair costs that unit one instruction.
 __device__ __forceinline__ uint32_t tanh_pack_bf16x2(float a, float b) {
-    uint32_t x, y;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(x) : "f"(b), "f"(a));
+    const uint32_t x = __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632);
+    uint32_t y;
     asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(x));
     return y;
 }

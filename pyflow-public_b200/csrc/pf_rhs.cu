@@ -699,19 +699,18 @@ static StageJob<T, TI> make_job(const GroupMember& m, const TI* in_u, const TI* 
 }
 
 int grouped_predictor_prepare(int prec) {
-    cudaError_t e = cudaSuccess;
     if (prec == PF_FP64) {
-        if ((e = grouped_prepare<double, double, kModeK>()) ||
-            (e = grouped_prepare<double, double, kModeFirst>()) ||
-            (e = grouped_prepare<double, double, kModeMid>()) ||
-            (e = grouped_prepare<double, double, kModeLast>()))
+        if (grouped_prepare<double, double, kModeK>() ||
+            grouped_prepare<double, double, kModeFirst>() ||
+            grouped_prepare<double, double, kModeMid>() ||
+            grouped_prepare<double, double, kModeLast>())
             return PF_ERR_CUDA;
         return PF_OK;
     }
-    if ((e = grouped_prepare<float, double, kModeK>()) ||
-        (e = grouped_prepare<float, double, kModeFirst>()) ||
-        (e = grouped_prepare<float, float, kModeMid>()) ||
-        (e = grouped_prepare<float, float, kModeLast>()))
+    if (grouped_prepare<float, double, kModeK>() ||
+        grouped_prepare<float, double, kModeFirst>() ||
+        grouped_prepare<float, float, kModeMid>() ||
+        grouped_prepare<float, float, kModeLast>())
         return PF_ERR_CUDA;
     return PF_OK;
 }

@@ -76,9 +76,15 @@ def _bf16(x):
     return x.to(torch.bfloat16).to(torch.float32)
 
 
+def _bf16_trunc(x):
+    """FP32 -> BF16 by truncation (the kernel keeps the high half of each
+    pre-activation), back to FP32."""
+    return torch.bitwise_and(x.float().contiguous().view(torch.int32), -65536).view(torch.float32)
+
+
 def reference_forward(grads, params, in_scale, out_scale):
     """Torch model of the tensor-core forward pass: BF16 inputs and weights,
-    FP32 accumulation, pre-activations rounded to BF16 before tanh, BF16
+    FP32 accumulation, pre-activations truncated to BF16 before tanh, BF16
     hidden activations.  grads: (9, n) float64 tensor."""
     dev = grads.device
     x = _bf16((grads.T.to(torch.float32) * in_scale))
@@ -86,8 +92,8 @@ def reference_forward(grads, params, in_scale, out_scale):
     W2 = _bf16(torch.as_tensor(params["W2"], device=dev))
     W3 = _bf16(torch.as_tensor(params["W3"], device=dev))
     b1, b2, b3 = (torch.as_tensor(params[k], device=dev) for k in ("b1", "b2", "b3"))
-    h1 = _bf16(torch.tanh(_bf16(x @ W1.T + b1)))
-    h2 = _bf16(torch.tanh(_bf16(h1 @ W2.T + b2)))
+    h1 = _bf16(torch.tanh(_bf16_trunc(x @ W1.T + b1)))
+    h2 = _bf16(torch.tanh(_bf16_trunc(h1 @ W2.T + b2)))
     y = h2 @ W3.T + b3
     return (y.to(torch.float64) * out_scale).T.contiguous()
 

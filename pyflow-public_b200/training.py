@@ -83,6 +83,12 @@ def _ste_bf16(x):
     return x + (x.to(torch.bfloat16).to(x.dtype) - x).detach()
 
 
+def _ste_bf16_trunc(x):
+    """BF16 truncation (the kernel's pre-activations) in the forward pass,
+    identity in the backward pass."""
+    return x + (M._bf16_trunc(x).to(x.dtype) - x).detach()
+
+
 def closure_torch(u, v, w, spacing, delta, W1, b1, W2, b2, W3, b3, rounding=True):
     """Torch restatement of the tensor-core closure: BF16 inputs, weights and
     hidden activations as straight-through roundings, FP32 accumulation.
@@ -94,13 +100,13 @@ def closure_torch(u, v, w, spacing, delta, W1, b1, W2, b2, W3, b3, rounding=True
     shape = u.shape
     x = g9.reshape(9, -1).T / g_rms
     if rounding:
-        rnd, dt = _ste_bf16, torch.float32
+        rnd, trn, dt = _ste_bf16, _ste_bf16_trunc, torch.float32
     else:
-        rnd, dt = (lambda t: t), torch.float64
+        rnd, trn, dt = (lambda t: t), (lambda t: t), torch.float64
     W1, b1, W2, b2, W3, b3 = (t.to(dt) for t in (W1, b1, W2, b2, W3, b3))
     x = rnd(x.to(dt))
-    h1 = rnd(torch.tanh(rnd(x @ rnd(W1).T + b1)))
-    h2 = rnd(torch.tanh(rnd(h1 @ rnd(W2).T + b2)))
+    h1 = rnd(torch.tanh(trn(x @ rnd(W1).T + b1)))
+    h2 = rnd(torch.tanh(trn(h1 @ rnd(W2).T + b2)))
     y = h2 @ rnd(W3).T + b3
     F = y.to(torch.float64) * ((delta * delta) * g2)
     return F.T.reshape((6,) + tuple(shape)).contiguous()
