@@ -188,6 +188,32 @@ int pf_mlp_closure(const pf_grid* g, const double* u, const double* v,
                    const double* w, const void* wpack, const float* scales,
                    double* out, int* err, void* stream);
 
+/* The reference's 'source'-type ML closure on the tensor cores: replaces
+ * residual_stress.update (src/sfsmodel/sfsmodel_ML.py:354-401; features
+ * :407-460, stencil input :464-510, network NeuralNetworkModel2 :77-116,
+ * closure terms :513-590) and the face interpolation the RHS subtracts
+ * (src/solver/velocity.py:374-383).  Inputs: the staggered FP64 velocity;
+ * the spacing used in every direction is g->dx, as in the reference.
+ * Outputs (FP64, 3n each): G = GX, GY, GZ at cell centres and S = the face
+ * sources 0.5 (G[i] + G[i-1]) along x, y, z.  The network runs as three
+ * TF32 MMAs per product (hi/lo split of both operands, FP32 accumulation in
+ * TMEM), close to the reference's FP32.
+ *   pf_mlsrc_pack: params = 13 device float pointers, the torch layouts of
+ *     fc1.weight (200x273), fc1.bias, fcG.weight, fcG.bias, fcG2.weight,
+ *     fcG2.bias, fc2.weight (200x200), fc2.bias, fc3.weight, fc3.bias,
+ *     fc4.weight (18x200), fc4.bias, then the 21 feature normalisation
+ *     constants; pack: device buffer of pf_mlsrc_pack_bytes(), 16-byte
+ *     aligned.  Repack after every parameter update.
+ *   pf_mlsrc_closure: ws: device buffer of pf_mlsrc_workspace_bytes(g)
+ *     (about 5 KB per cell), 256-byte aligned; err: device int set to 1 if a
+ *     tensor-core wait timed out.  Grids need at least 5 cells per axis. */
+size_t pf_mlsrc_pack_bytes(void);
+size_t pf_mlsrc_workspace_bytes(const pf_grid* g);
+int pf_mlsrc_pack(const float* const* params, void* pack, void* stream);
+int pf_mlsrc_closure(const pf_grid* g, const double* u, const double* v,
+                     const double* w, const void* pack, double* G, double* S,
+                     void* ws, size_t ws_bytes, int* err, void* stream);
+
 /* Exact discrete adjoint of the constant-viscosity RHS: out = J(u)^T mu where
  * J is the Jacobian of pf_rhs_ns (rhs_NavierStokes.evaluate,
  * src/solver/velocity.py:221-355) at state (u, v, w).  Replaces the

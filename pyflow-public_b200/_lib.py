@@ -66,6 +66,10 @@ def _load():
         "pf_restart_pack": ([G, P, P, P], I),
         "pf_restart_unpack": ([G, P, P, P], I),
         "pf_mlp_closure": ([G, P, P, P, P, P, P, P, P], I),
+        "pf_mlsrc_pack_bytes": ([], S),
+        "pf_mlsrc_workspace_bytes": ([G], S),
+        "pf_mlsrc_pack": ([ctypes.POINTER(ctypes.c_void_p), P, P], I),
+        "pf_mlsrc_closure": ([G, P, P, P, P, P, P, P, S, P, P], I),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)

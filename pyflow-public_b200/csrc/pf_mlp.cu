@@ -38,10 +38,13 @@
 #include "pf_common.cuh"
 #include "pf_kernels.cuh"
 #include "pf_profile.cuh"
+#include "pf_umma.cuh"
 
 namespace pf {
 
 namespace mlp {
+
+using namespace umma;
 
 constexpr int kHidden = 128;
 constexpr int kTile = 128;
@@ -54,106 +57,12 @@ constexpr int kBiasBytes = (128 + 128 + 16) * 4;
 constexpr int kPackBytes = kW1Bytes + kW2Bytes + kW3Bytes + kBiasBytes;
 constexpr int kHBytes = 32768;      // 128 x 128 bf16; its first 4 KB hold the 128 x 16 X tile
 constexpr unsigned kTmemCols = 128; // the three layers' accumulators, one after another
-constexpr long long kSpinLimit = 1LL << 22;
 
 // byte offset of element (row r, col k) in a K-major no-swizzle tile whose
 // 16-wide K slices are `slice` bytes apart
 __device__ __forceinline__ uint32_t kmajor_off(int r, int k, int slice) {
     return (uint32_t)((k >> 4) * slice + (r >> 3) * 256 + ((k >> 3) & 1) * 128 + (r & 7) * 16 +
                       (k & 7) * 2);
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// UMMA shared-memory descriptor: K-major, no swizzle, LBO 128 B, SBO 256 B,
-// descriptor version 1 (sm_100)
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFF);
-    d |= (uint64_t)(128 >> 4) << 16;
-    d |= (uint64_t)(256 >> 4) << 32;
-    d |= (uint64_t)1 << 46;
-    return d;  // base offset 0, lbo mode 0, layout type 0 (no swizzle)
-}
-
-// instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major
-__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-           ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b,
-                                         uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-        :: "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                 :: "r"(smem_u32(bar)) : "memory");
-}
-
-// bounded wait for the mbarrier phase; false on timeout
-__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t phase) {
-    const uint32_t a = smem_u32(bar);
-    for (long long it = 0; it < kSpinLimit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done) : "r"(a), "r"(phase) : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void fence_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-          "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-          "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 32 consecutive accumulator columns of this thread's lane (no wait)
-__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t* r) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-          "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-          "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
-          "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-          "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
 // tanh of two FP32 pre-activations as one packed BF16 pair (a in the low
@@ -320,14 +229,10 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
         for (int q = tid; q < kPackBytes / 16; q += blockDim.x) dst[q] = src[q];
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(bar)));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init(bar, 1);
+        mbar_init_fence();
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(tmem_slot)), "r"(kTmemCols));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
-    }
+    if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -336,7 +241,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     const uint32_t d1 = tmem, d2 = tmem, d3 = tmem;  // one 128-column accumulator
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     const float in_scale = scales[0], out_scale = scales[1];
-    const uint32_t id128 = instr_desc(128, 128), id16 = instr_desc(128, 16);
+    const uint32_t id128 = instr_desc(kFmtBF16, 128, 128), id16 = instr_desc(kFmtBF16, 128, 16);
     uint32_t phase = 0;
     bool ok = true;
     const long long ntiles = (d.n + kTile - 1) / kTile;
@@ -438,8 +343,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-                     :: "r"(tmem), "r"(kTmemCols));
+        tmem_dealloc(tmem, kTmemCols);
     }
 }
 

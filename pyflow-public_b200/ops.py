@@ -235,3 +235,52 @@ def sgs_closure(model, u, v, w, spacing, coef=1.0, out=None):
         ctypes.byref(g), mid, _p(u), _p(v), _p(w), float(coef), _p(out),
         _stream(u)))
     return out
+
+
+def mlsrc_pack(params, norm, pack=None):
+    """Pack the 'source' network for pf_mlsrc_closure (pf_mlsrc_pack).
+
+    params: the 12 float32 CUDA tensors fc1.weight, fc1.bias, fcG.weight,
+    fcG.bias, fcG2.weight, fcG2.bias, fc2.weight, fc2.bias, fc3.weight,
+    fc3.bias, fc4.weight, fc4.bias; norm: the 21 feature normalisation
+    constants (float32, CUDA)."""
+    ts = [t.detach().contiguous() for t in list(params) + [norm]]
+    if len(ts) != 13:
+        raise ValueError("expected 12 parameter tensors and the normalisation")
+    for i, t in enumerate(ts):
+        if not t.is_cuda or t.dtype != torch.float32:
+            raise TypeError("parameter %d must be a float32 CUDA tensor" % i)
+    nbytes = L.lib().pf_mlsrc_pack_bytes()
+    if pack is None or pack.numel() < nbytes:
+        pack = torch.empty(nbytes, dtype=torch.uint8, device=ts[0].device)
+    arr = (ctypes.c_void_p * 13)(*[t.data_ptr() for t in ts])
+    L.check("pf_mlsrc_pack", L.lib().pf_mlsrc_pack(arr, _p(pack), _stream(ts[0])))
+    return pack
+
+
+def mlsrc_closure(u, v, w, dx, pack, G=None, S=None, err=None):
+    """The 'source' closure (pf_mlsrc_closure): returns (G, S, err), G the
+    (3, nx, ny, nz) FP64 closure terms GX, GY, GZ at cell centres, S the face
+    sources the RHS subtracts, err a device int (1 if a tensor-core wait
+    timed out)."""
+    for t, nm in ((u, "u"), (v, "v"), (w, "w")):
+        _check(t, u.shape, torch.float64, nm)
+    shape = (3,) + tuple(u.shape)
+    if G is None:
+        G = torch.empty(shape, dtype=torch.float64, device=u.device)
+    if S is None:
+        S = torch.empty(shape, dtype=torch.float64, device=u.device)
+    if err is None:
+        err = torch.zeros(1, dtype=torch.int32, device=u.device)
+    g = grid(u.shape, (dx, dx, dx))
+    need = L.lib().pf_mlsrc_workspace_bytes(ctypes.byref(g))
+    key = ("mlsrc", torch.device(u.device))
+    ws = _ws_cache.get(key)
+    if ws is None or ws.numel() < need:
+        _ws_cache[key] = None
+        ws = torch.empty(need, dtype=torch.uint8, device=u.device)
+        _ws_cache[key] = ws
+    L.check("pf_mlsrc_closure", L.lib().pf_mlsrc_closure(
+        ctypes.byref(g), _p(u), _p(v), _p(w), _p(pack), _p(G), _p(S), _p(ws),
+        ctypes.c_size_t(ws.numel()), _p(err), _stream(u)))
+    return G, S, err

@@ -26,13 +26,19 @@ on all cells at least three cells away from a periodic boundary (the tests
 check exactly those cells).
 
 The network is torch modules with the reference's parameter names and
-shapes (a reference checkpoint's 'model_state_dict' loads as is); features
-and network run as torch ops on the device of the velocity (CUDA in the
-Domain; its GEMMs in cuBLAS, FP32).
+shapes (a reference checkpoint's 'model_state_dict' loads as is).  On a CUDA
+device in FP32 without gradients (every forward RK stage) the whole closure
+runs as the library's kernels (pf_mlsrc_closure: features, the network on
+the tensor cores as three TF32 products per FP32 product, closure terms and
+face sources), with the weights repacked whenever a parameter changed.
+With gradients (training), in FP64 (config key mlDtype) or on the CPU it
+runs as the torch ops below.
 """
 import numpy as np
 import torch
 import torch.nn as nn
+
+from . import ops
 
 H = 200
 N_FEATURES = 21
@@ -167,10 +173,38 @@ class residual_stress:
         self.model.to(self.dtype)
         self.norm = torch.tensor(NORM, dtype=self.dtype, device=self.device)
         self.GX = self.GY = self.GZ = None
+        self._faces = None          # face sources written by the kernel path
+        self._pack = None
+        self._pack_key = None
+
+    def _kernel_path(self, u, requires_grad):
+        return (not requires_grad and u.is_cuda and self.dtype == torch.float32
+                and all(p.dtype == torch.float32 and p.is_cuda for p in self.model.parameters())
+                and min(u.shape) >= 5)
+
+    def _packed(self):
+        """The packed network, rebuilt when a parameter changed (optimizer
+        steps and load_state_dict modify the parameters in place)."""
+        params = [self.model.fc1.weight, self.model.fc1.bias, self.model.fcG.weight,
+                  self.model.fcG.bias, self.model.fcG2.weight, self.model.fcG2.bias,
+                  self.model.fc2.weight, self.model.fc2.bias, self.model.fc3.weight,
+                  self.model.fc3.bias, self.model.fc4.weight, self.model.fc4.bias]
+        key = tuple((p.data_ptr(), p._version) for p in params)
+        if self._pack is None or key != self._pack_key:
+            self._pack = ops.mlsrc_pack(params, self.norm, self._pack)
+            self._pack_key = key
+        return self._pack
 
     def update(self, u, v, w, requires_grad=False):
         """Closure terms at cell centres from the staggered velocity (FP64
         interiors); stored as FP64 like the reference (:370-380)."""
+        self._faces = None
+        if self._kernel_path(u, requires_grad):
+            G, S, self._err = ops.mlsrc_closure(u.contiguous(), v.contiguous(), w.contiguous(),
+                                                self.dx, self._packed())
+            self.GX, self.GY, self.GZ = G[0], G[1], G[2]
+            self._faces = (S[0], S[1], S[2])
+            return
         with torch.set_grad_enabled(requires_grad):
             F = features(u, v, w, self.dx, self.dtype)
             x = network_input(F, self.norm)
@@ -183,6 +217,8 @@ class residual_stress:
     def face_sources(self):
         """interp_sc_x/y/z of GX, GY, GZ (src/metric/metric_staggered.py:112-124,
         interp factor 1/2 on a uniform grid): face i gets (G[i] + G[i-1]) / 2."""
+        if self._faces is not None:
+            return self._faces
         return (0.5 * (self.GX + torch.roll(self.GX, 1, 0)),
                 0.5 * (self.GY + torch.roll(self.GY, 1, 1)),
                 0.5 * (self.GZ + torch.roll(self.GZ, 1, 2)))
