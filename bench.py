@@ -451,6 +451,73 @@ def mlp_measurement(torch, dev):
     return out
 
 
+class _UniformGeo:
+    type = "uniform"
+
+    def __init__(self, dx):
+        self.dx = dx
+
+
+def ml_source_measurement(torch, dev, n=64):
+    """The reference's 'source' closure (273 -> 200 gated -> 18 network, one
+    evaluation per RK stage) at n^3: the library's kernels (features, three
+    TF32 tensor-core layers per FP32 product, closure terms) against the same
+    closure as FP32 torch ops (cuBLAS GEMMs).  Useful FLOPs per cell:
+    2*(3*273*200 + 2*200*200 + 200*18); executed TF32 MMA FLOPs per cell:
+    3 * 2*(3*312*208 + 2*200*208 + 200*16)."""
+    import pyflow_b200.initial as ic
+    import pyflow_b200.sfsmodel_ML as ML
+    import pyflow_b200.profiling as prof
+
+    class _Dec:
+        device = torch.device(dev)
+
+    class _IC:
+        simDt = 0.01
+
+    torch.manual_seed(0)
+    ml = ML.residual_stress(_IC(), _Dec(), _UniformGeo(2 * np.pi / n), model=ML.GatedClosureNet())
+    u, v, w = (t.contiguous() for t in
+               ic.spectral_velocity_device((n, n, n), k0=4.0, seed=3, device=dev))
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    ms = timed(lambda: ml.update(u, v, w), 10)
+    prof.enable(True)
+    for _ in range(3):
+        ml.update(u, v, w)
+    torch.cuda.synchronize(dev)
+    kt = prof.read()
+    prof.enable(False)
+
+    def torch_path():
+        with torch.no_grad():
+            F = ML.features(u, v, w, ml.dx, torch.float32)
+            return ML.closure_terms(ml.model(ML.network_input(F, ml.norm)), ml.dx)
+
+    ms_torch = timed(torch_path, 5)
+    useful = 2.0 * (3 * 273 * 200 + 2 * 200 * 200 + 200 * 18) * n ** 3
+    executed = 3 * 2.0 * (3 * 312 * 208 + 2 * 200 * 208 + 200 * 16) * n ** 3
+    out = {"grid": n, "ms": ms, "torch_fp32_ms": ms_torch,
+           "tflops_useful": useful / (ms * 1e-3) / 1e12,
+           "tflops_tf32_executed": executed / (ms * 1e-3) / 1e12,
+           "err_flag": int(ml._err.item()),
+           "kernels": {k: {"launches": v["launches"] // 3, "ms": v["ms"] / 3}
+                       for k, v in kt.items() if k.startswith("mlsrc")}}
+    del u, v, w, ml
+    return out
+
+
 def serve_measurement(a, torch, dev):
     """The request-stream workload: capacity from a burst of requests of
     every size served together, then ``a.requests`` requests with Poisson
@@ -589,6 +656,7 @@ def run_b200(a):
         torch.cuda.empty_cache()
 
     roof, ktimes, e2e, mlp, cpu, serve, les = None, {}, None, None, None, None, None
+    mlsrc = None
     prof_steps = 2
     if not a.no_extras:
         # per-kernel device time: CUDA events around each launch of the
@@ -619,6 +687,8 @@ def run_b200(a):
         if rank == 0:
             mlp = mlp_measurement(torch, dev)
             torch.cuda.empty_cache()
+            mlsrc = ml_source_measurement(torch, dev)
+            torch.cuda.empty_cache()
             if not a.no_serve and world == 1:
                 serve = serve_measurement(a, torch, dev)
                 torch.cuda.empty_cache()
@@ -648,7 +718,8 @@ def run_b200(a):
                                                 "max_div")},
             "fp64_arm": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * a.steps)) if launches_per_step else None,
-            "clocks": clocks, "mlp_tensor_core": mlp, "serve": serve, "les_training": les,
+            "clocks": clocks, "mlp_tensor_core": mlp, "ml_source_closure": mlsrc,
+            "serve": serve, "les_training": les,
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ktimes.items()},
         }
         print(json.dumps(line), flush=True)

@@ -95,26 +95,34 @@ __device__ __forceinline__ float tf32_rna(float x) {
 }
 
 // --- packing ------------------------------------------------------------------
-// W (rows x cols, row-major as torch stores nn.Linear.weight) into the TF32
-// pair of matrix m; layer-1 K index s*24 + f takes input column s*21 + f
+// K values per chunk of the layers' K loops: one stencil point (24) in layer 1,
+// 40 in the others
+__host__ __device__ constexpr int chunk_k(int m) { return m < 3 ? kFP : 40; }
+
+// W (rows x cols, row-major as torch stores nn.Linear.weight) into matrix m of
+// the pack: per K chunk, the TF32 hi parts of all rows and then the lo parts,
+// each in the K-major core-matrix order of the MMA's shared-memory operand,
+// so a chunk is one flat copy.  Layer-1 K index s*24 + f takes input column
+// s*21 + f.
 __global__ void pack_matrix(const float* __restrict__ W, int rows, int cols, int m,
                             float* __restrict__ pack) {
-    const int R = mat_rows(m), K = mat_k(m);
-    const long long total = (long long)R * K;
-    float* hi = pack + w_off(m);
-    float* lo = hi + total;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(e / K), k = (int)(e - (long long)r * K);
+    const int R = mat_rows(m), K = mat_k(m), CK = chunk_k(m);
+    const int total = R * K;
+    const int part = R * CK;  // floats of one part of a chunk
+    float* base = pack + w_off(m);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int r = e / K, k = e - r * K;
         int c = k;
         if (m < 3) {
             const int s = k / kFP, f = k - s * kFP;
             c = f < kF ? s * kF + f : cols;
         }
         const float x = (r < rows && c < cols) ? W[(long long)r * cols + c] : 0.f;
+        const int ch = k / CK, kk = k - ch * CK;
+        float* dst = base + (long long)ch * 2 * part + piece_off(r, kk >> 2, R) / 4 + (kk & 3);
         const float h = tf32_rna(x);
-        hi[e] = h;
-        lo[e] = x - h;
+        dst[0] = h;
+        dst[part] = x - h;
     }
 }
 
@@ -139,11 +147,10 @@ mlsrc_features(Dims d, const double* __restrict__ u, const double* __restrict__ 
                const double* __restrict__ w, float two_dx, float dx2,
                const float* __restrict__ norm, float* __restrict__ f_hi,
                float* __restrict__ f_lo) {
-    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;  // cells < 2^31 (checked)
     if (c >= d.n) return;
-    const int k = (int)(c % d.nz);
-    const long long r = c / d.nz;
-    const int j = (int)(r % d.ny), i = (int)(r / d.ny);
+    const int k = c % d.nz, r = c / d.nz;
+    const int j = r % d.ny, i = r / d.ny;
     const int ip = wrap(i + 1, d.nx), im = wrap(i - 1, d.nx);
     const int jp = wrap(j + 1, d.ny), jm = wrap(j - 1, d.ny);
     const int kp = wrap(k + 1, d.nz), km = wrap(k - 1, d.nz);
@@ -164,8 +171,8 @@ mlsrc_features(Dims d, const double* __restrict__ u, const double* __restrict__ 
         x[12 + 3 * q + 1] = (yp - 2.f * a + ym) / dx2;
         x[12 + 3 * q + 2] = (zp - 2.f * a + zm) / dx2;
     }
-    float4* oh = reinterpret_cast<float4*>(f_hi + c * kFP);
-    float4* ol = reinterpret_cast<float4*>(f_lo + c * kFP);
+    float4* oh = reinterpret_cast<float4*>(f_hi + (long long)c * kFP);
+    float4* ol = reinterpret_cast<float4*>(f_lo + (long long)c * kFP);
 #pragma unroll
     for (int q = 0; q < kFP / 4; ++q) {
         float h[4], l[4];
@@ -182,28 +189,35 @@ mlsrc_features(Dims d, const double* __restrict__ u, const double* __restrict__ 
 }
 
 // --- layers ---------------------------------------------------------------------
+// Activation tiles (the A operand of layers 2-4): per tile of 128 cells, per K
+// chunk of 40, the hi parts of the 128 rows and then the lo parts, each in the
+// core-matrix order of the shared-memory operand (one flat copy per chunk).
+constexpr int kActChunk = 2 * kTile * 40;       // floats of one chunk (both parts)
+constexpr int kActTile = 5 * kActChunk;         // floats of one tile (K = 200)
+// Gate tiles: per tile, column-major [208][128] FP32, so the lanes of a warp
+// (consecutive cells) touch consecutive addresses in the epilogues.
+constexpr int kGateTile = kNP * kTile;
+
 struct LayerMat {
-    const float* w;       // hi part of the packed matrix (lo follows)
+    const float* w;       // the matrix in the pack (chunk-tiled TF32 pairs)
     const float* bias;
-    const float* gate;    // kEpiGatedSplit: (n, 200) gate values
-    float* out_hi;
-    float* out_lo;        // second half of a split output
+    const float* gate;    // kEpiGatedSplit: gate tiles
+    float* out;           // activation tiles, gate tiles or (kEpiLinear) (n, 16) rows
     int epi;
 };
 
 struct LayerArgs {
     LayerMat m[3];        // blockIdx.y selects
-    const float* a_hi;    // A rows: feature rows (layer 1) or activation rows
+    const float* a_hi;    // layer 1: feature rows (hi, lo); later: activation tiles
     const float* a_lo;
     Dims d;
 };
 
 // layer-1 stencil: the cell, then +1/-1 along x, y, z, then +2/-2
-__device__ __forceinline__ long long stencil_cell(const Dims& d, long long c, int s) {
+__device__ __forceinline__ int stencil_cell(const Dims& d, int c, int s) {
     if (s == 0) return c;
-    const int k = (int)(c % d.nz);
-    const long long r = c / d.nz;
-    const int j = (int)(r % d.ny), i = (int)(r / d.ny);
+    const int k = c % d.nz, r = c / d.nz;
+    const int j = r % d.ny, i = r / d.ny;
     const int sh = s <= 6 ? 1 : 2;
     const int t = (s - 1) % 6;           // 0 +x, 1 -x, 2 +y, 3 -y, 4 +z, 5 -z
     const int dlt = (t & 1) ? -sh : sh;
@@ -211,7 +225,7 @@ __device__ __forceinline__ long long stencil_cell(const Dims& d, long long c, in
     const int ii = ax == 0 ? pmod(i + dlt, d.nx) : i;
     const int jj = ax == 1 ? pmod(j + dlt, d.ny) : j;
     const int kk = ax == 2 ? pmod(k + dlt, d.nz) : k;
-    return idx(d, ii, jj, kk);
+    return (int)idx(d, ii, jj, kk);
 }
 
 template <int KC, int NP>
@@ -222,9 +236,17 @@ struct LayerGeom {
     static constexpr int kTmemCols = NP <= 32 ? 32 : NP <= 64 ? 64 : NP <= 128 ? 128 : 256;
 };
 
+// stages, barriers, bias, layer-1 neighbour table
 template <int KC, int NP, bool GATHER>
 constexpr size_t layer_smem() {
-    return 2 * LayerGeom<KC, NP>::kStage + 64 + (GATHER ? kPts * kTile * 8 : 0);
+    return 2 * LayerGeom<KC, NP>::kStage + 64 + kNP * 4 + (GATHER ? kPts * kTile * 4 : 0);
+}
+
+// flat 16-byte copy of `bytes` (a multiple of 16) by all threads
+__device__ __forceinline__ void copy_flat(uint8_t* dst, const float* src, int bytes, int tid) {
+    const uint8_t* s8 = reinterpret_cast<const uint8_t*>(src);
+#pragma unroll 4
+    for (int o = tid * 16; o < bytes; o += kThreads * 16) cp_async_sm<16>(dst + o, s8 + o);
 }
 
 // KC K steps of 8 per chunk, NCH chunks, MMA N = NP.  GATHER: A rows are the
@@ -234,30 +256,30 @@ __global__ void __launch_bounds__(kThreads, 1)
 mlsrc_layer(LayerArgs args, int* __restrict__ err) {
     using G = LayerGeom<KC, NP>;
     constexpr int K = NCH * KC * 8;       // B row length
-    constexpr int AROW = GATHER ? kFP : kH;
     constexpr int QA = 2 * KC;            // 16-byte pieces of one row per chunk
     static_assert(!GATHER || (KC * 8 == kFP && NCH == kPts), "layer-1 chunking");
-    static_assert(GATHER || K == kH, "dense K");
+    static_assert(GATHER || (K == kH && KC * 8 == 40), "dense chunking");
     extern __shared__ __align__(1024) uint8_t smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * G::kStage);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
-    long long* nbr = reinterpret_cast<long long*>(smem + 2 * G::kStage + 64);
+    float* sbias = reinterpret_cast<float*>(smem + 2 * G::kStage + 64);
+    int* nbr = reinterpret_cast<int*>(sbias + kNP);
 
     const LayerMat& M = args.m[blockIdx.y];
     const Dims d = args.d;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const long long tile0 = (long long)blockIdx.x * kTile;
-    const long long last = d.n - 1;
-    const float* __restrict__ w_hi = M.w;
-    const float* __restrict__ w_lo = M.w + (long long)NP * K;
+    const int tile = blockIdx.x;
+    const int tile0 = tile * kTile;
+    const int last = (int)d.n - 1;
 
     if (GATHER) {
 #pragma unroll 1
         for (int e = tid; e < kPts * kTile; e += kThreads) {
             const int s = e / kTile, r = e - s * kTile;
-            nbr[e] = stencil_cell(d, std::min(tile0 + r, last), s);
+            nbr[e] = stencil_cell(d, min(tile0 + r, last), s);
         }
     }
+    for (int e = tid; e < NP; e += kThreads) sbias[e] = M.bias[e];
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -271,22 +293,19 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
 
     auto load_chunk = [&](int c, int stage) {
         uint8_t* sA = smem + stage * G::kStage;
-        uint8_t* sB = sA + 2 * G::kAPart;
+        if (GATHER) {
 #pragma unroll 4
-        for (int e = tid; e < 2 * kTile * QA; e += kThreads) {
-            const int q = e % QA, r = (e / QA) % kTile, part = e / (QA * kTile);
-            long long row;
-            if (GATHER) row = nbr[c * kTile + r] * AROW;
-            else row = std::min(tile0 + r, last) * AROW + c * KC * 8;
-            const float* src = (part ? args.a_lo : args.a_hi) + row + q * 4;
-            cp_async_sm<16>(sA + part * G::kAPart + piece_off(r, q, kTile), src);
+            for (int e = tid; e < 2 * kTile * QA; e += kThreads) {
+                const int q = e % QA, r = (e / QA) % kTile, part = e / (QA * kTile);
+                const float* src = (part ? args.a_lo : args.a_hi) +
+                                   (long long)nbr[c * kTile + r] * kFP + q * 4;
+                cp_async_sm<16>(sA + part * G::kAPart + piece_off(r, q, kTile), src);
+            }
+        } else {
+            copy_flat(sA, args.a_hi + (long long)tile * kActTile + c * kActChunk, 2 * G::kAPart,
+                      tid);
         }
-#pragma unroll 4
-        for (int e = tid; e < 2 * NP * QA; e += kThreads) {
-            const int q = e % QA, r = (e / QA) % NP, part = e / (QA * NP);
-            const float* src = (part ? w_lo : w_hi) + (long long)r * K + c * KC * 8 + q * 4;
-            cp_async_sm<16>(sB + part * G::kBPart + piece_off(r, q, NP), src);
-        }
+        copy_flat(sA + 2 * G::kAPart, M.w + (long long)c * (2 * NP * KC * 8), 2 * G::kBPart, tid);
     };
 
     constexpr uint32_t idesc = instr_desc(kFmtTF32, kTile, NP);
@@ -333,45 +352,49 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
         // warp w reads TMEM lane quarter w % 4 (cells 32 (w % 4) ..) and
         // every fourth 16-column group from group w / 4
         const int row = (warp & 3) * 32 + (tid & 31);
-        const long long cell = tile0 + row;
-        const bool valid = cell < d.n;
+        const int cell = tile0 + row;
         const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
         const int ncol = M.epi == kEpiLinear ? kNO : kH;
-        const int ld = M.epi == kEpiLinear ? kNO : kH;
+        float* const act = M.out + (long long)tile * kActTile;     // split outputs
+        float* const gto = M.out + (long long)tile * kGateTile;    // gate outputs
+        const float* const gti = M.gate + (long long)tile * kGateTile;
 #pragma unroll 1
         for (int c0 = 16 * (warp >> 2); c0 < NP; c0 += 64) {
             float y[16];
             tmem_ld16(taddr + c0, y);  // every lane of the warp takes part
-            if (!valid) continue;
-            const int cn = std::min(16, ncol - c0);
+            const int cn = min(16, ncol - c0);
             if (cn <= 0) continue;
-            float* oh = M.out_hi + cell * ld + c0;
-            float* ol = M.out_lo ? M.out_lo + cell * ld + c0 : nullptr;
-            const float* gt = M.gate ? M.gate + cell * kH + c0 : nullptr;
+            if (M.epi == kEpiLinear) {
+                if (cell > last) continue;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (4 * q >= cn) break;
-                float hv[4], lv[4];
-                float4 g4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (M.epi == kEpiGatedSplit) g4 = *reinterpret_cast<const float4*>(gt + 4 * q);
-                const float gv[4] = {g4.x, g4.y, g4.z, g4.w};
+                for (int q = 0; q < 4; ++q)
+                    *reinterpret_cast<float4*>(M.out + (long long)cell * kNO + c0 + 4 * q) =
+                        make_float4(y[4 * q] + sbias[c0 + 4 * q], y[4 * q + 1] + sbias[c0 + 4 * q + 1],
+                                    y[4 * q + 2] + sbias[c0 + 4 * q + 2],
+                                    y[4 * q + 3] + sbias[c0 + 4 * q + 3]);
+            } else if (M.epi == kEpiTanh) {
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const float a = y[4 * q + e] + M.bias[c0 + 4 * q + e];
-                    float h;
-                    if (M.epi == kEpiLinear) h = a;
-                    else if (M.epi == kEpiGatedSplit) h = tanhf(a) * gv[e];
-                    else h = tanhf(a);
-                    if (M.epi == kEpiTanhSplit || M.epi == kEpiGatedSplit) {
+                for (int e = 0; e < 16; ++e)
+                    if (e < cn) gto[(c0 + e) * kTile + row] = tanhf(y[e] + sbias[c0 + e]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (4 * q >= cn) break;
+                    float hv[4], lv[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int col = c0 + 4 * q + e;
+                        float h = tanhf(y[4 * q + e] + sbias[col]);
+                        if (M.epi == kEpiGatedSplit) h = h * gti[col * kTile + row];
                         hv[e] = tf32_rna(h);
                         lv[e] = h - hv[e];
-                    } else {
-                        hv[e] = h;
-                        lv[e] = 0.f;
                     }
+                    // column col = c0 + 4q .. +3 is K piece (col % 40) / 4 of chunk col / 40
+                    const int col = c0 + 4 * q, ch = col / 40, kk = col - ch * 40;
+                    float* dst = act + ch * kActChunk + piece_off(row, kk >> 2, kTile) / 4;
+                    *reinterpret_cast<float4*>(dst) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+                    *reinterpret_cast<float4*>(dst + kTile * 40) = make_float4(lv[0], lv[1], lv[2], lv[3]);
                 }
-                *reinterpret_cast<float4*>(oh + 4 * q) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-                if (ol) *reinterpret_cast<float4*>(ol + 4 * q) = make_float4(lv[0], lv[1], lv[2], lv[3]);
             }
         }
     } else {
@@ -410,11 +433,10 @@ __device__ __forceinline__ float div_term(const Dims& d, const float* P, int i, 
 __global__ void __launch_bounds__(256)
 mlsrc_terms(Dims d, const float* __restrict__ P, float two_dx, double* __restrict__ G,
             double* __restrict__ S) {
-    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= d.n) return;
-    const int k = (int)(c % d.nz);
-    const long long r = c / d.nz;
-    const int j = (int)(r % d.ny), i = (int)(r / d.ny);
+    const int k = c % d.nz, r = c / d.nz;
+    const int j = r % d.ny, i = r / d.ny;
     const double gx = (double)div_term(d, P, i, j, k, 0, two_dx);
     const double gy = (double)div_term(d, P, i, j, k, 3, two_dx);
     const double gz = (double)div_term(d, P, i, j, k, 6, two_dx);
@@ -431,10 +453,11 @@ mlsrc_terms(Dims d, const float* __restrict__ P, float two_dx, double* __restric
 
 // --- workspace --------------------------------------------------------------------
 struct Ws {
-    float *f_hi, *f_lo, *a_hi, *a_lo, *b_hi, *b_lo, *g1, *g2, *p;
+    float *f_hi, *f_lo, *act_a, *act_b, *g1, *g2, *p;
 };
 
 static size_t ws_layout(long long n, char* base, Ws* w) {
+    const long long ntiles = (n + kTile - 1) / kTile;
     size_t off = 0;
     auto take = [&](long long floats) {
         float* p = base ? reinterpret_cast<float*>(base + off) : nullptr;
@@ -444,12 +467,10 @@ static size_t ws_layout(long long n, char* base, Ws* w) {
     Ws t;
     t.f_hi = take(n * kFP);
     t.f_lo = take(n * kFP);
-    t.a_hi = take(n * kH);
-    t.a_lo = take(n * kH);
-    t.b_hi = take(n * kH);
-    t.b_lo = take(n * kH);
-    t.g1 = take(n * kH);
-    t.g2 = take(n * kH);
+    t.act_a = take(ntiles * kActTile);
+    t.act_b = take(ntiles * kActTile);
+    t.g1 = take(ntiles * kGateTile);
+    t.g2 = take(ntiles * kGateTile);
     t.p = take(n * kNO);
     if (w) *w = t;
     return off;
@@ -507,40 +528,37 @@ cudaError_t launch_mlsrc(const pf_grid* g, const double* u, const double* v, con
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const long long ntiles = (d.n + kTile - 1) / kTile;
-    auto mat = [&](int m, const float* gate, float* oh, float* ol, int epi) {
+    auto mat = [&](int m, const float* gate, float* out, int epi) {
         LayerMat M;
         M.w = pk + w_off(m);
         M.bias = pk + bias_off(m);
         M.gate = gate;
-        M.out_hi = oh;
-        M.out_lo = ol;
+        M.out = out;
         M.epi = epi;
         return M;
     };
-    // layer 1: H1 = tanh(fc1 x) (pair), gates tanh(fcG x), tanh(fcG2 x)
+    // layer 1: H1 = tanh(fc1 x) (pairs), gates tanh(fcG x), tanh(fcG2 x)
     LayerArgs a{};
-    a.m[0] = mat(0, nullptr, W.a_hi, W.a_lo, kEpiTanhSplit);
-    a.m[1] = mat(1, nullptr, W.g1, nullptr, kEpiTanh);
-    a.m[2] = mat(2, nullptr, W.g2, nullptr, kEpiTanh);
+    a.m[0] = mat(0, nullptr, W.act_a, kEpiTanhSplit);
+    a.m[1] = mat(1, nullptr, W.g1, kEpiTanh);
+    a.m[2] = mat(2, nullptr, W.g2, kEpiTanh);
     a.a_hi = W.f_hi;
     a.a_lo = W.f_lo;
     a.d = d;
     if ((e = launch_layer<3, kPts, kNP, true>(a, 3, ntiles, err, s, "mlsrc_layer1")))
         return e;
     // H2 = tanh(fc2 H1) * G1
-    a.m[0] = mat(3, W.g1, W.b_hi, W.b_lo, kEpiGatedSplit);
-    a.a_hi = W.a_hi;
-    a.a_lo = W.a_lo;
+    a.m[0] = mat(3, W.g1, W.act_b, kEpiGatedSplit);
+    a.a_hi = W.act_a;
+    a.a_lo = nullptr;
     if ((e = launch_layer<5, 5, kNP, false>(a, 1, ntiles, err, s, "mlsrc_layer2"))) return e;
     // H4 = tanh(fc3 H2) * G2
-    a.m[0] = mat(4, W.g2, W.a_hi, W.a_lo, kEpiGatedSplit);
-    a.a_hi = W.b_hi;
-    a.a_lo = W.b_lo;
+    a.m[0] = mat(4, W.g2, W.act_a, kEpiGatedSplit);
+    a.a_hi = W.act_b;
     if ((e = launch_layer<5, 5, kNP, false>(a, 1, ntiles, err, s, "mlsrc_layer3"))) return e;
     // out = fc4 H4 (outputs 0-15)
-    a.m[0] = mat(5, nullptr, W.p, nullptr, kEpiLinear);
-    a.a_hi = W.a_hi;
-    a.a_lo = W.a_lo;
+    a.m[0] = mat(5, nullptr, W.p, kEpiLinear);
+    a.a_hi = W.act_a;
     if ((e = launch_layer<5, 5, kNO, false>(a, 1, ntiles, err, s, "mlsrc_layer4"))) return e;
     PF_LAUNCH("mlsrc_terms", s,
               mlsrc_terms<<<pts, 256, 0, s>>>(d, W.p, two_dx, G, S));
@@ -572,6 +590,7 @@ extern "C" int pf_mlsrc_closure(const pf_grid* g, const double* u, const double*
     if (!g || g->nx < 5 || g->ny < 5 || g->nz < 5 || !(g->dx > 0) || !u || !v || !w ||
         !pack || !G || !S || !ws || !err)
         return PF_ERR_BAD_ARG;
+    if ((long long)g->nx * g->ny * g->nz >= (1LL << 31)) return PF_ERR_TOO_LARGE;
     if (((uintptr_t)pack & 15) != 0 || ((uintptr_t)ws & 255) != 0 ||
         ws_bytes < pf::mlsrc_ws_bytes(g))
         return PF_ERR_BAD_ARG;
