@@ -148,3 +148,49 @@ def step_roofline(ktimes, ncells, steps, step_ms):
     return {"bytes_per_step": per_step, "bytes_per_cell": per_step / ncells,
             "achieved": achieved, "peak": peak, "peak_source": src, "unit": "GB/s",
             "frac": achieved / peak}
+
+
+def closure_case(kind, n, reps=2, device="cuda"):
+    """A small seeded case of one closure kernel for profilers (ncu -k ...):
+    ``kind`` 'mlp' (the tensor-core MLP closure, pf_mlp_closure) or 'source'
+    (the reference's 'source' closure, pf_mlsrc_closure) on an n^3 grid of
+    the k0 = 4 spectral field, run ``reps`` times.  Returns the device error
+    flag.  Usage:
+        python -c "import pyflow_b200.profiling as p; p.closure_case('mlp', 128)"
+    """
+    import numpy as np
+    import torch
+    from . import initial as ic
+    u, v, w = (t.contiguous() for t in
+               ic.spectral_velocity_device((n, n, n), k0=4.0, seed=3, device=device))
+    sp = (2 * np.pi / n,) * 3
+    if kind == "mlp":
+        from . import sfsmodel_mlp as M
+        wp = torch.as_tensor(M.pack(M.xavier_init(1))).to(device)
+        res = None
+        for _ in range(reps):
+            res = M.closure(u, v, w, sp, wp, delta=sp[0], out=res[0] if res else None)
+        err = res[3]
+    elif kind == "source":
+        from . import sfsmodel_ML as ML
+
+        class _Geo:
+            type = "uniform"
+            dx = sp[0]
+
+        class _Dec:
+            pass
+
+        class _IC:
+            simDt = 0.01
+
+        _Dec.device = torch.device(device)
+        torch.manual_seed(0)
+        ml = ML.residual_stress(_IC(), _Dec(), _Geo(), model=ML.GatedClosureNet())
+        for _ in range(reps):
+            ml.update(u, v, w)
+        err = ml._err
+    else:
+        raise ValueError("kind must be 'mlp' or 'source'")
+    torch.cuda.synchronize(device)
+    return int(err.item())
