@@ -173,10 +173,14 @@ class BatchPlan:
 class StepPipeline:
     """Independent time steps on states that arrive in pinned host memory
     (a request stream), with the host<->device copies overlapped with the
-    computation: two field sets with one captured StepPlan each are used
-    alternately; host->device copies run on one copy stream and
+    computation: ``nsets`` field sets with one captured StepPlan each are
+    used in turn; host->device copies run on one copy stream and
     device->host copies on another (the two copy engines), so the input of
     request k+1 and the output of request k-1 move while request k computes.
+    A set is reused only after its previous request has been copied out, so
+    with two sets every pair of requests waits for one chain copy-in ->
+    step -> copy-out; three sets (the default) break that chain when the
+    copies take longer than the step, and the copy directions bound the rate.
     Ordering is by events only; nothing here synchronises the host.
 
     ``submit(u, v, w, p, stats_out, state_out=None)`` takes pinned host FP64
@@ -192,18 +196,21 @@ class StepPipeline:
     """
 
     def __init__(self, shape, spacing, mu, rho, dt, min_res=1e-10, max_it=20000,
-                 prec="fp64", rk4=True, device="cuda", stream=None):
+                 prec="fp64", rk4=True, device="cuda", stream=None, nsets=3):
         dev = torch.device(device)
+        if nsets < 1:
+            raise ValueError("nsets must be at least 1")
+        self.nsets = nsets
         self.sets = [[torch.zeros(shape, dtype=torch.float64, device=dev) for _ in range(5)]
-                     for _ in range(2)]
+                     for _ in range(nsets)]
         self.plans = [StepPlan(*f, spacing, mu, rho, dt, min_res=min_res, max_it=max_it,
                                prec=prec, rk4=rk4) for f in self.sets]
         self.compute = stream if stream is not None else torch.cuda.current_stream(dev)
         self.h2d = torch.cuda.Stream(dev)
         self.d2h = torch.cuda.Stream(dev)
-        self.ready = [torch.cuda.Event() for _ in range(2)]
-        self.done = [torch.cuda.Event() for _ in range(2)]
-        self.free = [torch.cuda.Event() for _ in range(2)]
+        self.ready = [torch.cuda.Event() for _ in range(nsets)]
+        self.done = [torch.cuda.Event() for _ in range(nsets)]
+        self.free = [torch.cuda.Event() for _ in range(nsets)]
         for e in self.free:
             e.record(self.compute)
         self.k = 0
@@ -213,7 +220,7 @@ class StepPipeline:
         self.d2h.wait_event(event)
 
     def submit(self, u, v, w, p, stats_out, state_out=None):
-        s = self.k & 1
+        s = self.k % self.nsets
         f = self.sets[s]
         # the set is free once its previous request has computed and copied out
         self.h2d.wait_event(self.free[s])

@@ -108,11 +108,12 @@ def test_plans_run_concurrently_on_streams():
         assert torch.equal(x, y)
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed_mg"])
-def test_pipeline_matches_plan(prec):
-    """StepPipeline (two field sets, host copies on a copy stream overlapped
-    with the previous request's step) returns, for each independent request,
-    bitwise the state and statistics of one StepPlan step on that request."""
+@pytest.mark.parametrize("prec,nsets", [("fp64", 3), ("mixed_mg", 3), ("mixed_mg", 2)])
+def test_pipeline_matches_plan(prec, nsets):
+    """StepPipeline (two or three field sets, host copies on copy streams
+    overlapped with the neighbouring requests' steps) returns, for each
+    independent request, bitwise the state and statistics of one StepPlan
+    step on that request."""
     import pyflow_b200.initial as ic
     from pyflow_b200.plan import StepPipeline, StepPlan
     shape = (24, 24, 32)
@@ -123,7 +124,8 @@ def test_pipeline_matches_plan(prec):
         u, v, w = ic.spectral_velocity(shape, k0=4.0, seed=20 + seed)
         p = np.random.default_rng(seed).standard_normal(shape)
         reqs.append([torch.tensor(a).pin_memory() for a in (u, v, w, p)])
-    pipe = StepPipeline(shape, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec)
+    pipe = StepPipeline(shape, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec,
+                        nsets=nsets)
     stats = [torch.zeros(10, dtype=torch.float64).pin_memory() for _ in reqs]
     states = [[torch.zeros(shape, dtype=torch.float64).pin_memory() for _ in range(4)]
               for _ in reqs]
