@@ -204,4 +204,142 @@ PF_HD inline void rhs_core(const Src& S, T mu, T rho, T dxi, T dyi, T dzi,
     if (xout) *xout = XFace<T>{fxx_c, fxy_c, fxz_c, cuu_p, cvu_p, cwu_p};
 }
 
+// ---------------------------------------------------------------------------
+// Face form of the same right-hand side (constant viscosity, no SFS stresses):
+// each cell computes the terms on its three plus faces once, and a cell's
+// minus-face terms are the plus-face terms of its neighbours at i-1, j-1 and
+// k-1 -- the same expressions on the same operands as rhs_core's minus terms,
+// so assembling them in rhs_core's order gives its result bit for bit.
+//   x-plus (XFace): fxx, fxy, fxz and the products u u, v u, w u
+//   y-plus (YFace): fxy, fyy, fyz and the products of u, v, w on the y face
+//   z-plus (ZFace): fxz, fyz, fzz and the products of u, v, w on the z face
+template <typename T>
+struct YFace {
+    T fxy, fyy, fyz, cuv, cvv, cwv;
+};
+
+template <typename T>
+struct ZFace {
+    T fxz, fyz, fzz, cuw, cvw, cww;
+};
+
+template <typename T>
+struct PlusFaces {
+    XFace<T> x;
+    YFace<T> y;
+    ZFace<T> z;
+};
+
+template <typename T>
+struct FluxCoef {
+    T dxi, dyi, dzi;
+    T two_mu_r;   // over_rho(2 mu): the diagonal fluxes' factor
+    T edge_r;     // over_rho(edge4(mu, mu, mu, mu)): the off-diagonal fluxes' factor
+};
+
+// rhs_core's scalar factors for constant viscosity (over_rho of the FP32 form
+// multiplies by 1/rho, the FP64 form divides)
+template <typename T>
+PF_HD inline FluxCoef<T> flux_coef(T mu, T rho, T dxi, T dyi, T dzi) {
+    constexpr bool f32 = sizeof(T) == 4;
+    const T irho = T(1) / rho;
+    auto over_rho = [&](T a) -> T { if constexpr (f32) return a * irho; else return a / rho; };
+    return FluxCoef<T>{dxi, dyi, dzi, over_rho(T(2.0) * mu), over_rho(edge4(mu, mu, mu, mu))};
+}
+
+template <typename T>
+PF_HD inline T div3_c(T ue, T uw, T vn, T vs, T wt, T wb, const FluxCoef<T>& c) {
+    const T s = (((ue - uw) * c.dxi) + ((vn - vs) * c.dyi)) + ((wt - wb) * c.dzi);
+    if constexpr (sizeof(T) == 4) return s * T(1.0f / 3.0f); else return s / T(3.0);
+}
+
+// Plus-face terms of one cell; with Y / Z false the y / z set is skipped (the
+// halo cells of a tile need only one set).  Uses the velocity at x, y, z
+// offsets 0 and +1 and, for the products, -1 in the other two directions.
+template <typename T, bool X = true, bool Y = true, bool Z = true, class Src>
+PF_HD inline PlusFaces<T> plus_faces(const Src& S, const FluxCoef<T>& c) {
+    const T h = T(0.5);
+    const T u_c = S.u(0, 0, 0), v_c = S.v(0, 0, 0), w_c = S.w(0, 0, 0);
+    const T u_xp = S.u(1, 0, 0), v_yp = S.v(0, 1, 0), w_zp = S.w(0, 0, 1);
+    const T D_c = div3_c(u_xp, u_c, v_yp, v_c, w_zp, w_c, c);
+    PlusFaces<T> f;
+    T fxy = T(0), fxz = T(0), fyz = T(0);
+    if (X || Y) {
+        const T u_yp = S.u(0, 1, 0), v_xp = S.v(1, 0, 0);
+        fxy = (((u_yp - u_c) * c.dyi) + ((v_xp - v_c) * c.dxi)) * c.edge_r;
+    }
+    if (X || Z) {
+        const T u_zp = S.u(0, 0, 1), w_xp = S.w(1, 0, 0);
+        fxz = (((u_zp - u_c) * c.dzi) + ((w_xp - w_c) * c.dxi)) * c.edge_r;
+    }
+    if (Y || Z) {
+        const T v_zp = S.v(0, 0, 1), w_yp = S.w(0, 1, 0);
+        fyz = (((v_zp - v_c) * c.dzi) + ((w_yp - w_c) * c.dyi)) * c.edge_r;
+    }
+    if (X) {
+        const T v_xp = S.v(1, 0, 0), w_xp = S.w(1, 0, 0);
+        const T cp = h * (u_xp + u_c);
+        const T vxp = h * (v_xp + v_c), uyp = h * (u_xp + S.u(1, -1, 0));
+        const T wxp = h * (w_xp + w_c), uzp = h * (u_xp + S.u(1, 0, -1));
+        f.x = XFace<T>{((u_xp - u_c) * c.dxi - D_c) * c.two_mu_r, fxy, fxz, cp * cp, vxp * uyp,
+                       wxp * uzp};
+    }
+    if (Y) {
+        const T u_yp = S.u(0, 1, 0), w_yp = S.w(0, 1, 0);
+        const T uyp = h * (u_yp + u_c), vxp = h * (v_yp + S.v(-1, 1, 0));
+        const T cp = h * (v_yp + v_c);
+        const T wyp = h * (w_yp + w_c), vzp = h * (v_yp + S.v(0, 1, -1));
+        f.y = YFace<T>{fxy, ((v_yp - v_c) * c.dyi - D_c) * c.two_mu_r, fyz, uyp * vxp, cp * cp,
+                       wyp * vzp};
+    }
+    if (Z) {
+        const T u_zp = S.u(0, 0, 1), v_zp = S.v(0, 0, 1);
+        const T uzp = h * (u_zp + u_c), wxp = h * (w_zp + S.w(-1, 0, 1));
+        const T vzp = h * (v_zp + v_c), wyp = h * (w_zp + S.w(0, -1, 1));
+        const T cp = h * (w_zp + w_c);
+        f.z = ZFace<T>{fxz, fyz, ((w_zp - w_c) * c.dzi - D_c) * c.two_mu_r, uzp * wxp, vzp * wyp,
+                       cp * cp};
+    }
+    return f;
+}
+
+// (ru, rv, rw) of a cell from its plus-face terms p and the plus-face terms of
+// its neighbours at i-1 (xm), j-1 (ym), k-1 (zm), in rhs_core's order
+template <typename T>
+PF_HD inline void assemble_faces(const PlusFaces<T>& p, const XFace<T>& xm, const YFace<T>& ym,
+                                 const ZFace<T>& zm, const FluxCoef<T>& c, T& ru_o, T& rv_o,
+                                 T& rw_o) {
+    const T dxi = c.dxi, dyi = c.dyi, dzi = c.dzi, one = T(1.0);
+    T ru = T(0), rv = T(0), rw = T(0);
+    ru = fma(dxi, p.x.fxx, ru); ru = fma(-dxi, xm.fxx, ru);
+    ru = fma(dyi, p.y.fxy, ru); ru = fma(-dyi, ym.fxy, ru);
+    ru = fma(dzi, p.z.fxz, ru); ru = fma(-dzi, zm.fxz, ru);
+    rv = fma(dxi, p.x.fxy, rv); rv = fma(-dxi, xm.fxy, rv);
+    rv = fma(dyi, p.y.fyy, rv); rv = fma(-dyi, ym.fyy, rv);
+    rv = fma(dzi, p.z.fyz, rv); rv = fma(-dzi, zm.fyz, rv);
+    rw = fma(dxi, p.x.fxz, rw); rw = fma(-dxi, xm.fxz, rw);
+    rw = fma(dyi, p.y.fyz, rw); rw = fma(-dyi, ym.fyz, rw);
+    rw = fma(dzi, p.z.fzz, rw); rw = fma(-dzi, zm.fzz, rw);
+    ru -= (p.x.cuu - xm.cuu) * dxi * one;
+    ru -= (p.y.cuv - ym.cuv) * dyi * one;
+    ru -= (p.z.cuw - zm.cuw) * dzi * one;
+    rv -= (p.x.cvu - xm.cvu) * dxi * one;
+    rv -= (p.y.cvv - ym.cvv) * dyi * one;
+    rv -= (p.z.cvw - zm.cvw) * dzi * one;
+    rw -= (p.x.cwu - xm.cwu) * dxi * one;
+    rw -= (p.y.cwv - ym.cwv) * dyi * one;
+    rw -= (p.z.cww - zm.cww) * dzi * one;
+    ru_o = ru; rv_o = rv; rw_o = rw;
+}
+
+// A source shifted by (a, b, c) cells: the neighbour's view of the same data
+template <class Src>
+struct Shifted {
+    const Src& s;
+    int a, b, c;
+    PF_HD auto u(int di, int dj, int dk) const { return s.u(di + a, dj + b, dk + c); }
+    PF_HD auto v(int di, int dj, int dk) const { return s.v(di + a, dj + b, dk + c); }
+    PF_HD auto w(int di, int dj, int dk) const { return s.w(di + a, dj + b, dk + c); }
+};
+
 }  // namespace pf

@@ -169,8 +169,20 @@ struct RhsSmem {
     static constexpr size_t kStg = kConv ? 4 * 3 * kRhsPos * sizeof(TI) : 0;             // [4][3][pos]
     static constexpr size_t kRing = 4 * 3 * kRhsPos * (kConv ? sizeof(T) : sizeof(TI)); // [4][3][pos]
     static constexpr size_t kEa = kA ? 2 * 3 * kRhsCells * sizeof(TA) : 0;               // [2][3][cells]
-    static constexpr size_t bytes = kEu + kStg + kRing + kEa;
+    // y-plus terms of the rows 2 ty - 1 (8 x 32) and z-plus terms of the
+    // halo column z = -1 (16 rows) of the face form
+    static constexpr size_t kFaces = ((8 * 32 * sizeof(YFace<T>) + kRhsTY * sizeof(ZFace<T>)) + 15) &
+                                     ~size_t(15);
+    static constexpr size_t bytes = kEu + kStg + kRing + kEa + kFaces;
 };
+
+template <typename T>
+__device__ __forceinline__ ZFace<T> shfl_up_z(const ZFace<T>& z) {
+    constexpr unsigned m = 0xffffffffu;
+    return ZFace<T>{__shfl_up_sync(m, z.fxz, 1), __shfl_up_sync(m, z.fyz, 1),
+                    __shfl_up_sync(m, z.fzz, 1), __shfl_up_sync(m, z.cuw, 1),
+                    __shfl_up_sync(m, z.cvw, 1), __shfl_up_sync(m, z.cww, 1)};
+}
 
 template <typename T, typename TI>
 struct SmemSrc {
@@ -187,6 +199,60 @@ struct SmemSrc {
     __device__ T visc(int, int, int) const { return T(0); }
     __device__ T sfs(int, int, int, int) const { return T(0); }
 };
+
+// The right-hand side of this thread's two cells of plane i (rows 2 ty and
+// 2 ty + 1, column tx of the tile) in the face form of pf_flux.cuh: every cell
+// computes its plus-face terms once; its x-minus terms are the x-plus terms
+// of the same cell on the previous plane (xf; on the tile's first plane they
+// are computed from plane i - 1), its y-minus terms those of the row below
+// (the thread's own first row, or through shared memory from thread ty - 1;
+// row -1 of the tile is computed by the first warp), its z-minus terms those
+// of the lane below (a shuffle; lane 0 reads the halo column z = -1, computed
+// by the second warp).  Bit-identical to rhs_core (checked on the host).
+// Every thread of the block must call it (it holds a block barrier); cells
+// outside the grid compute on wrapped data and are not stored.
+template <typename T, typename TI>
+__device__ __forceinline__ void
+rhs_plane_faces(const TI* ring, int s0, int s1, int s2, const FluxCoef<T>& fc, bool first,
+                XFace<T> (&xf)[2], YFace<T>* sY, ZFace<T>* sZh, T (&k3)[2][3]) {
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    PlusFaces<T> pf[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const SmemSrc<T, TI> src{ring, s0, s1, s2, 2 * ty + r + 1, tx + 1};
+        pf[r] = plus_faces<T>(src, fc);
+    }
+    if (ty < 7) sY[(ty + 1) * 32 + tx] = pf[1].y;
+    if (tid < 32) {            // row -1: its y-plus terms are the y-minus terms of row 0
+        const SmemSrc<T, TI> src{ring, s0, s1, s2, 0, tid + 1};
+        sY[tid] = plus_faces<T, false, true, false>(src, fc).y;
+    } else if (tid < 32 + kRhsTY) {  // column z = -1: z-plus terms for lane 0
+        const int row = tid - 32;
+        const SmemSrc<T, TI> src{ring, s0, s1, s2, row + 1, 0};
+        sZh[row] = plus_faces<T, false, false, true>(src, fc).z;
+    }
+    XFace<T> xm[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        if (first) {
+            const SmemSrc<T, TI> src{ring, s0, s1, s2, 2 * ty + r + 1, tx + 1};
+            const Shifted<SmemSrc<T, TI>> prev{src, -1, 0, 0};
+            xm[r] = plus_faces<T, true, false, false>(prev, fc).x;
+        } else {
+            xm[r] = xf[r];
+        }
+    }
+    ZFace<T> zm[2] = {shfl_up_z(pf[0].z), shfl_up_z(pf[1].z)};
+    __syncthreads();
+    if (tx == 0) {
+        zm[0] = sZh[2 * ty];
+        zm[1] = sZh[2 * ty + 1];
+    }
+    assemble_faces(pf[0], xm[0], sY[ty * 32 + tx], zm[0], fc, k3[0][0], k3[0][1], k3[0][2]);
+    assemble_faces(pf[1], xm[1], pf[0].y, zm[1], fc, k3[1][0], k3[1][1], k3[1][2]);
+    xf[0] = pf[0].x;
+    xf[1] = pf[1].x;
+}
 
 // The tiled stage for an FP64 input of an FP32 stage (first RK4 stage,
 // Euler's k): plane x's FP64 values arrive by cp.async in stg slot
@@ -207,6 +273,9 @@ rhs_tile_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
     extern __shared__ __align__(16) unsigned char smraw[];
     TI* stg = reinterpret_cast<TI*>(smraw);
     T* ring = reinterpret_cast<T*>(smraw + SM::kStg);
+    YFace<T>* sY = reinterpret_cast<YFace<T>*>(smraw + SM::kEu + SM::kStg + SM::kRing + SM::kEa);
+    ZFace<T>* sZh = reinterpret_cast<ZFace<T>*>(sY + 8 * 32);
+    const FluxCoef<T> fc = flux_coef<T>(a.mu, a.rho, a.dxi, a.dyi, a.dzi);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const long long plane = (long long)d.ny * d.nz;
     const TI* fld[3] = {a.u, a.v, a.w};
@@ -230,11 +299,12 @@ rhs_tile_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
             goff[p] = (long long)pmod(j0 + yy - 1, d.ny) * d.nz + pmod(k0 + zz - 1, d.nz);
             soff[p] = yy * kRhsSZ + zz;
         }
+        // this thread's owned cells: rows 2 ty and 2 ty + 1 of column tx
         bool cv[2];
         long long coff[2];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const int jl = ty + 8 * r;
+            const int jl = 2 * ty + r;
             cv[r] = tx < ez && jl < ey;
             coff[r] = (long long)(j0 + jl) * d.nz + k0 + tx;
         }
@@ -268,30 +338,23 @@ rhs_tile_conv(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a,
         convert(i0);
         convert(i0 + 1);
         __syncthreads();
-        XFace<T> xf[2];  // x-plus terms of this thread's two cells on the last plane
+        XFace<T> xf[2];  // x-plus terms of this thread's two cells on the previous plane
         for (int i = i0; i < i1; ++i) {
             const int c = i - i0;
             const int s0 = c & 3, s1 = (c + 1) & 3, s2 = (c + 2) & 3;
             if (i + 2 < i1) load_stg(i + 3);
             cp_async_commit();
+            T k3[2][3];
+            rhs_plane_faces<T, T>(ring, s0, s1, s2, fc, i == i0, xf, sY, sZh, k3);
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 if (!cv[r]) continue;
-                const int jl = ty + 8 * r;
-                SmemSrc<T, T> src{ring, s0, s1, s2, jl + 1, tx + 1};
-                T k3[3];
-                // the x-minus terms of plane i are the x-plus terms of plane i-1
-                if (i == i0)
-                    rhs_core<T, false>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
-                                       k3[0], k3[1], k3[2], nullptr, &xf[r]);
-                else
-                    rhs_core<T, true>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
-                                      k3[0], k3[1], k3[2], &xf[r], &xf[r]);
+                const int jl = 2 * ty + r;
                 const long long q = (long long)i * plane + coff[r];
                 const int pc = (jl + 1) * kRhsSZ + tx + 1;
 #pragma unroll
                 for (int f = 0; f < 3; ++f) {
-                    const T kf = k3[f];
+                    const T kf = k3[r][f];
                     if (MODE == kModeFirst) {
                         // ZAXPY(h, k, u) = h*k + u (src/data/state.py:157-165)
                         S[f][q] = TS(hdt * double(kf) + double(stg[(s1 * 3 + f) * kRhsPos + pc]));
@@ -322,6 +385,9 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
     double* eu = reinterpret_cast<double*>(smraw);
     TI* ring = reinterpret_cast<TI*>(smraw + SM::kEu);
     TA* ea = reinterpret_cast<TA*>(smraw + SM::kEu + SM::kRing);
+    YFace<T>* sY = reinterpret_cast<YFace<T>*>(smraw + SM::kEu + SM::kStg + SM::kRing + SM::kEa);
+    ZFace<T>* sZh = reinterpret_cast<ZFace<T>*>(sY + 8 * 32);
+    const FluxCoef<T> fc = flux_coef<T>(a.mu, a.rho, a.dxi, a.dyi, a.dzi);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const long long plane = (long long)d.ny * d.nz;
     const TI* fld[3] = {a.u, a.v, a.w};
@@ -346,12 +412,12 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
             goff[p] = (long long)pmod(j0 + yy - 1, d.ny) * d.nz + pmod(k0 + zz - 1, d.nz);
             soff[p] = yy * kRhsSZ + zz;
         }
-        // this thread's owned cells (rows ty, ty + 8) within the plane
+        // this thread's owned cells: rows 2 ty and 2 ty + 1 of column tx
         bool cv[2];
         long long coff[2];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const int jl = ty + 8 * r;
+            const int jl = 2 * ty + r;
             cv[r] = tx < ez && jl < ey;
             coff[r] = (long long)(j0 + jl) * d.nz + k0 + tx;
         }
@@ -370,7 +436,7 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 if (!cv[r]) continue;
-                const int c = (ty + 8 * r) * 32 + tx;
+                const int c = (2 * ty + r) * 32 + tx;
 #pragma unroll
                 for (int f = 0; f < 3; ++f) {
                     if (SM::kU) cp_async<8>(eu + (buf * 3 + f) * kRhsCells + c, U[f] + base + coff[r]);
@@ -387,7 +453,7 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
-        XFace<T> xf[2];  // x-plus terms of this thread's two cells on the last plane
+        XFace<T> xf[2];  // x-plus terms of this thread's two cells on the previous plane
         for (int i = i0; i < i1; ++i) {
             const int c = i - i0;
             const int s0 = c & 3, s1 = (c + 1) & 3, s2 = (c + 2) & 3;
@@ -397,24 +463,17 @@ rhs_tile(const Dims& d, const Tiling& tl, const RhsArgs<T, TI>& a, double* __res
                 load_epi(i + 1, buf ^ 1);
                 cp_async_commit();
             }
+            T k3[2][3];
+            rhs_plane_faces<T, TI>(ring, s0, s1, s2, fc, i == i0, xf, sY, sZh, k3);
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 if (!cv[r]) continue;
-                const int jl = ty + 8 * r;
-                SmemSrc<T, TI> src{ring, s0, s1, s2, jl + 1, tx + 1};
-                T k3[3];
-                // the x-minus terms of plane i are the x-plus terms of plane i-1
-                if (i == i0)
-                    rhs_core<T, false>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
-                                       k3[0], k3[1], k3[2], nullptr, &xf[r]);
-                else
-                    rhs_core<T, true>(src, a.mu, a.rho, a.dxi, a.dyi, a.dzi, false, false,
-                                      k3[0], k3[1], k3[2], &xf[r], &xf[r]);
+                const int jl = 2 * ty + r;
                 const long long q = (long long)i * plane + coff[r];
                 const int cc = jl * 32 + tx;
 #pragma unroll
                 for (int f = 0; f < 3; ++f) {
-                    const T kf = k3[f];
+                    const T kf = k3[r][f];
                     if (MODE == kModeFirst || MODE == kModeMid) {
                         // ZAXPY(h, k, u) = h*k + u (src/data/state.py:157-165)
                         S[f][q] = TS(hdt * double(kf) + eu[(buf * 3 + f) * kRhsCells + cc]);

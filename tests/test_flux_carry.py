@@ -1,8 +1,10 @@
-"""The RK4 stage kernels march along x and take each cell's x-minus flux terms
-from the x-plus terms of the cell before it (pf_flux.cuh, XFace).  This CPU
-test compiles the same per-cell routine for the host (tests/flux_carry_check.cpp)
-and checks that the carried march and the full evaluation agree bit for bit in
-FP64 and FP32 on small random periodic grids."""
+"""The RK4 stage kernels compute each face's flux terms once: a cell's x-minus
+terms are carried from the cell before it along the x march (XFace), its y- and
+z-minus terms are the plus-face terms of its neighbours (YFace, ZFace; the face
+form of pf_flux.cuh).  This CPU test compiles the same per-cell routines for the
+host (tests/flux_carry_check.cpp) and checks that both forms agree bit for bit
+with the full evaluation (rhs_core) in FP64 and FP32 on small random periodic
+grids."""
 import os
 import shutil
 import subprocess
@@ -23,4 +25,5 @@ def test_x_face_carry_is_bit_identical(tmp_path):
                    check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "fp64 0 fp32 0" in r.stdout
+    assert "mismatches fp64 0 fp32 0" in r.stdout
+    assert "face mismatches fp64 0 fp32 0" in r.stdout
