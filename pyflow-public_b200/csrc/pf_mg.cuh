@@ -43,7 +43,19 @@ struct MgPlan {
     // Krylov vectors (FP32, finest grid); p is double-buffered
     float *res, *res0, *p[2], *v, *s, *t, *ph, *sh, *e;
     float* pinv = nullptr;  // coarsest-level pseudo-inverse (small coarsest levels)
+    // one-thread-per-cell levels G .. C-1 (G < C) run as two cooperative
+    // launches per V-cycle with grid barriers (coop != 0, opt-in through
+    // PF_MG_COOP=1; bit-identical to the per-level kernels): coop_grid blocks,
+    // barrier words gbar[0..3] (arrivals, generation, failure; zeroed by
+    // mg_enqueue_setup and restored by every barrier)
+    int G = 0;
+    int coop = 0;
+    int coop_grid = 0;
+    unsigned* gbar = nullptr;
 };
+
+// Bytes of the grid-barrier words (a slot of their own).
+constexpr size_t kMgBarrierBytes = 256;
 
 // Level hierarchy of grid g (no memory touched).  Returns the number of
 // levels and sets *bottom; 0 when the finest level is itself at most

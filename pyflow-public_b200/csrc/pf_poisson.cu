@@ -980,7 +980,7 @@ size_t step_plan_ws_bytes(const pf_grid* g, int prec) {
     size_t r = std::max(std::max(predictor_ws_bytes(g, prec), vecs), stats_ws_bytes(g));
     // PF_MIXED_MG: the coarsest level's pseudo-inverse in a slot of its own
     // (the region r is reused by the predictor every step), computed once
-    const size_t pinv = prec == PF_MIXED_MG ? kPlanPinvBytes : 0;
+    const size_t pinv = prec == PF_MIXED_MG ? kPlanPinvBytes + kMgBarrierBytes : 0;
     return align256(n * sizeof(double)) + align256(sizeof(BicgScalars)) +
            align256(kNumPartials * kMaxPartials * sizeof(double)) + align256(r) + pinv;
 }
@@ -1024,7 +1024,11 @@ static int plan_layout(const pf_grid* g, int prec, void* ws, PlanLayout* L) {
         // the pseudo-inverse lives in the last slot of the workspace, outside
         // the region the predictor overwrites, and is computed once here
         if (L->mg.L && L->mg.pinv)
-            L->mg.pinv = (float*)((char*)ws + step_plan_ws_bytes(g, prec) - kPlanPinvBytes);
+            L->mg.pinv = (float*)((char*)ws + step_plan_ws_bytes(g, prec) - kPlanPinvBytes -
+                                  kMgBarrierBytes);
+        // the grid-barrier words too: the region is rewritten every step
+        if (L->mg.L)
+            L->mg.gbar = (unsigned*)((char*)ws + step_plan_ws_bytes(g, prec) - kMgBarrierBytes);
     }
     return PF_OK;
 }
@@ -1289,6 +1293,10 @@ int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, vo
     int rc = PF_OK;
     for (int r = 0; r < count && rc == PF_OK; ++r) rc = plan_layout(&m[r].grid, prec, m[r].ws, &P[r]);
     if (rc != PF_OK) { delete[] P; return rc; }
+    // the requests' solves run as parallel branches: their mid levels stay on
+    // the per-level kernels (no grid-barrier launches that could wait on one
+    // another for room on the SMs)
+    for (int r = 0; r < count; ++r) P[r].mg.coop = 0;
     if (predictor_prepare(prec) != cudaSuccess) { delete[] P; return PF_ERR_CUDA; }
     cudaStream_t cs;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {

@@ -87,3 +87,78 @@ def test_mg_forward_steps_match_fp64():
         assert float((x - y).abs().max()) <= 1e-7 * float(y.abs().max())
     div = ops.div_vel(*out["mixed_mg"][:3], sp)
     assert float(div.abs().max()) < 1e-8
+
+
+_COOP_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, {repo!r})
+import pyflow_b200.ops as ops
+from pyflow_b200.plan import StepPlan
+import pyflow_b200.initial as ic
+out = {{}}
+for n in (64, 128):
+    g = torch.Generator().manual_seed(n)
+    src = torch.randn((n, n, n), generator=g, dtype=torch.float64).cuda()
+    src -= src.mean()
+    sp = (2 * np.pi / n,) * 3
+    DP = torch.zeros_like(src); p = torch.zeros_like(src)
+    ops.bicgstab_solve(src, DP, p, sp, 1.0, 0.01, 1e-10, 2000, prec="mixed_mg")
+    torch.cuda.synchronize()
+    out["solve%d" % n] = DP.cpu().numpy()
+n = 128
+u, v, w = (torch.tensor(a, device="cuda") for a in ic.spectral_velocity((n, n, n), seed=4))
+f = [u, v, w, torch.zeros_like(u), torch.zeros_like(u)]
+plan = StepPlan(*f, (2 * np.pi / n,) * 3, 0.005, 1.0, 0.0025, prec="mixed_mg")
+plan.launch(3)
+torch.cuda.synchronize()
+plan.close()
+for k, t in zip("uvwp", f[:4]):
+    out["step_" + k] = t.cpu().numpy()
+np.savez({path!r}, **out)
+"""
+
+
+def test_mg_cooperative_mid_levels_bit_identical(tmp_path):
+    """The one-thread-per-cell levels as two cooperative launches per V-cycle
+    (PF_MG_COOP=1) and as per-level kernels (default) give bit-identical
+    solves (64^3, 128^3, host-driven) and steps (128^3, captured plan)."""
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for mode in ("1", "0"):
+        path = str(tmp_path / ("coop%s.npz" % mode))
+        env = dict(os.environ, PF_MG_COOP=mode)
+        r = subprocess.run([sys.executable, "-c", _COOP_SCRIPT.format(repo=repo, path=path)],
+                           env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-3000:]
+        res[mode] = np.load(path)
+    for k in res["1"].files:
+        assert np.array_equal(res["1"][k], res["0"][k]), k
+
+
+def test_mg_cooperative_path_runs(monkeypatch):
+    """With PF_MG_COOP=1, the host-driven mixed_mg solve at 128^3 launches the
+    cooperative mid levels (two per V-cycle) and no per-level kernels of
+    those levels."""
+    import pyflow_b200.ops as ops
+    import pyflow_b200.profiling as prof
+    monkeypatch.setenv("PF_MG_COOP", "1")
+    n = 128
+    g = torch.Generator().manual_seed(1)
+    src = torch.randn((n, n, n), generator=g, dtype=torch.float64).cuda()
+    src -= src.mean()
+    sp = (2 * np.pi / n,) * 3
+    DP = torch.zeros_like(src)
+    p = torch.zeros_like(src)
+    prof.enable(True)
+    info = ops.bicgstab_solve(src, DP, p, sp, 1.0, 0.01, 1e-10, 2000, prec="mixed_mg")
+    torch.cuda.synchronize()
+    kt = prof.read()
+    prof.enable(False)
+    assert info.status == 0
+    assert kt.get("mg_mid_down", {}).get("launches", 0) > 0
+    assert kt["mg_mid_down"]["launches"] == kt["mg_mid_up"]["launches"]
+    assert "mg_smooth0_pw" not in kt and "mg_prolong_smooth_pw" not in kt
+    assert _true_residual(src, DP, sp) <= 1e-10
