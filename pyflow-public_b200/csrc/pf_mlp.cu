@@ -6,22 +6,25 @@
 // accumulation; its six outputs times out_scale are the stresses FXX, FYY, FZZ,
 // FXY, FXZ, FYZ of the 'tensor' SFS slot (src/solver/velocity.py:262-267,...).
 //
-// CTAs of 128 threads (4 warps, three CTAs per SM) walk tiles of 128
-// consecutive cells; cell m of a tile is accumulator row / TMEM lane m and
-// belongs to thread m:
+// One CTA of 512 threads per SM: four warpgroups, each with its own H tile,
+// mbarrier and 128 of the SM's 512 TMEM columns, walk tiles of 128
+// consecutive cells independently (named barriers per warpgroup) and share
+// one copy of the weights; cell m of a warpgroup's tile is accumulator row /
+// TMEM lane m and belongs to the warpgroup's thread m:
 //   1. each thread computes its cell's gradients and writes 16 BF16 features
 //      (9 + 7 zero pads) into the X tile in shared memory (the first 4 KB of
 //      the H tile);
-//   2. thread 0 issues tcgen05.mma (M=128, N=128, K=16): D1 = X W1^T;
+//   2. the warpgroup's thread 0 issues tcgen05.mma (M=128, N=128, K=16):
+//      D1 = X W1^T;
 //   3. each thread reads its D1 row from TMEM (tcgen05.ld, 32 columns per
 //      wait), adds b1, truncates pairs of pre-activations to BF16, applies
 //      the packed BF16 tanh and writes them into the H tile;
 //   4. 8 tcgen05.mma (K=16 each): D2 = H W2^T; same epilogue back into H;
 //   5. 8 tcgen05.mma with N=16: D3 = H W3^T; each thread adds b3 and writes
 //      its six stresses (FP64) to global memory.
-// The three layers accumulate one after another into the same 128 TMEM
-// columns (each epilogue has read its accumulator before the next layer is
-// issued).
+// The three layers accumulate one after another into the warpgroup's 128
+// TMEM columns (each epilogue has read its accumulator before the next layer
+// is issued).
 // Completion of each MMA group is signalled by tcgen05.commit to an mbarrier;
 // every wait on it is bounded and reports a timeout through an error flag.
 //
@@ -48,15 +51,16 @@ using namespace umma;
 
 constexpr int kHidden = 128;
 constexpr int kTile = 128;
-constexpr int kThreads = 128;      // one thread per accumulator row
-constexpr int kCtasPerSm = 3;      // three tiles in flight per SM
+constexpr int kThreads = 512;      // four warpgroups, one tile each
+constexpr int kCtasPerSm = 1;      // four tiles in flight per SM
+constexpr int kGroups = 4;
 constexpr int kW1Bytes = 4096;      // 128 x 16 bf16
 constexpr int kW2Bytes = 32768;     // 128 x 128 bf16
 constexpr int kW3Bytes = 4096;      // 16 x 128 bf16
 constexpr int kBiasBytes = (128 + 128 + 16) * 4;
 constexpr int kPackBytes = kW1Bytes + kW2Bytes + kW3Bytes + kBiasBytes;
 constexpr int kHBytes = 32768;      // 128 x 128 bf16; its first 4 KB hold the 128 x 16 X tile
-constexpr unsigned kTmemCols = 128; // the three layers' accumulators, one after another
+constexpr unsigned kTmemCols = 512; // 128 columns per warpgroup
 
 // byte offset of element (row r, col k) in a K-major no-swizzle tile whose
 // 16-wide K slices are `slice` bytes apart
@@ -212,24 +216,34 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     // X shares the first 4 KB of the H tile: layer 1 reads X before the
     // epilogue that writes H, and the next tile writes X after layer 3 has
     // read H
-    uint8_t* sH = reinterpret_cast<uint8_t*>(sB) + kBiasBytes;
-    uint8_t* sX = sH;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sH + kHBytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    uint8_t* sH0 = reinterpret_cast<uint8_t*>(sB) + kBiasBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sH0 + kGroups * kHBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kGroups);
 
     // thread `row` owns accumulator row / TMEM lane `row`: its features, its
     // 128 hidden columns in the epilogues and its outputs.  Warp w reads TMEM
     // lanes 32 w .. 32 w + 31.
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const int row = tid, half = 0;
+    const int tid = threadIdx.x, warp = tid >> 5, grp = tid >> 7;
+    const int row = tid & 127;  // the warpgroup's thread / TMEM lane
+    uint8_t* sH = sH0 + grp * kHBytes;
+    uint8_t* sX = sH;
+    uint64_t* bar = bars + grp;
+    auto gsync = [&]() { asm volatile("bar.sync %0, 128;" :: "r"(grp + 1) : "memory"); };
+    auto gsync_and = [&](bool v) -> bool {
+        int r;
+        asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\t"
+                     "bar.red.and.pred q, %2, 128, p;\n\tselp.b32 %0, 1, 0, q;\n\t}"
+                     : "=r"(r) : "r"((int)v), "r"(grp + 1) : "memory");
+        return r != 0;
+    };
     // weights: a straight copy of the packed image
     {
         const uint4* src = reinterpret_cast<const uint4*>(wpack);
         uint4* dst = reinterpret_cast<uint4*>(smem);
         for (int q = tid; q < kPackBytes / 16; q += blockDim.x) dst[q] = src[q];
     }
-    if (tid == 0) {
-        mbar_init(bar, 1);
+    if (tid < kGroups) {
+        mbar_init(&bars[tid], 1);
         mbar_init_fence();
     }
     if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
@@ -237,7 +251,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem = *tmem_slot + (uint32_t)(grp * 128);
     const uint32_t d1 = tmem, d2 = tmem, d3 = tmem;  // one 128-column accumulator
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     const float in_scale = scales[0], out_scale = scales[1];
@@ -246,15 +260,16 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
     bool ok = true;
     const long long ntiles = (d.n + kTile - 1) / kTile;
     CellNb nb;
-    if (half == 0) {
-        const long long c0 = (long long)blockIdx.x * kTile + row;
-        if (blockIdx.x < ntiles && c0 < d.n) load_nb(d, u, v, w, c0, nb);
+    const long long t0 = (long long)blockIdx.x * kGroups + grp, stride = (long long)gridDim.x * kGroups;
+    {
+        const long long c0 = t0 * kTile + row;
+        if (t0 < ntiles && c0 < d.n) load_nb(d, u, v, w, c0, nb);
     }
-    for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    for (long long t = t0; t < ntiles && ok; t += stride) {
         const long long cell = t * kTile + row;
         const bool valid = cell < d.n;
-        // ---- features -> X (row `row`, first half)
-        if (half == 0) {
+        // ---- features -> X (row `row`)
+        {
             double g[9];
             if (valid) nb_gradients(nb, dxi, dyi, dzi, g);
             uint32_t p[8];
@@ -270,28 +285,28 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
         }
         fence_async_smem();
         tc_fence_before();
-        __syncthreads();
+        gsync();
         // ---- layer 1
-        if (tid == 0) {
+        if (row == 0) {
             tc_fence_after();
             mma_bf16(d1, smem_desc(smem_u32(sX)), smem_desc(smem_u32(sW1)), id128, 0u);
             commit(bar);
         }
         // the next tile's neighbourhood loads run under this tile's layers
-        if (half == 0) {
-            const long long cn = (t + gridDim.x) * kTile + row;
-            if (t + gridDim.x < ntiles && cn < d.n) load_nb(d, u, v, w, cn, nb);
+        {
+            const long long cn = (t + stride) * kTile + row;
+            if (t + stride < ntiles && cn < d.n) load_nb(d, u, v, w, cn, nb);
         }
-        ok = __syncthreads_and(wait_phase(bar, phase));
+        ok = gsync_and(wait_phase(bar, phase));
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
         hidden_epilogue(lane_base + d1, sB, sH, row, 0);
         fence_async_smem();
         tc_fence_before();
-        __syncthreads();
+        gsync();
         // ---- layer 2
-        if (tid == 0) {
+        if (row == 0) {
             tc_fence_after();
 #pragma unroll 1
             for (int kb = 0; kb < 8; ++kb)
@@ -299,16 +314,16 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
                          id128, kb > 0 ? 1u : 0u);
             commit(bar);
         }
-        ok = __syncthreads_and(wait_phase(bar, phase));
+        ok = gsync_and(wait_phase(bar, phase));
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
         hidden_epilogue(lane_base + d2, sB + 128, sH, row, 0);
         fence_async_smem();
         tc_fence_before();
-        __syncthreads();
+        gsync();
         // ---- layer 3
-        if (tid == 0) {
+        if (row == 0) {
             tc_fence_after();
 #pragma unroll 1
             for (int kb = 0; kb < 8; ++kb)
@@ -316,11 +331,11 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
                          id16, kb > 0 ? 1u : 0u);
             commit(bar);
         }
-        ok = __syncthreads_and(wait_phase(bar, phase));
+        ok = gsync_and(wait_phase(bar, phase));
         phase ^= 1u;
         if (!ok) break;
         tc_fence_after();
-        if (half == 0) {
+        {
             float y[16];
             mlp::tmem_ld16(lane_base + d3, y);
             if (valid) {
@@ -331,12 +346,12 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
             }
         }
         tc_fence_before();
-        __syncthreads();
+        gsync();
     }
     if (!ok) {
         // an MMA group did not signal completion: record it, and give the
         // tensor core one more bounded wait before the TMEM is released
-        if (tid == 0) atomicExch(err, 1);
+        if (row == 0) atomicExch(err, 1);
         wait_phase(bar, phase ^ 1u);  // the phase whose wait gave up
     }
     tc_fence_before();
@@ -348,7 +363,7 @@ mlp_closure_kernel(Dims d, const double* __restrict__ u, const double* __restric
 }
 
 size_t mlp_smem_bytes() {
-    return (size_t)mlp::kPackBytes + mlp::kHBytes + 64;
+    return (size_t)mlp::kPackBytes + mlp::kGroups * mlp::kHBytes + 64;
 }
 
 cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
@@ -363,7 +378,7 @@ cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
         cudaError_t e = cudaFuncSetAttribute(mlp_closure_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        // the largest shared-memory carveout, so three CTAs fit on an SM
+        // the largest shared-memory carveout (170 KB per CTA)
         e = cudaFuncSetAttribute(mlp_closure_kernel,
                                  cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
@@ -374,11 +389,11 @@ cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long ntiles = (d.n + mlp::kTile - 1) / mlp::kTile;
-    // three CTAs per SM, so the tensor-core layers of some overlap the
-    // epilogues of the others: each holds 128 of the SM's 512 TMEM columns
-    // and ~73 KB of shared memory (a fourth would not fit in shared memory,
-    // so a TMEM allocation never has to wait for another CTA of this kernel)
-    const int grid = (int)std::min<long long>(ntiles, (long long)mlp::kCtasPerSm * sms);
+    // one CTA per SM (four tiles in flight, the layers of some overlapping
+    // the epilogues of the others; the weights are shared, 170 KB of shared
+    // memory and all 512 TMEM columns per CTA)
+    const int grid = (int)std::min<long long>((ntiles + mlp::kGroups - 1) / mlp::kGroups,
+                                              (long long)mlp::kCtasPerSm * sms);
     PF_LAUNCH("mlp_closure", s, mlp_closure_kernel<<<grid, mlp::kThreads, smem, s>>>(
         d, u, v, w, 1.0 / g->dx, 1.0 / g->dy, 1.0 / g->dz, (const uint8_t*)wpack, scales,
         out, err));
