@@ -79,6 +79,19 @@ struct SrcP {  // p' = res + beta (p - omega v), stored to p_new
     __device__ void store(long long q, float c) const { p_new[q] = c; }
 };
 
+// The p update of the first iteration of a pass (beta == 0): the same
+// expression with p = v = 0, which are not read (they hold nothing yet).
+struct SrcP0 {
+    static constexpr int kRows = 4;
+    const float* res;
+    float* p_new;
+    float beta, omega;
+    struct Raw { float r; };
+    __device__ Raw raw(long long q, int = 0, int = 0, int = 0) const { return Raw{res[q]}; }
+    __device__ float op(const Raw& a) const { return fmaf(beta, fmaf(-omega, 0.0f, 0.0f), a.r); }
+    __device__ void store(long long q, float c) const { p_new[q] = c; }
+};
+
 struct SrcS {  // s = res - alpha v, stored to s
     static constexpr int kRows = 4;
     const float *res, *v;
@@ -246,6 +259,25 @@ mg_smooth0(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc,
     if (sc->done) return;
     ph.src.setup(sc);
     sweep<float>(d, tl, cf, ph);
+}
+
+// The p update and first smoothing pass of M p; the first iteration of a
+// pass (beta == 0) reads neither p nor v.
+__global__ void __launch_bounds__(kBlock, 2)
+mg_smooth0_p(Dims d, Tiling tl, LapCoef<float> cf, const BicgScalars* sc,
+             PhaseSmooth0<SrcP> ph) {
+    pdl_wait();
+    if (sc->done) return;
+    ph.src.setup(sc);
+    if (ph.src.beta == 0.0f) {
+        PhaseSmooth0<SrcP0> p0{};
+        p0.src = SrcP0{ph.src.res, ph.src.p_new, ph.src.beta, ph.src.omega};
+        p0.x = ph.x;
+        p0.wd = ph.wd;
+        sweep<float>(d, tl, cf, p0);
+    } else {
+        sweep<float>(d, tl, cf, ph);
+    }
 }
 
 __global__ void __launch_bounds__(kBlock, 2)
@@ -1395,6 +1427,8 @@ mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
         return;
     }
     const float alpha = float(sc->alpha), omega = float(sc->omega);
+    // the first iteration of a pass starts from e = 0 (e is not read)
+    const bool first = sc->iter == 0;
     double dot = 0.0, mx = 0.0;
     auto cell = [&](float& ev, float phv, float shq, float sv, float tv, float r0, float& rv) {
         const float x = fmaf(alpha, phv, ev);
@@ -1408,7 +1442,7 @@ mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
     const long long n4 = d.n >> 2;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
-        float4 ev = reinterpret_cast<const float4*>(e)[i];
+        float4 ev = first ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : reinterpret_cast<const float4*>(e)[i];
         const float4 pv = reinterpret_cast<const float4*>(ph)[i];
         const float4 hv = reinterpret_cast<const float4*>(shv)[i];
         const float4 sv = reinterpret_cast<const float4*>(s)[i];
@@ -1424,7 +1458,7 @@ mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
     }
     for (long long q = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += stride) {
-        float ev = e[q], rv;
+        float ev = first ? 0.0f : e[q], rv;
         cell(ev, ph[q], shv[q], s[q], t[q], res0[q], rv);
         e[q] = ev;
         res[q] = rv;
@@ -1456,7 +1490,10 @@ mg_update(Dims d, BicgScalars* sc, double* part, float* e, const float* ph,
     }
 }
 
-// res = res0 = float(r / scale); e = p = v = 0; rho = (res, res0)
+// res = res0 = float(r / scale); rho = (res, res0).  e, p and v are not
+// cleared: the first iteration reads none of them (beta == 0 in the p
+// update, e = 0 in mg_update), and a pass that ends before its first
+// iteration folds nothing (fold_* skip iter == 0).
 __global__ void __launch_bounds__(kBlock)
 mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
         float* res, float* res0, float* e, float* p0, float* p1, float* v,
@@ -1475,7 +1512,6 @@ mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
     // aligned), then the tail
     const long long n4 = d.n >> 2;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
         const double2 a = reinterpret_cast<const double2*>(r)[2 * i];
         const double2 b = reinterpret_cast<const double2*>(r)[2 * i + 1];
@@ -1486,16 +1522,11 @@ mg_init(Dims d, BicgScalars* sc, double* part, const double* __restrict__ r,
         x.w = cell(b.y);
         reinterpret_cast<float4*>(res)[i] = x;
         reinterpret_cast<float4*>(res0)[i] = x;
-        reinterpret_cast<float4*>(e)[i] = z4;
-        reinterpret_cast<float4*>(p0)[i] = z4;
-        reinterpret_cast<float4*>(p1)[i] = z4;
-        reinterpret_cast<float4*>(v)[i] = z4;
     }
     for (long long q = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += stride) {
         const float x = cell(r[q]);
         res[q] = x; res0[q] = x;
-        e[q] = 0.0f; p0[q] = 0.0f; p1[q] = 0.0f; v[q] = 0.0f;
     }
     const double bs = block_sum<kBlock>(s, sh);
     const double bm = block_max<kBlock>(m, sh);
@@ -1837,7 +1868,7 @@ int mg_enqueue_iteration(const MgPlan& P, BicgScalars* sc, double* part, int k,
         PhaseSmooth0<SrcP> ph{};
         ph.src.res = P.res; ph.src.p_old = p_old; ph.src.v = P.v; ph.src.p_new = p_new;
         ph.x = P.ph; ph.wd = f.wd;
-        PF_LAUNCH("mg_smooth0_p", s, launch_pdl(mg_smooth0<SrcP>, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
+        PF_LAUNCH("mg_smooth0_p", s, launch_pdl(mg_smooth0_p, dim3(gt), dim3(blk), 0, s, f.d, f.tl, f.cf, sc, ph));
     }
     vcycle_tail(P, p_new, P.ph, sc, s);
     const int ga = tiled_grid(f.ta1);

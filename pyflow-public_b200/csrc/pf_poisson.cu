@@ -318,6 +318,9 @@ __global__ void __launch_bounds__(kBlock)
 fold_correction(Dims d, const BicgScalars* sc, const T* e, double* x, int guard = 0) {
     // graph mode: a pass that ended non-finite or in breakdown is discarded
     if (guard && (sc->status == PF_NONFINITE || sc->status == PF_BREAKDOWN)) return;
+    // a pass that stopped before its first iteration has e = 0 (and may not
+    // have written it)
+    if (sc->iter == 0) return;
     const double s = sc->scale;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += (long long)gridDim.x * blockDim.x)
@@ -901,6 +904,7 @@ fold_mixed(Dims d, const BicgScalars* sc, const float* e32, const double* e64, d
     const bool f64 = sc->use64 != 0;
     if (!f64 && (sc->status == PF_NONFINITE || sc->status == PF_BREAKDOWN)) return;
     if (f64 && sc->status == PF_NONFINITE) return;
+    if (sc->iter == 0) return;  // no iteration ran: e = 0, possibly unwritten
     const double s = sc->scale;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.n;
          q += (long long)gridDim.x * blockDim.x)
