@@ -6,6 +6,13 @@
 
 namespace pf {
 
+// Unique id of the CUDA context current on this thread (0 when none is).
+int context_id(unsigned long long* id);
+// Runs setup() once per (key, current CUDA context): kernel attributes and
+// symbol addresses belong to a context, not to a device (pf_ctx.cu).
+cudaError_t once_per_context(const void* key, cudaError_t (*setup)());
+
+
 cudaError_t launch_rhs(const pf_grid* g, int prec, const void* u,
                        const void* v, const void* w, const void* visc,
                        double mu, double rho, const void* sfs, void* ru,

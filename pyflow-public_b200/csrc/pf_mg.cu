@@ -1317,21 +1317,20 @@ static cudaError_t launch_cluster(const MgCluster& m, size_t smem, const float* 
 // Whether this device runs the plan's cluster kernel (shared memory within
 // kClusterSmemMax and at least one cluster resident); otherwise the split
 // levels fall back to the per-level kernels.
+static cudaError_t cluster_attrs() {
+    return cudaFuncSetAttribute(mg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kClusterSmemMax);
+}
+
 static bool cluster_usable(const MgPlan& P) {
     size_t fl = 0;
     cluster_params(P, &fl);
     const size_t bytes = fl * sizeof(float);
     if (bytes > kClusterSmemMax) return false;
-    static int dev_done[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !dev_done[dev]) {
-        if (cudaFuncSetAttribute(mg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kClusterSmemMax) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        dev_done[dev] = 1;
+    // once per CUDA context (function attributes belong to the context)
+    if (once_per_context((const void*)&cluster_attrs, &cluster_attrs) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
     }
     cudaLaunchAttribute at[2];
     const cudaLaunchConfig_t cfg = cluster_config(bytes, nullptr, at, false);
@@ -1627,6 +1626,20 @@ static bool async_attrs() {
            smem_attr(mg_at<TZ>, async_sweep_smem<kAsTY1, TZ, AsyncAt>());
 }
 
+// Dynamic shared-memory limits of the multigrid kernels.
+static cudaError_t mg_attrs() {
+    // the bottom levels (at most 4096 + 512 + 64 + ... cells, 3 arrays each)
+    // need more than the default 48 KiB of shared memory
+    const int bytes = int(sizeof(float) * (3 * (kMgBottomMax + kMgBottomMax / 7 + 64) +
+                                            kMgPinvMax * kMgPinvMax));
+    const cudaError_t e = cudaFuncSetAttribute(mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               bytes);
+    if (e != cudaSuccess) return e;
+    // the cp.async sweeps' plane rings (up to ~93 KiB)
+    if (async_attrs<32>() || async_attrs<64>()) return cudaErrorInvalidValue;
+    return cudaSuccess;
+}
+
 int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
     P->L = mg_levels(g, P->lv, &P->B);
     if (!P->L) return PF_ERR_BAD_ARG;
@@ -1636,21 +1649,10 @@ int mg_setup(const pf_grid* g, void* region, MgPlan* P) {
         for (int l = P->C; l < P->B; ++l) P->lv[l].kind = kMgPointwise;
         P->C = P->B;
     }
-    static int dev_done[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !dev_done[dev]) {
-        // the bottom levels (at most 4096 + 512 + 64 + ... cells, 3 arrays
-        // each) need more than the default 48 KiB of shared memory
-        const int bytes = int(sizeof(float) * (3 * (kMgBottomMax + kMgBottomMax / 7 + 64) +
-                                                kMgPinvMax * kMgPinvMax));
-        if (cudaFuncSetAttribute(mg_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 bytes) != cudaSuccess)
-            return PF_ERR_CUDA;
-        // the cp.async sweeps' plane rings (up to ~93 KiB)
-        if (async_attrs<32>() || async_attrs<64>()) return PF_ERR_CUDA;
-        dev_done[dev] = 1;
-    }
+    // once per CUDA context (function attributes belong to the context)
+    if (once_per_context((const void*)&mg_attrs, &mg_attrs) != cudaSuccess) return PF_ERR_CUDA;
     char* ptr = (char*)region;
     const size_t fb = align256(P->lv[0].d.n * sizeof(float));
     float** f[kMgFineVecs] = {&P->res, &P->res0, &P->p[0], &P->p[1], &P->v, &P->s,

@@ -366,24 +366,24 @@ size_t mlp_smem_bytes() {
     return (size_t)mlp::kPackBytes + mlp::kGroups * mlp::kHBytes + 64;
 }
 
+static cudaError_t mlp_attrs() {
+    cudaError_t e = cudaFuncSetAttribute(mlp_closure_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mlp_smem_bytes());
+    if (e != cudaSuccess) return e;
+    // the largest shared-memory carveout (170 KB per CTA)
+    return cudaFuncSetAttribute(mlp_closure_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared);
+}
+
 cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
                        const double* w, const void* wpack, const float* scales,
                        double* out, int* err, cudaStream_t s) {
     Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     const size_t smem = mlp_smem_bytes();
-    static bool attr[64] = {false};  // per device
-    int cur = 0;
-    cudaGetDevice(&cur);
-    if (cur < 0 || cur >= 64 || !attr[cur]) {
-        cudaError_t e = cudaFuncSetAttribute(mlp_closure_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {   // once per CUDA context (function attributes belong to the context)
+        const cudaError_t e = once_per_context((const void*)&mlp_attrs, &mlp_attrs);
         if (e != cudaSuccess) return e;
-        // the largest shared-memory carveout (170 KB per CTA)
-        e = cudaFuncSetAttribute(mlp_closure_kernel,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        if (cur >= 0 && cur < 64) attr[cur] = true;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);

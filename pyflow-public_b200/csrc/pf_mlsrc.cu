@@ -477,12 +477,20 @@ static size_t ws_layout(long long n, char* base, Ws* w) {
 }
 
 template <int KC, int NCH, int NP, bool GATHER>
+static cudaError_t layer_attrs() {
+    return cudaFuncSetAttribute(mlsrc_layer<KC, NCH, NP, GATHER>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)layer_smem<KC, NP, GATHER>());
+}
+
+template <int KC, int NCH, int NP, bool GATHER>
 static cudaError_t launch_layer(const LayerArgs& a, int nmat, long long ntiles, int* err,
                                 cudaStream_t s, const char* name) {
     auto kern = mlsrc_layer<KC, NCH, NP, GATHER>;
     const size_t smem = layer_smem<KC, NP, GATHER>();
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    // once per CUDA context (function attributes belong to the context)
+    cudaError_t e = once_per_context((const void*)&layer_attrs<KC, NCH, NP, GATHER>,
+                                     &layer_attrs<KC, NCH, NP, GATHER>);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)ntiles, (unsigned)nmat);
     PF_LAUNCH(name, s, kern<<<grid, kThreads, smem, s>>>(a, err));

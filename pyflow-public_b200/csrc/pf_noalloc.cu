@@ -18,7 +18,7 @@
 //     CUDA context (not per device), so the call looks the address up with
 //     cudaGetSymbolAddress once per context -- the first call in a context,
 //     with that context current -- and caches it under the context's unique
-//     id (cuCtxGetId).  A host application that makes its own context
+//     id (cuCtxGetId, pf::context_id).  A host application that makes its own context
 //     current, or a context destroyed and created again (cudaDeviceReset),
 //     therefore gets a fresh lookup, never a stale address.  The first call
 //     in a context may load the library's device code, so make it before any
@@ -31,8 +31,6 @@
 //     caller.
 //   * The call allocates nothing: no cudaMalloc, cudaFree or allocating
 //     library routine.
-#include <cuda.h>  // driver-API types only; the functions come from cudaGetDriverEntryPoint
-
 #include <mutex>
 
 #include "pf_common.cuh"
@@ -48,9 +46,6 @@ constexpr size_t kNoallocBytes = 8 * (size_t)kNoallocMaxCells * sizeof(double) +
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
-using CtxGetCurrentFn = CUresult (*)(CUcontext*);
-using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
-
 // scratch address per context id (a small ring: the oldest entry is reused
 // when a process has created more contexts than it holds)
 constexpr int kMaxContexts = 64;
@@ -61,36 +56,13 @@ struct CtxScratch {
 std::mutex g_noalloc_mu;
 CtxScratch g_noalloc_tab[kMaxContexts];
 int g_noalloc_used = 0, g_noalloc_next = 0;
-CtxGetCurrentFn g_ctx_current = nullptr;
-CtxGetIdFn g_ctx_id = nullptr;
-
-// Unique id of the context current on this thread (0 when none is current).
-int current_context_id(unsigned long long* id) {
-    *id = 0;
-    if (!g_ctx_current || !g_ctx_id) {
-        void* f1 = nullptr;
-        void* f2 = nullptr;
-        cudaDriverEntryPointQueryResult q1, q2;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) !=
-                cudaSuccess || q1 != cudaDriverEntryPointSuccess || !f1 ||
-            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) !=
-                cudaSuccess || q2 != cudaDriverEntryPointSuccess || !f2)
-            return PF_ERR_CUDA;
-        g_ctx_current = (CtxGetCurrentFn)f1;
-        g_ctx_id = (CtxGetIdFn)f2;
-    }
-    CUcontext c = nullptr;
-    if (g_ctx_current(&c) != CUDA_SUCCESS) return PF_ERR_CUDA;
-    if (c && g_ctx_id(c, id) != CUDA_SUCCESS) return PF_ERR_CUDA;
-    return PF_OK;
-}
 
 // Device address of the scratch array in the context the runtime uses on
 // this thread (looked up once per context).
 int noalloc_scratch(void** out) {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     unsigned long long id = 0;
-    int rc = current_context_id(&id);
+    int rc = pf::context_id(&id);
     if (rc != PF_OK) return rc;
     if (id != 0)
         for (int e = 0; e < g_noalloc_used; ++e)
@@ -102,7 +74,7 @@ int noalloc_scratch(void** out) {
     // the device's primary context current, as any runtime call would
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PF_ERR_CUDA;
-    if (id == 0 && ((rc = current_context_id(&id)) != PF_OK || id == 0)) return PF_ERR_CUDA;
+    if (id == 0 && ((rc = pf::context_id(&id)) != PF_OK || id == 0)) return PF_ERR_CUDA;
     g_noalloc_tab[g_noalloc_next] = CtxScratch{id, p};
     g_noalloc_next = (g_noalloc_next + 1) % kMaxContexts;
     if (g_noalloc_used < kMaxContexts) ++g_noalloc_used;

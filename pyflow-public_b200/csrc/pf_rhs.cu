@@ -573,13 +573,10 @@ rhs_stage_grouped(const StageJob<T, TI>* __restrict__ jobs, int njobs, long long
     }
 }
 
-// Sets the dynamic shared-memory limit of one tiled instance once per device.
+// Sets the dynamic shared-memory limit of one tiled instance, once per CUDA
+// context (function attributes belong to the context).
 template <typename T, typename TI, int MODE>
-static cudaError_t tiled_prepare() {
-    static bool done[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+static cudaError_t tiled_prepare_ctx() {
     cudaError_t e = cudaFuncSetAttribute(
         rhs_stage_tiled<T, TI, T, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)RhsSmem<T, TI, T, MODE>::bytes);
@@ -591,8 +588,13 @@ static cudaError_t tiled_prepare() {
         e = cudaFuncSetAttribute(rhs_stage_tiled<T, TI, T, T, MODE>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     }
-    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
+}
+
+template <typename T, typename TI, int MODE>
+static cudaError_t tiled_prepare() {
+    return once_per_context((const void*)&tiled_prepare_ctx<T, TI, MODE>,
+                            &tiled_prepare_ctx<T, TI, MODE>);
 }
 
 // Euler.step's update u += k dt (src/solver/advancer.py:49-57), applied after
@@ -719,11 +721,7 @@ static cudaError_t predictor_impl(const pf_grid* g, int rk4, double* u,
 // stage (rhs_stage_grouped over per-stage job tables in device memory).
 // ---------------------------------------------------------------------------
 template <typename T, typename TI, int MODE>
-static cudaError_t grouped_prepare() {
-    static bool done[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+static cudaError_t grouped_prepare_ctx() {
     const size_t sm = RhsSmem<T, TI, T, MODE>::bytes;
     cudaError_t e = cudaFuncSetAttribute(rhs_stage_grouped<T, TI, MODE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -733,8 +731,14 @@ static cudaError_t grouped_prepare() {
         e = cudaFuncSetAttribute(rhs_stage_grouped<T, TI, MODE>,
                                  cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     }
-    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
+}
+
+// once per CUDA context (function attributes belong to the context)
+template <typename T, typename TI, int MODE>
+static cudaError_t grouped_prepare() {
+    return once_per_context((const void*)&grouped_prepare_ctx<T, TI, MODE>,
+                            &grouped_prepare_ctx<T, TI, MODE>);
 }
 
 // Job of one request for one stage (the arguments the single-request
