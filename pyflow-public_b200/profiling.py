@@ -64,7 +64,9 @@ def bytes_per_cell(name):
         "mg_smooth0_p": 20, "mg_smooth0_s": 16, "mg_smooth_l0": 12,
         "mg_restrict_l0": 8.5, "mg_prolong_l0": 8.5, "mg_av": 12, "mg_at": 12,
         "mg_update": 32, "mg_init": 16, "fold_correction": 20,
-        "mixed_b_init": 24, "mixed_update": 20, "mixed_residual": 24,
+        # warm-started mixed solves: source in, b out (a cold start also
+        # clears DP: 24)
+        "mixed_b_init": 16, "mixed_update": 20, "mixed_residual": 24,
         "add_inplace": 24, "div_vel": 32, "vel_corr": 56, "stats": 24,
         "laplace_apply": 16, "jacobi_sweep": 24, "jacobi_prep": 24,
         "jacobi_residual": 16}
