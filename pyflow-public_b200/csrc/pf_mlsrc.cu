@@ -21,11 +21,13 @@
 //      stored as a TF32 pair, hi = value rounded to TF32 and lo = value - hi
 //      (exact), in rows of 24 floats (21 features + 3 zeros) per cell.
 //   2. mlsrc_layer: one CTA of 512 threads per (tile of 128 cells, weight
-//      matrix).  A loop over K chunks streams the A rows (layer 1: the feature
-//      rows of the 13 stencil neighbours, one neighbour per chunk; later
-//      layers: rows of the previous layer's activations) and the weight rows
-//      into shared memory with cp.async, two stages deep, while one thread
-//      issues three tcgen05.mma kind::tf32 per K step of 8,
+//      matrix), two CTAs per SM (256 TMEM columns each), so one CTA's
+//      epilogue overlaps the other's products.  A loop over K steps of 8
+//      streams the A rows (layer 1: eight features of one of the 13 stencil
+//      neighbours' feature rows; later layers: eight columns of the previous
+//      layer's activations) and the weight rows into shared memory with
+//      cp.async, four stages deep, while one thread issues three
+//      tcgen05.mma kind::tf32 per K step,
 //          D += A_lo B_hi + A_hi B_lo + A_hi B_hi,
 //      which keeps about 21 bits of every FP32 product (the dropped A_lo B_lo
 //      term and the TF32 truncation of the lo parts are below 2^-21 of the
@@ -95,9 +97,8 @@ __device__ __forceinline__ float tf32_rna(float x) {
 }
 
 // --- packing ------------------------------------------------------------------
-// K values per chunk of the layers' K loops: one stencil point (24) in layer 1,
-// 40 in the others
-__host__ __device__ constexpr int chunk_k(int m) { return m < 3 ? kFP : 40; }
+// K values per chunk of the layers' K loops: one MMA K step (8)
+__host__ __device__ constexpr int chunk_k(int) { return 8; }
 
 // W (rows x cols, row-major as torch stores nn.Linear.weight) into matrix m of
 // the pack: per K chunk, the TF32 hi parts of all rows and then the lo parts,
@@ -190,10 +191,11 @@ mlsrc_features(Dims d, const double* __restrict__ u, const double* __restrict__ 
 
 // --- layers ---------------------------------------------------------------------
 // Activation tiles (the A operand of layers 2-4): per tile of 128 cells, per K
-// chunk of 40, the hi parts of the 128 rows and then the lo parts, each in the
+// step of 8, the hi parts of the 128 rows and then the lo parts, each in the
 // core-matrix order of the shared-memory operand (one flat copy per chunk).
-constexpr int kActChunk = 2 * kTile * 40;       // floats of one chunk (both parts)
-constexpr int kActTile = 5 * kActChunk;         // floats of one tile (K = 200)
+constexpr int kActK = 8;                        // K values per chunk (one MMA K step)
+constexpr int kActChunk = 2 * kTile * kActK;    // floats of one chunk (both parts)
+constexpr int kActTile = (kH / kActK) * kActChunk;  // floats of one tile (K = 200)
 // Gate tiles: per tile, column-major [208][128] FP32, so the lanes of a warp
 // (consecutive cells) touch consecutive addresses in the epilogues.
 constexpr int kGateTile = kNP * kTile;
@@ -236,10 +238,10 @@ struct LayerGeom {
     static constexpr int kTmemCols = NP <= 32 ? 32 : NP <= 64 ? 64 : NP <= 128 ? 128 : 256;
 };
 
-// stages, barriers, bias, layer-1 neighbour table
-template <int KC, int NP, bool GATHER>
+// NS stages, barriers, bias, layer-1 neighbour table
+template <int KC, int NP, bool GATHER, int NS>
 constexpr size_t layer_smem() {
-    return 2 * LayerGeom<KC, NP>::kStage + 64 + kNP * 4 + (GATHER ? kPts * kTile * 4 : 0);
+    return NS * LayerGeom<KC, NP>::kStage + 64 + kNP * 4 + (GATHER ? kPts * kTile * 4 : 0);
 }
 
 // flat 16-byte copy of `bytes` (a multiple of 16) by all threads
@@ -249,20 +251,23 @@ __device__ __forceinline__ void copy_flat(uint8_t* dst, const float* src, int by
     for (int o = tid * 16; o < bytes; o += kThreads * 16) cp_async_sm<16>(dst + o, s8 + o);
 }
 
-// KC K steps of 8 per chunk, NCH chunks, MMA N = NP.  GATHER: A rows are the
-// feature rows of the stencil neighbours (chunk = stencil point).
-template <int KC, int NCH, int NP, bool GATHER>
-__global__ void __launch_bounds__(kThreads, 1)
+// KC K steps of 8 per chunk, NCH chunks, MMA N = NP, NS shared-memory
+// stages (the copies of chunk c + NS - 1 are issued while chunk c is
+// multiplied).  GATHER: A rows are the feature rows of the stencil neighbours
+// (chunk c = K step c % 3 of stencil point c / 3).
+template <int KC, int NCH, int NP, bool GATHER, int NS>
+__global__ void __launch_bounds__(kThreads, 2)
 mlsrc_layer(LayerArgs args, int* __restrict__ err) {
     using G = LayerGeom<KC, NP>;
     constexpr int K = NCH * KC * 8;       // B row length
     constexpr int QA = 2 * KC;            // 16-byte pieces of one row per chunk
-    static_assert(!GATHER || (KC * 8 == kFP && NCH == kPts), "layer-1 chunking");
-    static_assert(GATHER || (K == kH && KC * 8 == 40), "dense chunking");
+    static_assert(!GATHER || (KC == 1 && K == kK1), "layer-1 chunking");
+    static_assert(GATHER || (K == kH && KC * 8 == kActK), "dense chunking");
+    static_assert(NS >= 2 && NS <= 6 && NCH >= NS, "stages");
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * G::kStage);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
-    float* sbias = reinterpret_cast<float*>(smem + 2 * G::kStage + 64);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NS * G::kStage);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + NS);
+    float* sbias = reinterpret_cast<float*>(smem + NS * G::kStage + 64);
     int* nbr = reinterpret_cast<int*>(sbias + kNP);
 
     const LayerMat& M = args.m[blockIdx.y];
@@ -281,8 +286,7 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
     }
     for (int e = tid; e < NP; e += kThreads) sbias[e] = M.bias[e];
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int q = 0; q < NS; ++q) mbar_init(&bar[q], 1);
         mbar_init_fence();
     }
     if (warp == 0) tmem_alloc(tmem_slot, G::kTmemCols);
@@ -297,8 +301,10 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
 #pragma unroll 4
             for (int e = tid; e < 2 * kTile * QA; e += kThreads) {
                 const int q = e % QA, r = (e / QA) % kTile, part = e / (QA * kTile);
+                // chunk c: K step c % 3 of stencil point c / 3
+                const int sp = c / 3, sub = c - 3 * sp;
                 const float* src = (part ? args.a_lo : args.a_hi) +
-                                   (long long)nbr[c * kTile + r] * kFP + q * 4;
+                                   (long long)nbr[sp * kTile + r] * kFP + sub * 8 + q * 4;
                 cp_async_sm<16>(sA + part * G::kAPart + piece_off(r, q, kTile), src);
             }
         } else {
@@ -310,20 +316,22 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
 
     constexpr uint32_t idesc = instr_desc(kFmtTF32, kTile, NP);
     bool ok = true;
-    load_chunk(0, 0);
-    cp_async_commit_group();
+#pragma unroll
+    for (int q = 0; q < NS - 1; ++q) {  // one copy group per chunk
+        load_chunk(q, q);
+        cp_async_commit_group();
+    }
 #pragma unroll 1
     for (int c = 0; c < NCH; ++c) {
-        const int stage = c & 1;
-        if (c + 1 < NCH) {
-            // the stage of chunk c+1 last held chunk c-1: wait for its MMAs
-            if (c >= 1) ok = ok && wait_phase(&bar[(c + 1) & 1], ((c - 1) >> 1) & 1, kSpin);
-            if (ok) load_chunk(c + 1, (c + 1) & 1);
-            cp_async_commit_group();
-            cp_async_wait_groups<1>();
-        } else {
-            cp_async_wait_groups<0>();
+        const int stage = c % NS;
+        const int nxt = c + NS - 1;
+        if (nxt < NCH) {
+            // the stage of chunk nxt last held chunk c - 1: wait for its MMAs
+            if (c >= 1) ok = ok && wait_phase(&bar[(c - 1) % NS], ((c - 1) / NS) & 1, kSpin);
+            if (ok) load_chunk(nxt, nxt % NS);
         }
+        cp_async_commit_group();
+        cp_async_wait_groups<NS - 1>();  // chunk c's copies have landed
         fence_async_smem();
         ok = __syncthreads_and(ok);
         if (!ok) break;
@@ -345,7 +353,7 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
         }
     }
     // MMAs complete in order: the last chunk's commit covers all of them
-    if (ok) ok = wait_phase(&bar[(NCH - 1) & 1], ((NCH - 1) >> 1) & 1, kSpin);
+    if (ok) ok = wait_phase(&bar[(NCH - 1) % NS], ((NCH - 1) / NS) & 1, kSpin);
     ok = __syncthreads_and(ok);
     if (ok) {
         tc_fence_after();
@@ -389,11 +397,12 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
                         hv[e] = tf32_rna(h);
                         lv[e] = h - hv[e];
                     }
-                    // column col = c0 + 4q .. +3 is K piece (col % 40) / 4 of chunk col / 40
-                    const int col = c0 + 4 * q, ch = col / 40, kk = col - ch * 40;
+                    // column col = c0 + 4q .. +3 is K piece (col % 8) / 4 of chunk col / 8
+                    const int col = c0 + 4 * q, ch = col / kActK, kk = col - ch * kActK;
                     float* dst = act + ch * kActChunk + piece_off(row, kk >> 2, kTile) / 4;
                     *reinterpret_cast<float4*>(dst) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-                    *reinterpret_cast<float4*>(dst + kTile * 40) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+                    *reinterpret_cast<float4*>(dst + kTile * kActK) =
+                        make_float4(lv[0], lv[1], lv[2], lv[3]);
                 }
             }
         }
@@ -401,8 +410,7 @@ mlsrc_layer(LayerArgs args, int* __restrict__ err) {
         // a wait gave up: record it, and give the tensor core one more
         // bounded wait for each stage before the TMEM is released
         if (tid == 0) atomicExch(err, 1);
-        wait_phase(&bar[0], 0, kSpin);
-        wait_phase(&bar[1], 0, kSpin);
+        for (int q = 0; q < NS; ++q) wait_phase(&bar[q], 0, kSpin);
         cp_async_wait_groups<0>();
     }
     tc_fence_before();
@@ -476,21 +484,21 @@ static size_t ws_layout(long long n, char* base, Ws* w) {
     return off;
 }
 
-template <int KC, int NCH, int NP, bool GATHER>
+template <int KC, int NCH, int NP, bool GATHER, int NS>
 static cudaError_t layer_attrs() {
-    return cudaFuncSetAttribute(mlsrc_layer<KC, NCH, NP, GATHER>,
+    return cudaFuncSetAttribute(mlsrc_layer<KC, NCH, NP, GATHER, NS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)layer_smem<KC, NP, GATHER>());
+                                (int)layer_smem<KC, NP, GATHER, NS>());
 }
 
-template <int KC, int NCH, int NP, bool GATHER>
+template <int KC, int NCH, int NP, bool GATHER, int NS>
 static cudaError_t launch_layer(const LayerArgs& a, int nmat, long long ntiles, int* err,
                                 cudaStream_t s, const char* name) {
-    auto kern = mlsrc_layer<KC, NCH, NP, GATHER>;
-    const size_t smem = layer_smem<KC, NP, GATHER>();
+    auto kern = mlsrc_layer<KC, NCH, NP, GATHER, NS>;
+    const size_t smem = layer_smem<KC, NP, GATHER, NS>();
     // once per CUDA context (function attributes belong to the context)
-    cudaError_t e = once_per_context((const void*)&layer_attrs<KC, NCH, NP, GATHER>,
-                                     &layer_attrs<KC, NCH, NP, GATHER>);
+    cudaError_t e = once_per_context((const void*)&layer_attrs<KC, NCH, NP, GATHER, NS>,
+                                     &layer_attrs<KC, NCH, NP, GATHER, NS>);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)ntiles, (unsigned)nmat);
     PF_LAUNCH(name, s, kern<<<grid, kThreads, smem, s>>>(a, err));
@@ -553,21 +561,21 @@ cudaError_t launch_mlsrc(const pf_grid* g, const double* u, const double* v, con
     a.a_hi = W.f_hi;
     a.a_lo = W.f_lo;
     a.d = d;
-    if ((e = launch_layer<3, kPts, kNP, true>(a, 3, ntiles, err, s, "mlsrc_layer1")))
+    if ((e = launch_layer<1, kK1 / 8, kNP, true, 4>(a, 3, ntiles, err, s, "mlsrc_layer1")))
         return e;
     // H2 = tanh(fc2 H1) * G1
     a.m[0] = mat(3, W.g1, W.act_b, kEpiGatedSplit);
     a.a_hi = W.act_a;
     a.a_lo = nullptr;
-    if ((e = launch_layer<5, 5, kNP, false>(a, 1, ntiles, err, s, "mlsrc_layer2"))) return e;
+    if ((e = launch_layer<1, kH / 8, kNP, false, 4>(a, 1, ntiles, err, s, "mlsrc_layer2"))) return e;
     // H4 = tanh(fc3 H2) * G2
     a.m[0] = mat(4, W.g2, W.act_a, kEpiGatedSplit);
     a.a_hi = W.act_b;
-    if ((e = launch_layer<5, 5, kNP, false>(a, 1, ntiles, err, s, "mlsrc_layer3"))) return e;
+    if ((e = launch_layer<1, kH / 8, kNP, false, 4>(a, 1, ntiles, err, s, "mlsrc_layer3"))) return e;
     // out = fc4 H4 (outputs 0-15)
     a.m[0] = mat(5, nullptr, W.p, kEpiLinear);
     a.a_hi = W.act_a;
-    if ((e = launch_layer<5, 5, kNO, false>(a, 1, ntiles, err, s, "mlsrc_layer4"))) return e;
+    if ((e = launch_layer<1, kH / 8, kNO, false, 4>(a, 1, ntiles, err, s, "mlsrc_layer4"))) return e;
     PF_LAUNCH("mlsrc_terms", s,
               mlsrc_terms<<<pts, 256, 0, s>>>(d, W.p, two_dx, G, S));
     return cudaGetLastError();
