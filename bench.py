@@ -585,6 +585,58 @@ def les_measurement(torch, dev, windows=3):
                     "through the stage-exact RK4 adjoint with recomputed stages"}
 
 
+def les_plan_measurement(torch, dev, n=64, steps=20):
+    """LES steps with the Smagorinsky closure (Cs = 0.18, Delta = dx) at the
+    LES size of the training workload (64^3, nu = 0.001, dt = 0.005), mixed
+    multigrid form: the closure inside the step graph (pf_step_plan_create_sfs)
+    against the host-driven composition of Domain.forwardStep (closure,
+    viscosity field, synchronous pf_forward_step), both from the same field,
+    CUDA events around the same number of steps."""
+    import pyflow_b200.ops as ops
+    from pyflow_b200.plan import StepPlan
+    u0, v0, w0 = (torch.tensor(x, device=dev)
+                  for x in make_fields({"n": n, "k0": 4.0, "seed": 1}))
+    sp = (2 * np.pi / n,) * 3
+    nu, dt = 0.001, 0.005
+    coef = (0.18 * sp[0]) ** 2
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f = [u0.clone(), v0.clone(), w0.clone(), torch.zeros_like(u0), torch.zeros_like(u0)]
+    plan = StepPlan(*f, sp, nu, 1.0, dt, min_res=TOL, max_it=MAX_IT, prec="mixed_mg",
+                    closure="smagorinsky", coef=coef)
+    plan.launch(3, stream=st)
+    plan.reset_counters()
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    plan.launch(steps, stream=st)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    graph_ms = e0.elapsed_time(e1) / steps
+    its = plan.stats()["total_iterations"] / steps
+    plan.close()
+    g = [u0.clone(), v0.clone(), w0.clone(), torch.zeros_like(u0), torch.zeros_like(u0)]
+
+    def host_step():
+        visc = (nu + ops.sgs_closure("smagorinsky", *g[:3], sp, coef=coef)).float()
+        ops.forward_step(*g, sp, nu, 1.0, dt, min_res=TOL, max_it=MAX_IT, prec="mixed_mg",
+                         warm=True, visc=visc)
+
+    for _ in range(3):
+        host_step()
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    for _ in range(steps):
+        host_step()
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    host_ms = e0.elapsed_time(e1) / steps
+    del f, g, u0, v0, w0
+    return {"grid": n, "closure": "smagorinsky", "prec": "mixed_mg", "steps": steps,
+            "graph_ms_per_step": graph_ms, "host_driven_ms_per_step": host_ms,
+            "iterations_per_step": its,
+            "graph_cell_steps_per_s": n ** 3 / (graph_ms / 1e3)}
+
+
 def run_serve(a, torch, dev):
     sv = serve_measurement(a, torch, dev)
     line = {"metric": "serve latency p50/p99 (s) and aggregate cell-steps/s",
@@ -656,7 +708,7 @@ def run_b200(a):
         torch.cuda.empty_cache()
 
     roof, ktimes, e2e, mlp, cpu, serve, les = None, {}, None, None, None, None, None
-    mlsrc = None
+    mlsrc = les_plan = None
     prof_steps = 2
     if not a.no_extras:
         # per-kernel device time: CUDA events around each launch of the
@@ -691,6 +743,8 @@ def run_b200(a):
             torch.cuda.empty_cache()
             mlsrc = ml_source_measurement(torch, dev)
             torch.cuda.empty_cache()
+            les_plan = les_plan_measurement(torch, dev)
+            torch.cuda.empty_cache()
             if not a.no_serve and world == 1:
                 serve = serve_measurement(a, torch, dev)
                 torch.cuda.empty_cache()
@@ -721,7 +775,7 @@ def run_b200(a):
             "fp64_arm": fp64, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * a.steps)) if launches_per_step else None,
             "clocks": clocks, "mlp_tensor_core": mlp, "ml_source_closure": mlsrc,
-            "serve": serve, "les_training": les,
+            "serve": serve, "les_training": les, "les_step_graph": les_plan,
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ktimes.items()},
         }
         print(json.dumps(line), flush=True)

@@ -269,6 +269,31 @@ int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u,
 int pf_step_plan_launch(pf_step_plan* plan, int nsteps, void* stream);
 int pf_step_plan_destroy(pf_step_plan* plan);
 
+/* pf_step_plan_create for LES: an SFS closure runs inside the graph at the
+ * start of every step, as the SFS pre-step of Domain.forwardStep
+ * (src/data/domain.py:347-355), and the RK4 stages read its field:
+ *   PF_CLOSURE_SMAGORINSKY: the viscosity field mu + coef |S|
+ *     (stress_constCs.eddyVisc, src/sfsmodel/sfsmodel_smagorinsky.py:65-88,
+ *     added to the molecular viscosity as src/data/domain.py:352 does;
+ *     coef = rho (Cs Delta)^2);
+ *   PF_CLOSURE_GRADIENT: the six 'tensor' stresses coef du_i/dx_k du_j/dx_k
+ *     (src/sfsmodel/sfsmodel_gradient.py:70-148; coef = dx^2/12).
+ * cfield: device buffer of pf_step_closure_bytes(g, prec, closure) bytes,
+ * 256-byte aligned, owned by the plan, that receives the field each step in
+ * the stages' type (double for PF_FP64, float for the mixed forms; the six
+ * stresses as consecutive fields FXX,FYY,FZZ,FXY,FXZ,FYZ).  Every step
+ * computes what pf_sgs_closure, the FP64 addition of mu, the conversion to
+ * the stage type and pf_forward_step with that visc or sfs compute, bit for
+ * bit (the mixed forms from a warm start, as pf_step_plan_create). */
+enum { PF_CLOSURE_SMAGORINSKY = 1, PF_CLOSURE_GRADIENT = 2 };
+size_t pf_step_closure_bytes(const pf_grid* g, int prec, int closure);
+int pf_step_plan_create_sfs(const pf_grid* g, int prec, int rk4, double* u,
+                            double* v, double* w, double* p, double* DP,
+                            double mu, double rho, double dt, double min_res,
+                            int max_it, int closure, double coef, void* cfield,
+                            size_t cfield_bytes, void* ws, size_t ws_bytes,
+                            double* stats, pf_step_plan** plan);
+
 /* NGA restart I/O from device memory (readNGArestart / writeNGArestart,
  * src/data/dataReader.py:119-208, whose MPI-IO path is :215-390): a restart
  * file stores each variable as an FP64 array in Fortran order (x fastest).

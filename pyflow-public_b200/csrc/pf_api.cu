@@ -181,7 +181,35 @@ int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* 
         return PF_ERR_BAD_ARG;
     void* h = nullptr;
     const int rc = step_plan_create(g, prec, rk4, u, v, w, p, DP, mu, rho, dt, min_res, max_it,
-                                    ws, stats, &h);
+                                    0, 0.0, nullptr, ws, stats, &h);
+    if (rc == PF_OK) *plan = (pf_step_plan*)h;
+    return rc;
+}
+
+size_t pf_step_closure_bytes(const pf_grid* g, int prec, int closure) {
+    if (!grid_ok(g) || !prec_ok(prec) || (closure != PF_CLOSURE_SMAGORINSKY &&
+                                          closure != PF_CLOSURE_GRADIENT))
+        return 0;
+    const size_t n = (size_t)g->nx * g->ny * g->nz;
+    const size_t fields = closure == PF_CLOSURE_SMAGORINSKY ? 1 : 6;
+    return fields * n * (prec == PF_FP64 ? sizeof(double) : sizeof(float));
+}
+
+int pf_step_plan_create_sfs(const pf_grid* g, int prec, int rk4, double* u, double* v,
+                            double* w, double* p, double* DP, double mu, double rho,
+                            double dt, double min_res, int max_it, int closure,
+                            double coef, void* cfield, size_t cfield_bytes, void* ws,
+                            size_t ws_bytes, double* stats, pf_step_plan** plan) {
+    if (!grid_ok(g) || !prec_ok(prec) || !u || !v || !w || !p || !DP || !stats || !plan ||
+        !(rho != 0.0) || !(dt != 0.0) || max_it < 1 || !cfield || ((uintptr_t)cfield & 255) ||
+        (closure != PF_CLOSURE_SMAGORINSKY && closure != PF_CLOSURE_GRADIENT) ||
+        cfield_bytes < pf_step_closure_bytes(g, prec, closure))
+        return PF_ERR_BAD_ARG;
+    if (!ws || ws_bytes < step_plan_ws_bytes(g, prec) || ((uintptr_t)ws & 255) != 0)
+        return PF_ERR_BAD_ARG;
+    void* h = nullptr;
+    const int rc = step_plan_create(g, prec, rk4, u, v, w, p, DP, mu, rho, dt, min_res, max_it,
+                                    closure, coef, cfield, ws, stats, &h);
     if (rc == PF_OK) *plan = (pf_step_plan*)h;
     return rc;
 }

@@ -74,10 +74,18 @@ cudaError_t launch_flow_stats(const pf_grid* g, const double* u, const double* v
                               cudaStream_t s);
 
 size_t step_plan_ws_bytes(const pf_grid* g, int prec);
+// SGS closure fields (pf_sgs_closure models 0-2) as FP64 (f32 false) or
+// float; model 0 adds `add` to coef |S|
+cudaError_t launch_sgs(const pf_grid* g, int model, const double* u,
+                       const double* v, const double* w, double coef,
+                       double add, void* out, bool f32, cudaStream_t s);
+
+// closure: 0 none, 1 Smagorinsky (cfield = mu + coef |S|), 2 gradient model
+// (cfield = six stresses), cfield in the stage type of prec
 int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
                      double* w, double* p, double* DP, double mu, double rho,
-                     double dt, double min_res, int max_it, void* ws,
-                     double* stats, void** out);
+                     double dt, double min_res, int max_it, int closure,
+                     double coef, void* cfield, void* ws, double* stats, void** out);
 int step_plan_launch(void* plan, int nsteps, cudaStream_t s);
 int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
                       void** out);

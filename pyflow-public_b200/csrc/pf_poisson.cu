@@ -1245,8 +1245,8 @@ static void plan_free(StepPlan* plan) {
 
 int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
                      double* w, double* p, double* DP, double mu, double rho,
-                     double dt, double min_res, int max_it, void* ws,
-                     double* stats, void** out) {
+                     double dt, double min_res, int max_it, int closure,
+                     double coef, void* cfield, void* ws, double* stats, void** out) {
     PlanLayout P;
     int rc = plan_layout(g, prec, ws, &P);
     if (rc != PF_OK) return rc;
@@ -1265,9 +1265,18 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
         if (cudaGraphCreate(&plan->graph, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
         cudaGraph_t G = plan->graph;
         cudaGraphNode_t n0, nend;
+        // the SFS pre-step (src/data/domain.py:347-355) reads the fields the
+        // previous step left; the stages read its field in their own type
+        const void* visc = closure == 1 ? cfield : nullptr;
+        const void* sfs = closure == 2 ? cfield : nullptr;
         if ((rc = add_captured(G, cs, [&](cudaStream_t st) {
-                 return launch_predictor(g, prec, rk4, u, v, w, nullptr, mu, rho, nullptr, dt,
-                                         P.R, st);
+                 if (closure) {
+                     const cudaError_t e = launch_sgs(g, closure - 1, u, v, w, coef,
+                                                      closure == 1 ? mu : 0.0, cfield,
+                                                      prec != PF_FP64, st);
+                     if (e != cudaSuccess) return e;
+                 }
+                 return launch_predictor(g, prec, rk4, u, v, w, visc, mu, rho, sfs, dt, P.R, st);
              }, &n0)))
             break;
         if ((rc = add_solve_chain(G, n0, g, prec, P, u, v, w, p, DP, rho, dt, min_res, max_it,

@@ -17,14 +17,18 @@
 
 namespace pf {
 
-// model 0: Smagorinsky mu_t = coef |S| (sfsmodel_smagorinsky.py:72-88)
+// model 0: Smagorinsky mu_t = coef |S| (sfsmodel_smagorinsky.py:72-88), plus
+//          `add` (the molecular viscosity when the field is the total one)
 // model 1: gradient model, six stresses (sfsmodel_gradient.py:77-148)
 // model 2: the nine gradients themselves (ux,uy,uz,vx,...,wz)
+// Every value is formed in FP64 and rounded once to T: for T = float that is
+// the FP64 closure field converted to the mixed forms' stage type.
+template <typename T>
 __global__ void __launch_bounds__(256)
 sgs_kernel(Dims d, int model, const double* __restrict__ u,
            const double* __restrict__ v, const double* __restrict__ w,
-           double dxi, double dyi, double dzi, double coef,
-           double* __restrict__ out) {
+           double dxi, double dyi, double dzi, double coef, double add,
+           T* __restrict__ out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int i = blockIdx.z;
@@ -39,28 +43,33 @@ sgs_kernel(Dims d, int model, const double* __restrict__ u,
         const double s23 = 0.5 * (g.vz + g.wy);
         const double smag = sqrt(((s11 * s11 + s22 * s22) + s33 * s33) +
                                  2.0 * ((s12 * s12 + s13 * s13) + s23 * s23));
-        out[q] = coef * smag;
+        out[q] = (T)(coef * smag + add);
     } else if (model == 1) {
-        out[q] = ((g.ux * g.ux + g.uy * g.uy) + g.uz * g.uz) * coef;
-        out[n + q] = ((g.vx * g.vx + g.vy * g.vy) + g.vz * g.vz) * coef;
-        out[2 * n + q] = ((g.wx * g.wx + g.wy * g.wy) + g.wz * g.wz) * coef;
-        out[3 * n + q] = ((g.ux * g.vx + g.uy * g.vy) + g.uz * g.vz) * coef;
-        out[4 * n + q] = ((g.ux * g.wx + g.uy * g.wy) + g.uz * g.wz) * coef;
-        out[5 * n + q] = ((g.vx * g.wx + g.vy * g.wy) + g.vz * g.wz) * coef;
+        out[q] = (T)(((g.ux * g.ux + g.uy * g.uy) + g.uz * g.uz) * coef);
+        out[n + q] = (T)(((g.vx * g.vx + g.vy * g.vy) + g.vz * g.vz) * coef);
+        out[2 * n + q] = (T)(((g.wx * g.wx + g.wy * g.wy) + g.wz * g.wz) * coef);
+        out[3 * n + q] = (T)(((g.ux * g.vx + g.uy * g.vy) + g.uz * g.vz) * coef);
+        out[4 * n + q] = (T)(((g.ux * g.wx + g.uy * g.wy) + g.uz * g.wz) * coef);
+        out[5 * n + q] = (T)(((g.vx * g.wx + g.vy * g.wy) + g.vz * g.wz) * coef);
     } else {
         const double a[9] = {g.ux, g.uy, g.uz, g.vx, g.vy, g.vz, g.wx, g.wy, g.wz};
 #pragma unroll
-        for (int c = 0; c < 9; ++c) out[c * n + q] = a[c];
+        for (int c = 0; c < 9; ++c) out[c * n + q] = (T)a[c];
     }
 }
 
 cudaError_t launch_sgs(const pf_grid* g, int model, const double* u,
                        const double* v, const double* w, double coef,
-                       double* out, cudaStream_t s) {
+                       double add, void* out, bool f32, cudaStream_t s) {
     Dims d{g->nx, g->ny, g->nz, (long long)g->nx * g->ny * g->nz};
     dim3 blk(32, 8), grd((d.nz + 31) / 32, (d.ny + 7) / 8, d.nx);
-    PF_LAUNCH("sgs_closure", s, sgs_kernel<<<grd, blk, 0, s>>>(
-        d, model, u, v, w, 1.0 / g->dx, 1.0 / g->dy, 1.0 / g->dz, coef, out));
+    const double dxi = 1.0 / g->dx, dyi = 1.0 / g->dy, dzi = 1.0 / g->dz;
+    if (f32)
+        PF_LAUNCH("sgs_closure_f32", s, sgs_kernel<float><<<grd, blk, 0, s>>>(
+            d, model, u, v, w, dxi, dyi, dzi, coef, add, (float*)out));
+    else
+        PF_LAUNCH("sgs_closure", s, sgs_kernel<double><<<grd, blk, 0, s>>>(
+            d, model, u, v, w, dxi, dyi, dzi, coef, add, (double*)out));
     return cudaGetLastError();
 }
 
@@ -72,6 +81,7 @@ extern "C" int pf_sgs_closure(const pf_grid* g, int model, const double* u,
     if (!g || g->nx < 2 || g->ny < 2 || g->nz < 2 || !(g->dx > 0) || !(g->dy > 0) ||
         !(g->dz > 0) || !u || !v || !w || !out || model < 0 || model > 2)
         return PF_ERR_BAD_ARG;
-    return pf::launch_sgs(g, model, u, v, w, coef, out, (cudaStream_t)stream) == cudaSuccess
-               ? PF_OK : PF_ERR_CUDA;
+    const cudaError_t e =
+        pf::launch_sgs(g, model, u, v, w, coef, 0.0, out, false, (cudaStream_t)stream);
+    return e == cudaSuccess ? PF_OK : PF_ERR_CUDA;
 }

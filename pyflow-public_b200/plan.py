@@ -22,6 +22,14 @@ _lib.pf_step_plan_create.argtypes = [
     ctypes.c_double] * 4 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
 _lib.pf_step_plan_create.restype = ctypes.c_int
+_lib.pf_step_closure_bytes.argtypes = [ctypes.POINTER(L.Grid), ctypes.c_int, ctypes.c_int]
+_lib.pf_step_closure_bytes.restype = ctypes.c_size_t
+_lib.pf_step_plan_create_sfs.argtypes = [
+    ctypes.POINTER(L.Grid), ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5 + [
+    ctypes.c_double] * 4 + [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                            ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+_lib.pf_step_plan_create_sfs.restype = ctypes.c_int
 _lib.pf_step_plan_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
 _lib.pf_step_plan_launch.restype = ctypes.c_int
 _lib.pf_step_plan_destroy.argtypes = [ctypes.c_void_p]
@@ -43,13 +51,22 @@ _lib.pf_batch_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER
 _lib.pf_batch_plan_create.restype = ctypes.c_int
 MAX_BATCH = 64
 
+# SFS closures a plan can evaluate inside its graph (pf_step_plan_create_sfs)
+CLOSURES = {"smagorinsky": 1, "gradient": 2}
+
 STAT_NAMES = ("max_u", "max_v", "max_w", "tke", "max_div", "max_res",
               "iterations", "status", "total_iterations", "steps")
 
 
 class StepPlan:
+    """One field set's step graph.  ``closure`` ('smagorinsky' or 'gradient',
+    with its ``coef`` as for ops.sgs_closure) adds the SFS pre-step of
+    Domain.forwardStep (src/data/domain.py:347-355) to the graph; its field
+    (the viscosity mu + coef|S|, or the six stresses) is ``self.cfield``, in
+    the stages' type."""
+
     def __init__(self, u, v, w, p, DP, spacing, mu, rho, dt, min_res=1e-10,
-                 max_it=20000, prec="fp64", rk4=True):
+                 max_it=20000, prec="fp64", rk4=True, closure=None, coef=0.0):
         for t, nm in ((u, "u"), (v, "v"), (w, "w"), (p, "p"), (DP, "DP")):
             ops._check(t, u.shape, torch.float64, nm)
         self.fields = (u, v, w, p, DP)
@@ -60,13 +77,26 @@ class StepPlan:
         self.stats_dev = torch.zeros(10, dtype=torch.float64, device=u.device)
         self.cells = u.numel()
         self._h = ctypes.c_void_p(0)
+        self.cfield = None
+        if closure is not None:
+            kind = CLOSURES[closure]
+            sdt = torch.float64 if pr == L.PF_FP64 else torch.float32
+            shape = tuple(u.shape) if kind == 1 else (6,) + tuple(u.shape)
+            self.cfield = torch.empty(shape, dtype=sdt, device=u.device)
+            assert self.cfield.numel() * self.cfield.element_size() == \
+                _lib.pf_step_closure_bytes(ctypes.byref(self.grid), pr, kind)
         # the fields must be ready: wait for the stream that produced them
         torch.cuda.current_stream(u.device).synchronize()
-        L.check("pf_step_plan_create", _lib.pf_step_plan_create(
-            ctypes.byref(self.grid), pr, 1 if rk4 else 0, *(ops._p(t) for t in self.fields),
-            float(mu), float(rho), float(dt), float(min_res), int(max_it),
-            ops._p(self.ws), self.ws.numel(), ops._p(self.stats_dev),
-            ctypes.byref(self._h)))
+        common = (ctypes.byref(self.grid), pr, 1 if rk4 else 0,
+                  *(ops._p(t) for t in self.fields), float(mu), float(rho), float(dt),
+                  float(min_res), int(max_it))
+        tail = (ops._p(self.ws), self.ws.numel(), ops._p(self.stats_dev), ctypes.byref(self._h))
+        if closure is None:
+            L.check("pf_step_plan_create", _lib.pf_step_plan_create(*common, *tail))
+        else:
+            L.check("pf_step_plan_create_sfs", _lib.pf_step_plan_create_sfs(
+                *common, kind, float(coef), ops._p(self.cfield),
+                self.cfield.numel() * self.cfield.element_size(), *tail))
 
     def launch(self, nsteps=1, stream=None):
         s = stream if stream is not None else torch.cuda.current_stream(self.ws.device)

@@ -80,3 +80,46 @@ def test_step_plan_workspace_sizes():
         # the coarsest level's pseudo-inverse and the grid-barrier words
         assert mg == mixed + 64 * 64 * 4 + 256
         assert mg % 256 == 0 and mixed % 256 == 0
+
+
+def test_step_closure_sizes_and_argument_checks():
+    """pf_step_closure_bytes: one field (Smagorinsky viscosity) or six
+    (gradient-model stresses) in the stages' type; pf_step_plan_create_sfs
+    rejects an unknown closure, a short or misaligned closure buffer before
+    any CUDA call."""
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(LIB)
+
+    class Grid(ctypes.Structure):
+        _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                    ("nz", ctypes.c_int), ("dx", ctypes.c_double),
+                    ("dy", ctypes.c_double), ("dz", ctypes.c_double)]
+
+    lib.pf_step_closure_bytes.restype = ctypes.c_size_t
+    lib.pf_step_closure_bytes.argtypes = [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int]
+    g = Grid(24, 20, 36, 0.1, 0.1, 0.1)
+    n = 24 * 20 * 36
+    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 1) == 8 * n
+    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 2) == 6 * 8 * n
+    assert lib.pf_step_closure_bytes(ctypes.byref(g), 2, 1) == 4 * n
+    assert lib.pf_step_closure_bytes(ctypes.byref(g), 1, 2) == 6 * 4 * n
+    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 3) == 0
+    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 0) == 0
+    P, D, I, S = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_size_t
+    lib.pf_step_plan_create_sfs.restype = I
+    lib.pf_step_plan_create_sfs.argtypes = [ctypes.POINTER(Grid), I, I] + [P] * 5 + [D] * 4 + [
+        I, I, D, P, S, P, S, P, ctypes.POINTER(P)]
+    fake = 1 << 20  # never dereferenced: every call below fails its checks first
+    h = P(0)
+
+    def create(closure, cfield, cbytes):
+        return lib.pf_step_plan_create_sfs(
+            ctypes.byref(g), 0, 1, fake, fake, fake, fake, fake, 0.01, 1.0, 0.001, 1e-10, 100,
+            closure, 0.001, cfield, cbytes, fake, 1 << 30, fake, ctypes.byref(h))
+
+    assert create(3, fake, 6 * 8 * n) == 1
+    assert create(1, fake, 8 * n - 8) == 1
+    assert create(1, fake + 16, 8 * n) == 1
+    assert create(2, None, 6 * 8 * n) == 1
+    assert h.value is None

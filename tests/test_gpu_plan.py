@@ -145,3 +145,56 @@ def test_pipeline_matches_plan(prec, nsets):
         # statistics of the step (the running totals 8, 9 differ by design)
         assert torch.equal(s_[:8], ref[:8])
         assert int(s_[7]) == 0
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed_mg"])
+@pytest.mark.parametrize("closure", ["smagorinsky", "gradient"])
+def test_plan_sfs_matches_forward_step(prec, closure):
+    """A plan with the SFS closure in its graph against the host-driven
+    composition of Domain.forwardStep (src/data/domain.py:347-367): the
+    closure by pf_sgs_closure, the FP64 addition of the molecular viscosity
+    (Smagorinsky), the conversion to the mixed forms' FP32 stage type, then
+    pf_forward_step with that visc or sfs.  Bit for bit in FP64; the mixed
+    form to the tolerance of test_plan_matches_forward_step.  The closure
+    field the plan leaves is the one of its last step, bit for bit."""
+    import pyflow_b200.initial as ic
+    import pyflow_b200.ops as ops
+    from pyflow_b200.plan import StepPlan
+    shape = (24, 20, 28)
+    sp = tuple(2 * np.pi / n for n in shape)
+    f0 = [torch.tensor(a, device="cuda") for a in ic.spectral_velocity(shape, k0=4.0, seed=9)]
+    nu, dt, steps = 0.004, 0.004, 4
+    coef = (0.18 * sp[0]) ** 2 if closure == "smagorinsky" else sp[0] ** 2 / 12.0
+    model = "smagorinsky" if closure == "smagorinsky" else "gradient"
+    a = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    for _ in range(steps):
+        fld = ops.sgs_closure(model, *a[:3], sp, coef=coef)
+        if closure == "smagorinsky":
+            fld = nu + fld
+        if prec != "fp64":
+            fld = fld.float()
+        kw = {"visc": fld} if closure == "smagorinsky" else {"sfs": fld.contiguous()}
+        info = ops.forward_step(*a, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec,
+                                warm=prec != "fp64", **kw)
+    b = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    plan = StepPlan(*b, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec,
+                    closure=closure, coef=coef)
+    plan.launch(steps)
+    torch.cuda.synchronize()
+    st = plan.stats()
+    assert plan.cfield.dtype == fld.dtype and torch.equal(plan.cfield, fld)
+    plan.close()
+    assert st["status"] == 0 and st["max_res"] <= 1e-10
+    assert int(st["iterations"]) == info.iterations
+    if prec == "fp64":
+        for x, y in zip(a[:4], b[:4]):
+            assert torch.equal(x, y)
+    else:
+        for x, y in zip(a[:3], b[:3]):
+            assert (x - y).abs().max().item() <= 1e-12 * y.abs().max().item()
+    # the closure acted: the step differs from the one without it
+    c = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    for _ in range(steps):
+        ops.forward_step(*c, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec,
+                         warm=prec != "fp64")
+    assert (c[0] - b[0]).abs().max().item() > 1e-9
