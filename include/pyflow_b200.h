@@ -294,6 +294,49 @@ int pf_step_plan_create_sfs(const pf_grid* g, int prec, int rk4, double* u,
                             size_t cfield_bytes, void* ws, size_t ws_bytes,
                             double* stats, pf_step_plan** plan);
 
+/* x-slab decomposition (replaces decomp and communicate_border,
+ * src/library/parallel.py:118-414, and comms.parallel_sum / parallel_max,
+ * :60-94, for a periodic box split along x over ranks).  A rank's fields are
+ * a LOCAL EXTENDED grid g: g->nx = halo + interior planes + halo, ny and nz
+ * the global ones, z fastest; plane `halo` is the first interior plane.  The
+ * caller moves ghost planes between neighbours (planes are contiguous) and
+ * gathers every rank's 2-double `send` buffer, in rank order, into `recv`
+ * (world x 2 doubles, device) -- the only communication of the solve.
+ * Kernels without reductions (pf_predictor_step, pf_div_vel, pf_vel_corr)
+ * run unchanged on g: with halo >= 4 ghost planes exchanged, a whole RK4
+ * predictor is exact on the interior.
+ *
+ * The pressure solve is solver_bicgstab.solve (src/solver/pressure.py:196-297)
+ * in FP64 with the reference's three reductions per iteration; scalars stay
+ * on the device and every rank folds the gathered values in rank order, so
+ * all ranks take the same branches.  One rank's loop:
+ *   pf_slab_bicg_init -> gather -> phase START;
+ *   repeat { exchange(pp, 1 plane) -> APPLY_P -> gather -> S ->
+ *            exchange(s, 1 plane) -> APPLY_S -> gather -> FINAL -> gather ->
+ *            NEXT }   until pf_slab_bicg_info reports done (after NEXT);
+ *   then pf_slab_add (p += DP), exchange(DP, 1 plane), pf_vel_corr.
+ * pp and s (the exchanged vectors) live in the workspace
+ * (pf_slab_bicg_vectors).  info: 4 device doubles [max_res, iterations,
+ * status, done].  After `done` the phases return at once, so ranks may poll
+ * every few iterations.  halo >= 1 for the solve. */
+enum {
+    PF_SLAB_START = 0,    /* fold the init gather; pp = res */
+    PF_SLAB_NEXT = 1,     /* fold the stop test and rho1; pp = (pp - w vv) b + res */
+    PF_SLAB_APPLY_P = 2,  /* vv = A pp; send = [(vv, res0), 0] */
+    PF_SLAB_S = 3,        /* fold gamma; DP += a pp; s = res - a vv */
+    PF_SLAB_APPLY_S = 4,  /* t = A s; send = [(s, t), (t, t)] */
+    PF_SLAB_FINAL = 5     /* fold omega; DP += w s; res = s - w t; send = [(res, res0), max|res|] */
+};
+size_t pf_slab_workspace_bytes(const pf_grid* g);
+int pf_slab_bicg_vectors(const pf_grid* g, void* ws, double** pp, double** s);
+int pf_slab_bicg_init(const pf_grid* g, int halo, double rho, double dt,
+                      double min_res, int max_it, const double* div, double* DP,
+                      void* ws, size_t ws_bytes, double* send, void* stream);
+int pf_slab_bicg_phase(const pf_grid* g, int halo, int phase, const double* recv,
+                       int world, double* DP, void* ws, double* send, void* stream);
+int pf_slab_bicg_info(const pf_grid* g, void* ws, double* info, void* stream);
+int pf_slab_add(const pf_grid* g, int halo, const double* DP, double* p, void* stream);
+
 /* NGA restart I/O from device memory (readNGArestart / writeNGArestart,
  * src/data/dataReader.py:119-208, whose MPI-IO path is :215-390): a restart
  * file stores each variable as an FP64 array in Fortran order (x fastest).

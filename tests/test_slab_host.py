@@ -1,0 +1,115 @@
+"""Host logic of the x-slab decomposition (pyflow_b200.slab), on the CPU:
+the plane split against the reference's formula, the periodic extension of
+a global field, and the ghost exchange and gather of both transports --
+LocalSlabs in one process and DistSlabs over gloo with world sizes 2 and 3
+-- against the periodic extension.  No kernel runs here."""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _ref_split(nx, npx, iproc):
+    """The reference's x split, src/library/parallel.py:226-235."""
+    q, r = nx // npx, nx % npx
+    if iproc + 1 <= r:
+        return iproc * (q + 1), q + 1
+    return r * (q + 1) + (iproc - r) * q, q
+
+
+@pytest.mark.parametrize("nx,npx", [(16, 1), (16, 2), (17, 3), (64, 8), (30, 7)])
+def test_plane_ranges_match_reference_split(nx, npx):
+    from pyflow_b200.slab import plane_ranges
+    got = plane_ranges(nx, npx)
+    assert got == [_ref_split(nx, npx, i) for i in range(npx)]
+    assert sum(n for _, n in got) == nx
+
+
+def test_plane_ranges_rejects_too_many_ranks():
+    from pyflow_b200.slab import plane_ranges
+    with pytest.raises(ValueError):
+        plane_ranges(3, 4)
+
+
+def _global(nx=13, ny=3, nz=4):
+    return torch.arange(nx * ny * nz, dtype=torch.float64).reshape(nx, ny, nz)
+
+
+def test_extend_fills_ghosts_periodically():
+    from pyflow_b200.slab import extend
+    g = _global()
+    e = extend(g, 11, 2, halo=4)
+    assert e.shape == (10, 3, 4)
+    for a in range(10):
+        assert torch.equal(e[a], g[(11 - 4 + a) % 13])
+
+
+@pytest.mark.parametrize("R,planes", [(1, 4), (2, 1), (3, 4), (3, 2)])
+def test_local_exchange_equals_periodic_extension(R, planes):
+    from pyflow_b200.slab import HALO, LocalSlabs, extend, plane_ranges
+    g = _global(14)
+    rng = plane_ranges(14, R)
+    # interiors from the global field, ghosts poisoned
+    fields = []
+    for x0, n in rng:
+        e = torch.full((n + 2 * HALO, 3, 4), -1.0, dtype=torch.float64)
+        e[HALO:HALO + n] = g[x0:x0 + n]
+        fields.append([e, e.clone() * 2])
+    LocalSlabs(R).exchange(fields, [n for _, n in rng], planes)
+    for (x0, n), (a, b) in zip(rng, fields):
+        want = extend(g, x0, n)
+        lo, hi = HALO - planes, HALO + n + planes
+        assert torch.equal(a[lo:hi], want[lo:hi])
+        assert torch.equal(b[lo:hi], 2 * want[lo:hi])
+        # planes beyond the exchanged depth are untouched
+        assert bool((a[:lo] == -1.0).all()) and bool((a[hi:] == -1.0).all())
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _dist_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from pyflow_b200.slab import HALO, DistSlabs, extend, plane_ranges
+        T = DistSlabs()
+        nx = 4 * world + 3
+        g = _global(nx)
+        x0, n = plane_ranges(nx, world)[rank]
+        e = torch.full((n + 2 * HALO, 3, 4), -1.0, dtype=torch.float64)
+        e[HALO:HALO + n] = g[x0:x0 + n]
+        T.exchange([[e]], [n], HALO)
+        ok_x = torch.equal(e, extend(g, x0, n))
+        send = torch.tensor([float(rank), 10.0 * rank], dtype=torch.float64)
+        recv = torch.zeros(2 * world, dtype=torch.float64)
+        T.allgather([send], [recv])
+        want = torch.tensor([v for r in range(world) for v in (float(r), 10.0 * r)],
+                            dtype=torch.float64)
+        q.put((rank, bool(ok_x), bool(torch.equal(recv, want))))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+@pytest.mark.parametrize("world", [2, 3])
+def test_dist_exchange_and_gather_gloo(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_dist_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(150)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=5) for _ in range(world))
+    assert got == [(r, True, True) for r in range(world)]
