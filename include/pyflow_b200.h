@@ -235,8 +235,10 @@ int pf_sfs_adjoint(const pf_grid* g, const double* mu_u, const double* mu_v,
  * a plugin whose host application owns the whole device-memory budget, or a
  * loop that must not allocate after start-up).  Scratch is a fixed 16.25 MiB
  * array inside the library (held by every GPU that loads it); grids above
- * 64^3 = 262144 cells return PF_ERR_TOO_LARGE.  The first call on a device
- * looks up the array's device address, so make it before any stream capture.
+ * 64^3 = 262144 cells return PF_ERR_TOO_LARGE.  The array's device address
+ * is looked up once per CUDA context (keyed by the context's unique id), at
+ * the first call in that context, so make that call before any stream
+ * capture.
  * All calls share the array: calls that overlap on the GPU race.  Allocates
  * nothing.  Synchronous, like pf_bicgstab_solve. */
 int pf_bicgstab_solve_noalloc(const pf_grid* g, double rho, double dt,
