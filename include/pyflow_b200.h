@@ -184,6 +184,14 @@ int pf_sgs_closure(const pf_grid* g, int model, const double* u,
  * scales: 2 device floats; err: device int set to 1 if a tensor-core wait
  * timed out. */
 size_t pf_mlp_pack_bytes(void);
+/* The MLP closure's scales from the nine cell-centred gradients:
+ * g2 = their mean square (FP64, fixed summation order), scales[0] =
+ * 1/sqrt(g2), scales[1] = delta2 g2, each rounded once to float (device).
+ * ws: pf_mlp_scales_workspace_bytes() bytes, 256-byte aligned. */
+size_t pf_mlp_scales_workspace_bytes(void);
+int pf_mlp_scales(const pf_grid* g, const double* u, const double* v,
+                  const double* w, double delta2, float* scales, void* ws,
+                  size_t ws_bytes, void* stream);
 int pf_mlp_closure(const pf_grid* g, const double* u, const double* v,
                    const double* w, const void* wpack, const float* scales,
                    double* out, int* err, void* stream);
@@ -279,22 +287,35 @@ int pf_step_plan_destroy(pf_step_plan* plan);
  *     added to the molecular viscosity as src/data/domain.py:352 does;
  *     coef = rho (Cs Delta)^2);
  *   PF_CLOSURE_GRADIENT: the six 'tensor' stresses coef du_i/dx_k du_j/dx_k
- *     (src/sfsmodel/sfsmodel_gradient.py:70-148; coef = dx^2/12).
- * cfield: device buffer of pf_step_closure_bytes(g, prec, closure) bytes,
- * 256-byte aligned, owned by the plan, that receives the field each step in
- * the stages' type (double for PF_FP64, float for the mixed forms; the six
- * stresses as consecutive fields FXX,FYY,FZZ,FXY,FXZ,FYZ).  Every step
- * computes what pf_sgs_closure, the FP64 addition of mu, the conversion to
- * the stage type and pf_forward_step with that visc or sfs compute, bit for
- * bit (the mixed forms from a warm start, as pf_step_plan_create). */
-enum { PF_CLOSURE_SMAGORINSKY = 1, PF_CLOSURE_GRADIENT = 2 };
-size_t pf_step_closure_bytes(const pf_grid* g, int prec, int closure);
+ *     (src/sfsmodel/sfsmodel_gradient.py:70-148; coef = dx^2/12);
+ *   PF_CLOSURE_MLP: the tensor-core MLP's six stresses (pf_mlp_scales with
+ *     delta2 = coef = Delta^2, then pf_mlp_closure with wpack and err).
+ * field: device buffer of pf_step_closure_bytes(g, prec, kind) bytes,
+ * 256-byte aligned, owned by the plan.  The field the stages read is in
+ * their type (double for PF_FP64, float for the mixed forms; the stresses as
+ * consecutive fields FXX,FYY,FZZ,FXY,FXZ,FYZ) at byte
+ * pf_step_closure_stage_offset(g, prec, kind) of it; for the MLP the buffer
+ * also holds the scales (2 floats at byte 0) and the six FP64 stresses.
+ * Every step computes what the host-driven closure (pf_sgs_closure; or
+ * pf_mlp_scales and pf_mlp_closure), the FP64 addition of mu, the conversion
+ * to the stage type and pf_forward_step with that visc or sfs compute, bit
+ * for bit (the mixed forms from a warm start, as pf_step_plan_create). */
+enum { PF_CLOSURE_SMAGORINSKY = 1, PF_CLOSURE_GRADIENT = 2, PF_CLOSURE_MLP = 3 };
+typedef struct pf_step_closure {
+    int kind;            /* PF_CLOSURE_* */
+    double coef;
+    const void* wpack;   /* PF_CLOSURE_MLP: as for pf_mlp_closure */
+    int* err;            /* PF_CLOSURE_MLP: as for pf_mlp_closure */
+    void* field;
+    size_t field_bytes;
+} pf_step_closure;
+size_t pf_step_closure_bytes(const pf_grid* g, int prec, int kind);
+size_t pf_step_closure_stage_offset(const pf_grid* g, int prec, int kind);
 int pf_step_plan_create_sfs(const pf_grid* g, int prec, int rk4, double* u,
                             double* v, double* w, double* p, double* DP,
                             double mu, double rho, double dt, double min_res,
-                            int max_it, int closure, double coef, void* cfield,
-                            size_t cfield_bytes, void* ws, size_t ws_bytes,
-                            double* stats, pf_step_plan** plan);
+                            int max_it, const pf_step_closure* closure, void* ws,
+                            size_t ws_bytes, double* stats, pf_step_plan** plan);
 
 /* x-slab decomposition (replaces decomp and communicate_border,
  * src/library/parallel.py:118-414, and comms.parallel_sum / parallel_max,

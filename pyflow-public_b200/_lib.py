@@ -66,6 +66,8 @@ def _load():
         "pf_restart_pack": ([G, P, P, P], I),
         "pf_restart_unpack": ([G, P, P, P], I),
         "pf_mlp_closure": ([G, P, P, P, P, P, P, P, P], I),
+        "pf_mlp_scales_workspace_bytes": ([], S),
+        "pf_mlp_scales": ([G, P, P, P, D, P, P, S, P], I),
         "pf_mlsrc_pack_bytes": ([], S),
         "pf_mlsrc_workspace_bytes": ([G], S),
         "pf_mlsrc_pack": ([ctypes.POINTER(ctypes.c_void_p), P, P], I),

@@ -181,35 +181,42 @@ int pf_step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* 
         return PF_ERR_BAD_ARG;
     void* h = nullptr;
     const int rc = step_plan_create(g, prec, rk4, u, v, w, p, DP, mu, rho, dt, min_res, max_it,
-                                    0, 0.0, nullptr, ws, stats, &h);
+                                    nullptr, ws, stats, &h);
     if (rc == PF_OK) *plan = (pf_step_plan*)h;
     return rc;
 }
 
-size_t pf_step_closure_bytes(const pf_grid* g, int prec, int closure) {
-    if (!grid_ok(g) || !prec_ok(prec) || (closure != PF_CLOSURE_SMAGORINSKY &&
-                                          closure != PF_CLOSURE_GRADIENT))
-        return 0;
-    const size_t n = (size_t)g->nx * g->ny * g->nz;
-    const size_t fields = closure == PF_CLOSURE_SMAGORINSKY ? 1 : 6;
-    return fields * n * (prec == PF_FP64 ? sizeof(double) : sizeof(float));
+static bool closure_kind_ok(int kind) {
+    return kind == PF_CLOSURE_SMAGORINSKY || kind == PF_CLOSURE_GRADIENT || kind == PF_CLOSURE_MLP;
+}
+
+size_t pf_step_closure_bytes(const pf_grid* g, int prec, int kind) {
+    if (!grid_ok(g) || !prec_ok(prec) || !closure_kind_ok(kind)) return 0;
+    return closure_layout(g, prec, kind).bytes;
+}
+
+size_t pf_step_closure_stage_offset(const pf_grid* g, int prec, int kind) {
+    if (!grid_ok(g) || !prec_ok(prec) || !closure_kind_ok(kind)) return 0;
+    return closure_layout(g, prec, kind).stage;
 }
 
 int pf_step_plan_create_sfs(const pf_grid* g, int prec, int rk4, double* u, double* v,
                             double* w, double* p, double* DP, double mu, double rho,
-                            double dt, double min_res, int max_it, int closure,
-                            double coef, void* cfield, size_t cfield_bytes, void* ws,
-                            size_t ws_bytes, double* stats, pf_step_plan** plan) {
+                            double dt, double min_res, int max_it, const pf_step_closure* c,
+                            void* ws, size_t ws_bytes, double* stats, pf_step_plan** plan) {
     if (!grid_ok(g) || !prec_ok(prec) || !u || !v || !w || !p || !DP || !stats || !plan ||
-        !(rho != 0.0) || !(dt != 0.0) || max_it < 1 || !cfield || ((uintptr_t)cfield & 255) ||
-        (closure != PF_CLOSURE_SMAGORINSKY && closure != PF_CLOSURE_GRADIENT) ||
-        cfield_bytes < pf_step_closure_bytes(g, prec, closure))
+        !(rho != 0.0) || !(dt != 0.0) || max_it < 1 || !c || !closure_kind_ok(c->kind) ||
+        !c->field || ((uintptr_t)c->field & 255) ||
+        c->field_bytes < closure_layout(g, prec, c->kind).bytes)
+        return PF_ERR_BAD_ARG;
+    if (c->kind == PF_CLOSURE_MLP &&
+        (!c->wpack || ((uintptr_t)c->wpack & 15) || !c->err || g->nx < 2 || g->ny < 2 || g->nz < 2))
         return PF_ERR_BAD_ARG;
     if (!ws || ws_bytes < step_plan_ws_bytes(g, prec) || ((uintptr_t)ws & 255) != 0)
         return PF_ERR_BAD_ARG;
     void* h = nullptr;
     const int rc = step_plan_create(g, prec, rk4, u, v, w, p, DP, mu, rho, dt, min_res, max_it,
-                                    closure, coef, cfield, ws, stats, &h);
+                                    c, ws, stats, &h);
     if (rc == PF_OK) *plan = (pf_step_plan*)h;
     return rc;
 }

@@ -80,12 +80,32 @@ cudaError_t launch_sgs(const pf_grid* g, int model, const double* u,
                        const double* v, const double* w, double coef,
                        double add, void* out, bool f32, cudaStream_t s);
 
-// closure: 0 none, 1 Smagorinsky (cfield = mu + coef |S|), 2 gradient model
-// (cfield = six stresses), cfield in the stage type of prec
+// the MLP closure's input and output scales (pf_mlp_scales); ws of
+// mlp_scales_ws_bytes(), 256-byte aligned
+size_t mlp_scales_ws_bytes();
+cudaError_t launch_mlp_scales(const pf_grid* g, const double* u, const double* v,
+                              const double* w, double delta2, float* scales, void* ws,
+                              cudaStream_t s);
+cudaError_t launch_to_float(const double* in, float* out, long long n, cudaStream_t s);
+cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
+                       const double* w, const void* wpack, const float* scales,
+                       double* out, int* err, cudaStream_t s);
+cudaError_t mlp_prepare();
+
+// byte layout of a plan's closure buffer (pf_step_closure.field)
+struct ClosureLayout {
+    size_t scratch;    // MLP: scales (2 floats) at 0, the reduction scratch at 256
+    size_t f64;        // MLP: the six FP64 stresses
+    size_t stage;      // the field the stages read (stage type)
+    size_t bytes;      // total
+};
+ClosureLayout closure_layout(const pf_grid* g, int prec, int kind);
+
+// c: NULL for a plan without SFS closure
 int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
                      double* w, double* p, double* DP, double mu, double rho,
-                     double dt, double min_res, int max_it, int closure,
-                     double coef, void* cfield, void* ws, double* stats, void** out);
+                     double dt, double min_res, int max_it, const pf_step_closure* c,
+                     void* ws, double* stats, void** out);
 int step_plan_launch(void* plan, int nsteps, cudaStream_t s);
 int batch_plan_create(int prec, int rk4, const pf_batch_member* m, int count, void* table,
                       void** out);

@@ -376,6 +376,8 @@ static cudaError_t mlp_attrs() {
                                 (int)cudaSharedmemCarveoutMaxShared);
 }
 
+cudaError_t mlp_prepare() { return once_per_context((const void*)&mlp_attrs, &mlp_attrs); }
+
 cudaError_t launch_mlp(const pf_grid* g, const double* u, const double* v,
                        const double* w, const void* wpack, const float* scales,
                        double* out, int* err, cudaStream_t s) {

@@ -1243,14 +1243,54 @@ static void plan_free(StepPlan* plan) {
     delete plan;
 }
 
+ClosureLayout closure_layout(const pf_grid* g, int prec, int kind) {
+    const size_t n = (size_t)g->nx * g->ny * g->nz;
+    const size_t tsz = prec == PF_FP64 ? sizeof(double) : sizeof(float);
+    ClosureLayout L{0, 0, 0, 0};
+    if (kind == PF_CLOSURE_SMAGORINSKY || kind == PF_CLOSURE_GRADIENT) {
+        L.bytes = (kind == PF_CLOSURE_SMAGORINSKY ? 1 : 6) * n * tsz;
+        return L;
+    }
+    // MLP: scales + reduction scratch, the FP64 stresses, their float copy
+    L.f64 = align256(256 + mlp_scales_ws_bytes());
+    L.stage = L.f64;
+    L.bytes = L.f64 + align256(6 * n * sizeof(double));
+    if (prec != PF_FP64) {
+        L.stage = L.bytes;
+        L.bytes += align256(6 * n * sizeof(float));
+    }
+    return L;
+}
+
+// the SFS pre-step of a plan (src/data/domain.py:347-355): the closure's
+// field from the fields the previous step left, in the stages' type
+static cudaError_t enqueue_closure(const pf_grid* g, int prec, const pf_step_closure* c,
+                                   double mu, const double* u, const double* v, const double* w,
+                                   cudaStream_t st) {
+    char* f = (char*)c->field;
+    const bool f32 = prec != PF_FP64;
+    if (c->kind != PF_CLOSURE_MLP)
+        return launch_sgs(g, c->kind - 1, u, v, w, c->coef,
+                          c->kind == PF_CLOSURE_SMAGORINSKY ? mu : 0.0, f, f32, st);
+    const ClosureLayout L = closure_layout(g, prec, c->kind);
+    float* scales = (float*)f;
+    cudaError_t e = launch_mlp_scales(g, u, v, w, c->coef, scales, f + 256, st);
+    if (e != cudaSuccess) return e;
+    e = launch_mlp(g, u, v, w, c->wpack, scales, (double*)(f + L.f64), c->err, st);
+    if (e != cudaSuccess || !f32) return e;
+    const long long n6 = 6LL * g->nx * g->ny * g->nz;
+    return launch_to_float((const double*)(f + L.f64), (float*)(f + L.stage), n6, st);
+}
+
 int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
                      double* w, double* p, double* DP, double mu, double rho,
-                     double dt, double min_res, int max_it, int closure,
-                     double coef, void* cfield, void* ws, double* stats, void** out) {
+                     double dt, double min_res, int max_it, const pf_step_closure* c,
+                     void* ws, double* stats, void** out) {
     PlanLayout P;
     int rc = plan_layout(g, prec, ws, &P);
     if (rc != PF_OK) return rc;
     if (predictor_prepare(prec) != cudaSuccess) return PF_ERR_CUDA;
+    if (c && c->kind == PF_CLOSURE_MLP && mlp_prepare() != cudaSuccess) return PF_ERR_CUDA;
     cudaStream_t cs;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return PF_ERR_CUDA;
     if (P.mg.L) {
@@ -1265,15 +1305,14 @@ int step_plan_create(const pf_grid* g, int prec, int rk4, double* u, double* v,
         if (cudaGraphCreate(&plan->graph, 0) != cudaSuccess) { rc = PF_ERR_CUDA; break; }
         cudaGraph_t G = plan->graph;
         cudaGraphNode_t n0, nend;
-        // the SFS pre-step (src/data/domain.py:347-355) reads the fields the
-        // previous step left; the stages read its field in their own type
-        const void* visc = closure == 1 ? cfield : nullptr;
-        const void* sfs = closure == 2 ? cfield : nullptr;
+        // the SFS pre-step reads the fields the previous step left; the
+        // stages read its field in their own type
+        const void* cf = c ? (const char*)c->field + closure_layout(g, prec, c->kind).stage : nullptr;
+        const void* visc = c && c->kind == PF_CLOSURE_SMAGORINSKY ? cf : nullptr;
+        const void* sfs = c && c->kind != PF_CLOSURE_SMAGORINSKY ? cf : nullptr;
         if ((rc = add_captured(G, cs, [&](cudaStream_t st) {
-                 if (closure) {
-                     const cudaError_t e = launch_sgs(g, closure - 1, u, v, w, coef,
-                                                      closure == 1 ? mu : 0.0, cfield,
-                                                      prec != PF_FP64, st);
+                 if (c) {
+                     const cudaError_t e = enqueue_closure(g, prec, c, mu, u, v, w, st);
                      if (e != cudaSuccess) return e;
                  }
                  return launch_predictor(g, prec, rk4, u, v, w, visc, mu, rho, sfs, dt, P.R, st);

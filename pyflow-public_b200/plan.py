@@ -22,13 +22,22 @@ _lib.pf_step_plan_create.argtypes = [
     ctypes.c_double] * 4 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
                             ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
 _lib.pf_step_plan_create.restype = ctypes.c_int
-_lib.pf_step_closure_bytes.argtypes = [ctypes.POINTER(L.Grid), ctypes.c_int, ctypes.c_int]
-_lib.pf_step_closure_bytes.restype = ctypes.c_size_t
+
+
+class StepClosure(ctypes.Structure):
+    """pf_step_closure (include/pyflow_b200.h)."""
+    _fields_ = [("kind", ctypes.c_int), ("coef", ctypes.c_double), ("wpack", ctypes.c_void_p),
+                ("err", ctypes.c_void_p), ("field", ctypes.c_void_p),
+                ("field_bytes", ctypes.c_size_t)]
+
+
+for _fn in (_lib.pf_step_closure_bytes, _lib.pf_step_closure_stage_offset):
+    _fn.argtypes = [ctypes.POINTER(L.Grid), ctypes.c_int, ctypes.c_int]
+    _fn.restype = ctypes.c_size_t
 _lib.pf_step_plan_create_sfs.argtypes = [
     ctypes.POINTER(L.Grid), ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5 + [
-    ctypes.c_double] * 4 + [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
-                            ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
-                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    ctypes.c_double] * 4 + [ctypes.c_int, ctypes.POINTER(StepClosure), ctypes.c_void_p,
+                            ctypes.c_size_t, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
 _lib.pf_step_plan_create_sfs.restype = ctypes.c_int
 _lib.pf_step_plan_launch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
 _lib.pf_step_plan_launch.restype = ctypes.c_int
@@ -52,21 +61,24 @@ _lib.pf_batch_plan_create.restype = ctypes.c_int
 MAX_BATCH = 64
 
 # SFS closures a plan can evaluate inside its graph (pf_step_plan_create_sfs)
-CLOSURES = {"smagorinsky": 1, "gradient": 2}
+CLOSURES = {"smagorinsky": 1, "gradient": 2, "mlp": 3}
 
 STAT_NAMES = ("max_u", "max_v", "max_w", "tke", "max_div", "max_res",
               "iterations", "status", "total_iterations", "steps")
 
 
 class StepPlan:
-    """One field set's step graph.  ``closure`` ('smagorinsky' or 'gradient',
-    with its ``coef`` as for ops.sgs_closure) adds the SFS pre-step of
-    Domain.forwardStep (src/data/domain.py:347-355) to the graph; its field
+    """One field set's step graph.  ``closure`` adds the SFS pre-step of
+    Domain.forwardStep (src/data/domain.py:347-355) to the graph:
+    'smagorinsky' or 'gradient' with its ``coef`` as for ops.sgs_closure, or
+    'mlp' with coef = Delta^2, the packed network ``wpack`` and an int32
+    error flag ``err`` (sfsmodel_mlp.closure).  The field the stages read
     (the viscosity mu + coef|S|, or the six stresses) is ``self.cfield``, in
     the stages' type."""
 
     def __init__(self, u, v, w, p, DP, spacing, mu, rho, dt, min_res=1e-10,
-                 max_it=20000, prec="fp64", rk4=True, closure=None, coef=0.0):
+                 max_it=20000, prec="fp64", rk4=True, closure=None, coef=0.0, wpack=None,
+                 err=None):
         for t, nm in ((u, "u"), (v, "v"), (w, "w"), (p, "p"), (DP, "DP")):
             ops._check(t, u.shape, torch.float64, nm)
         self.fields = (u, v, w, p, DP)
@@ -80,11 +92,24 @@ class StepPlan:
         self.cfield = None
         if closure is not None:
             kind = CLOSURES[closure]
+            g = ctypes.byref(self.grid)
+            nbytes = _lib.pf_step_closure_bytes(g, pr, kind)
+            off = _lib.pf_step_closure_stage_offset(g, pr, kind)
+            self.cbuf = torch.empty(nbytes, dtype=torch.uint8, device=u.device)
             sdt = torch.float64 if pr == L.PF_FP64 else torch.float32
             shape = tuple(u.shape) if kind == 1 else (6,) + tuple(u.shape)
-            self.cfield = torch.empty(shape, dtype=sdt, device=u.device)
-            assert self.cfield.numel() * self.cfield.element_size() == \
-                _lib.pf_step_closure_bytes(ctypes.byref(self.grid), pr, kind)
+            count = 1
+            for a in shape:
+                count *= a
+            self.cfield = self.cbuf[off:].view(sdt)[:count].view(shape)
+            if kind == 3:
+                self.err = err if err is not None else torch.zeros(1, dtype=torch.int32,
+                                                                   device=u.device)
+                self.wpack = wpack
+            self.closure = StepClosure(kind, float(coef),
+                                       ops._p(wpack) if kind == 3 else None,
+                                       ops._p(self.err) if kind == 3 else None,
+                                       ops._p(self.cbuf), nbytes)
         # the fields must be ready: wait for the stream that produced them
         torch.cuda.current_stream(u.device).synchronize()
         common = (ctypes.byref(self.grid), pr, 1 if rk4 else 0,
@@ -95,8 +120,7 @@ class StepPlan:
             L.check("pf_step_plan_create", _lib.pf_step_plan_create(*common, *tail))
         else:
             L.check("pf_step_plan_create_sfs", _lib.pf_step_plan_create_sfs(
-                *common, kind, float(coef), ops._p(self.cfield),
-                self.cfield.numel() * self.cfield.element_size(), *tail))
+                *common, ctypes.byref(self.closure), *tail))
 
     def launch(self, nsteps=1, stream=None):
         s = stream if stream is not None else torch.cuda.current_stream(self.ws.device)

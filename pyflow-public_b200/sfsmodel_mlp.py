@@ -98,22 +98,35 @@ def reference_forward(grads, params, in_scale, out_scale):
     return (y.to(torch.float64) * out_scale).T.contiguous()
 
 
-def closure(u, v, w, spacing, wpack, delta, out=None, err=None):
+_scales_ws = {}
+
+
+def closure(u, v, w, spacing, wpack, delta, out=None, err=None, grads=False):
     """Run the tensor-core closure; returns (stresses (6,nx,ny,nz) float64,
-    g_rms).  The input normalisation uses the RMS of the nine gradients."""
-    g9 = ops.sgs_closure("gradients", u, v, w, spacing)
-    g2 = torch.mean(g9 * g9)
-    g_rms = torch.sqrt(g2)
-    scales = torch.stack([1.0 / g_rms, (delta * delta) * g2]).to(torch.float32)
+    the nine gradients (9,nx,ny,nz) when ``grads`` else None, scales, err).
+    The input normalisation uses the RMS of the nine gradients: scales =
+    [1/g_rms, delta^2 g_rms^2] from pf_mlp_scales (FP64 mean square in a
+    fixed order, rounded once to float), the same kernel a step plan with
+    this closure runs."""
+    g = ops.grid(u.shape, spacing)
+    dev = u.device
+    ws = _scales_ws.get(dev)
+    if ws is None:
+        ws = torch.empty(L.lib().pf_mlp_scales_workspace_bytes(), dtype=torch.uint8, device=dev)
+        _scales_ws[dev] = ws
+    scales = torch.empty(2, dtype=torch.float32, device=dev)
+    L.check("pf_mlp_scales", L.lib().pf_mlp_scales(
+        ctypes.byref(g), ops._p(u), ops._p(v), ops._p(w), float(delta) * float(delta),
+        ops._p(scales), ops._p(ws), ws.numel(), ops._stream(u)))
     shape = (6,) + tuple(u.shape)
     if out is None or tuple(out.shape) != shape:
-        out = torch.empty(shape, dtype=torch.float64, device=u.device)
+        out = torch.empty(shape, dtype=torch.float64, device=dev)
     if err is None:
-        err = torch.zeros(1, dtype=torch.int32, device=u.device)
-    g = ops.grid(u.shape, spacing)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
     L.check("pf_mlp_closure", L.lib().pf_mlp_closure(
         ctypes.byref(g), ops._p(u), ops._p(v), ops._p(w), ops._p(wpack),
         ops._p(scales), ops._p(out), ops._p(err), ops._stream(u)))
+    g9 = ops.sgs_closure("gradients", u, v, w, spacing) if grads else None
     return out, g9, scales, err
 
 

@@ -84,9 +84,11 @@ def test_step_plan_workspace_sizes():
 
 def test_step_closure_sizes_and_argument_checks():
     """pf_step_closure_bytes: one field (Smagorinsky viscosity) or six
-    (gradient-model stresses) in the stages' type; pf_step_plan_create_sfs
-    rejects an unknown closure, a short or misaligned closure buffer before
-    any CUDA call."""
+    (gradient-model stresses) in the stages' type; for the MLP a scratch of
+    scales and reduction partials, the six FP64 stresses and, for the mixed
+    forms, their float copy, each 256-byte aligned.  pf_step_plan_create_sfs
+    rejects an unknown closure, a short or misaligned closure buffer and an
+    MLP closure without its network before any CUDA call."""
     if not os.path.exists(LIB):
         pytest.skip("library not built")
     lib = ctypes.CDLL(LIB)
@@ -96,30 +98,46 @@ def test_step_closure_sizes_and_argument_checks():
                     ("nz", ctypes.c_int), ("dx", ctypes.c_double),
                     ("dy", ctypes.c_double), ("dz", ctypes.c_double)]
 
-    lib.pf_step_closure_bytes.restype = ctypes.c_size_t
-    lib.pf_step_closure_bytes.argtypes = [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int]
+    class Closure(ctypes.Structure):
+        _fields_ = [("kind", ctypes.c_int), ("coef", ctypes.c_double),
+                    ("wpack", ctypes.c_void_p), ("err", ctypes.c_void_p),
+                    ("field", ctypes.c_void_p), ("field_bytes", ctypes.c_size_t)]
+
+    for fn in (lib.pf_step_closure_bytes, lib.pf_step_closure_stage_offset):
+        fn.restype = ctypes.c_size_t
+        fn.argtypes = [ctypes.POINTER(Grid), ctypes.c_int, ctypes.c_int]
     g = Grid(24, 20, 36, 0.1, 0.1, 0.1)
     n = 24 * 20 * 36
-    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 1) == 8 * n
-    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 2) == 6 * 8 * n
-    assert lib.pf_step_closure_bytes(ctypes.byref(g), 2, 1) == 4 * n
-    assert lib.pf_step_closure_bytes(ctypes.byref(g), 1, 2) == 6 * 4 * n
-    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 3) == 0
-    assert lib.pf_step_closure_bytes(ctypes.byref(g), 0, 0) == 0
+    a256 = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    by = lambda pr, k: lib.pf_step_closure_bytes(ctypes.byref(g), pr, k)  # noqa: E731
+    off = lambda pr, k: lib.pf_step_closure_stage_offset(ctypes.byref(g), pr, k)  # noqa: E731
+    assert by(0, 1) == 8 * n and by(0, 2) == 6 * 8 * n
+    assert by(2, 1) == 4 * n and by(1, 2) == 6 * 4 * n
+    assert off(0, 1) == off(2, 2) == 0
+    scratch = a256(256 + 256 + 1024 * 8)
+    assert off(0, 3) == scratch and by(0, 3) == scratch + a256(48 * n)
+    assert off(2, 3) == scratch + a256(48 * n) and by(2, 3) == off(2, 3) + a256(24 * n)
+    assert by(0, 4) == 0 and by(0, 0) == 0
     P, D, I, S = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_size_t
     lib.pf_step_plan_create_sfs.restype = I
     lib.pf_step_plan_create_sfs.argtypes = [ctypes.POINTER(Grid), I, I] + [P] * 5 + [D] * 4 + [
-        I, I, D, P, S, P, S, P, ctypes.POINTER(P)]
+        I, ctypes.POINTER(Closure), P, S, P, ctypes.POINTER(P)]
     fake = 1 << 20  # never dereferenced: every call below fails its checks first
     h = P(0)
 
-    def create(closure, cfield, cbytes):
+    def create(kind, field, nbytes, wpack=fake, err=fake):
+        c = Closure(kind, 0.001, wpack, err, field, nbytes)
         return lib.pf_step_plan_create_sfs(
             ctypes.byref(g), 0, 1, fake, fake, fake, fake, fake, 0.01, 1.0, 0.001, 1e-10, 100,
-            closure, 0.001, cfield, cbytes, fake, 1 << 30, fake, ctypes.byref(h))
+            ctypes.byref(c), fake, 1 << 30, fake, ctypes.byref(h))
 
-    assert create(3, fake, 6 * 8 * n) == 1
+    assert create(4, fake, 6 * 8 * n) == 1
     assert create(1, fake, 8 * n - 8) == 1
     assert create(1, fake + 16, 8 * n) == 1
     assert create(2, None, 6 * 8 * n) == 1
+    assert create(3, fake, by(0, 3), wpack=None) == 1
+    assert create(3, fake, by(0, 3), err=None) == 1
+    assert create(3, fake, by(0, 3) - 256) == 1
     assert h.value is None
+    lib.pf_mlp_scales_workspace_bytes.restype = S
+    assert lib.pf_mlp_scales_workspace_bytes() == 256 + 1024 * 8

@@ -30,7 +30,7 @@ def test_mlp_closure_matches_bf16_model(shape):
     for k in ("b1", "b2", "b3"):
         params[k] = (0.1 * rng.standard_normal(params[k].shape)).astype(np.float32)
     wpack = torch.as_tensor(M.pack(params)).cuda()
-    out, g9, scales, err = M.closure(u, v, w, sp, wpack, delta=sp[0])
+    out, g9, scales, err = M.closure(u, v, w, sp, wpack, delta=sp[0], grads=True)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     ref = M.reference_forward(g9.reshape(9, -1), params, float(scales[0]),
@@ -59,7 +59,7 @@ def test_mlp_closure_vs_fp64_model(shape):
     for k in ("b1", "b2", "b3"):
         params[k] = (0.1 * rng.standard_normal(params[k].shape)).astype(np.float32)
     wpack = torch.as_tensor(M.pack(params)).cuda()
-    out, g9, scales, err = M.closure(u, v, w, sp, wpack, delta=sp[0])
+    out, g9, scales, err = M.closure(u, v, w, sp, wpack, delta=sp[0], grads=True)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     g2 = torch.mean(g9 * g9)
@@ -95,3 +95,23 @@ def test_mlp_in_rhs_slot_runs():
     assert int(err.item()) == 0
     d = max((a - b).abs().max().item() for a, b in zip(r0, r1))
     assert 0 < d < 1e3
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (12, 20, 9)])
+def test_mlp_scales_match_torch_mean(shape):
+    """pf_mlp_scales (FP64 mean square of the nine gradients in a fixed
+    order) against torch.mean of the gradient fields: the float scales agree
+    to one float rounding."""
+    import pyflow_b200.initial as ic
+    import pyflow_b200.ops as ops
+    import pyflow_b200.sfsmodel_mlp as M
+    sp = tuple(2 * np.pi / n for n in shape)
+    u, v, w = (torch.tensor(a, device="cuda") for a in
+               ic.spectral_velocity(shape, k0=3.0, seed=6))
+    wpack = torch.as_tensor(M.pack(M.xavier_init(1))).cuda()
+    _, _, scales, _ = M.closure(u, v, w, sp, wpack, delta=sp[0])
+    g9 = ops.sgs_closure("gradients", u, v, w, sp)
+    g2 = torch.mean(g9 * g9)
+    want = torch.stack([1.0 / torch.sqrt(g2), (sp[0] * sp[0]) * g2]).to(torch.float32)
+    rel = ((scales.double() - want.double()).abs() / want.double().abs()).max().item()
+    assert rel <= 1.2e-7, rel

@@ -148,27 +148,34 @@ def test_pipeline_matches_plan(prec, nsets):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed_mg"])
-@pytest.mark.parametrize("closure", ["smagorinsky", "gradient"])
+@pytest.mark.parametrize("closure", ["smagorinsky", "gradient", "mlp"])
 def test_plan_sfs_matches_forward_step(prec, closure):
     """A plan with the SFS closure in its graph against the host-driven
     composition of Domain.forwardStep (src/data/domain.py:347-367): the
-    closure by pf_sgs_closure, the FP64 addition of the molecular viscosity
-    (Smagorinsky), the conversion to the mixed forms' FP32 stage type, then
-    pf_forward_step with that visc or sfs.  Bit for bit in FP64; the mixed
-    form to the tolerance of test_plan_matches_forward_step.  The closure
-    field the plan leaves is the one of its last step, bit for bit."""
+    closure by pf_sgs_closure (or pf_mlp_scales + pf_mlp_closure), the FP64
+    addition of the molecular viscosity (Smagorinsky), the conversion to the
+    mixed forms' FP32 stage type, then pf_forward_step with that visc or sfs.
+    Bit for bit in FP64; the mixed form to the tolerance of
+    test_plan_matches_forward_step.  The closure field the plan leaves is
+    the one of its last step, bit for bit."""
     import pyflow_b200.initial as ic
     import pyflow_b200.ops as ops
+    import pyflow_b200.sfsmodel_mlp as M
     from pyflow_b200.plan import StepPlan
     shape = (24, 20, 28)
     sp = tuple(2 * np.pi / n for n in shape)
     f0 = [torch.tensor(a, device="cuda") for a in ic.spectral_velocity(shape, k0=4.0, seed=9)]
     nu, dt, steps = 0.004, 0.004, 4
-    coef = (0.18 * sp[0]) ** 2 if closure == "smagorinsky" else sp[0] ** 2 / 12.0
-    model = "smagorinsky" if closure == "smagorinsky" else "gradient"
+    coef = {"smagorinsky": (0.18 * sp[0]) ** 2, "gradient": sp[0] ** 2 / 12.0,
+            "mlp": sp[0] * sp[0]}[closure]
+    wpack = torch.as_tensor(M.pack(M.xavier_init(1))).cuda() if closure == "mlp" else None
     a = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
     for _ in range(steps):
-        fld = ops.sgs_closure(model, *a[:3], sp, coef=coef)
+        if closure == "mlp":
+            fld, _, _, err = M.closure(*a[:3], sp, wpack, sp[0])
+            assert int(err.item()) == 0
+        else:
+            fld = ops.sgs_closure(closure, *a[:3], sp, coef=coef)
         if closure == "smagorinsky":
             fld = nu + fld
         if prec != "fp64":
@@ -178,11 +185,13 @@ def test_plan_sfs_matches_forward_step(prec, closure):
                                 warm=prec != "fp64", **kw)
     b = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
     plan = StepPlan(*b, sp, nu, 1.0, dt, min_res=1e-10, max_it=5000, prec=prec,
-                    closure=closure, coef=coef)
+                    closure=closure, coef=coef, wpack=wpack)
     plan.launch(steps)
     torch.cuda.synchronize()
     st = plan.stats()
     assert plan.cfield.dtype == fld.dtype and torch.equal(plan.cfield, fld)
+    if closure == "mlp":
+        assert int(plan.err.item()) == 0
     plan.close()
     assert st["status"] == 0 and st["max_res"] <= 1e-10
     assert int(st["iterations"]) == info.iterations
