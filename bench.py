@@ -637,6 +637,68 @@ def les_plan_measurement(torch, dev, n=64, steps=20):
             "graph_cell_steps_per_s": n ** 3 / (graph_ms / 1e3)}
 
 
+def slab_measurement(torch, dev, n=256, steps=2):
+    """The x-slab decomposition on this one GPU (slab.LocalSlabs: the ranks'
+    slabs in one process, exchanges as device copies): FP64 steps of the
+    256^3 decaying-turbulence field (k0 = 4, nu = 0.005, dt = 0.0025) on one
+    and on two slabs, CUDA events around the same number of steps, and the
+    per-kernel roofline of the solve on one slab (launch timings of one more
+    step; algorithmic bytes per interior cell from profiling.bytes_per_cell).
+    Multi-GPU runs are not measured here."""
+    import pyflow_b200.profiling as prof
+    from pyflow_b200.slab import LocalSlabs, SlabDomain
+    f0 = [torch.tensor(x, device=dev) for x in make_fields({"n": n, "k0": 4.0, "seed": 1})]
+    sp = (2 * np.pi / n,) * 3
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"grid": n, "prec": "fp64", "steps": steps, "transport": "LocalSlabs (one GPU)"}
+    import pyflow_b200.ops as ops
+    a = [t.clone() for t in f0] + [torch.zeros_like(f0[0]), torch.zeros_like(f0[0])]
+    ops.forward_step(*a, sp, 0.005, 1.0, 0.0025, min_res=TOL, max_it=MAX_IT)
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    its = sum(ops.forward_step(*a, sp, 0.005, 1.0, 0.0025, min_res=TOL, max_it=MAX_IT).iterations
+              for _ in range(steps))
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    out["single_box"] = {"ms_per_step": ms, "iterations_per_step": its / steps,
+                         "ms_per_iteration": ms / max(1.0, its / steps)}
+    del a
+    for R in (1, 2):
+        D = SlabDomain((n, n, n), sp, 0.005, 1.0, 0.0025, LocalSlabs(R), min_res=TOL,
+                       max_it=MAX_IT, poll=8)
+        D.set_state(*f0)
+        D.forward_step()
+        torch.cuda.synchronize(dev)
+        e0.record(st)
+        its = sum(D.forward_step().iterations for _ in range(steps))
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        out["slabs_%d" % R] = {"ms_per_step": ms, "iterations_per_step": its / steps,
+                               "ms_per_iteration": ms / max(1.0, its / steps)}
+        if R == 1:
+            prof.enable(True)
+            D.forward_step()
+            torch.cuda.synchronize(dev)
+            kt = prof.read()
+            prof.enable(False)
+            peak, src = prof.peaks()
+            kern = {}
+            for name, k in kt.items():
+                b = prof.bytes_per_cell(name)
+                if not name.startswith("slab_") or b is None or not k["launches"]:
+                    continue
+                gbs = b * n ** 3 / (k["ms"] / k["launches"] * 1e-3) / 1e9
+                kern[name] = {"launches": k["launches"], "ms": k["ms"], "GB/s": gbs,
+                              "frac": gbs / peak}
+            out["kernels_one_slab"] = kern
+            out["peak_GBs"], out["peak_source"] = peak, src
+        del D
+    return out
+
+
 def run_serve(a, torch, dev):
     sv = serve_measurement(a, torch, dev)
     line = {"metric": "serve latency p50/p99 (s) and aggregate cell-steps/s",
@@ -708,7 +770,7 @@ def run_b200(a):
         torch.cuda.empty_cache()
 
     roof, ktimes, e2e, mlp, cpu, serve, les = None, {}, None, None, None, None, None
-    mlsrc = les_plan = None
+    mlsrc = les_plan = slab = None
     prof_steps = 2
     if not a.no_extras:
         # per-kernel device time: CUDA events around each launch of the
@@ -745,6 +807,8 @@ def run_b200(a):
             torch.cuda.empty_cache()
             les_plan = les_plan_measurement(torch, dev)
             torch.cuda.empty_cache()
+            slab = slab_measurement(torch, dev)
+            torch.cuda.empty_cache()
             if not a.no_serve and world == 1:
                 serve = serve_measurement(a, torch, dev)
                 torch.cuda.empty_cache()
@@ -776,6 +840,7 @@ def run_b200(a):
             "gpu_launches": int(round(launches_per_step * a.steps)) if launches_per_step else None,
             "clocks": clocks, "mlp_tensor_core": mlp, "ml_source_closure": mlsrc,
             "serve": serve, "les_training": les, "les_step_graph": les_plan,
+            "slab_decomposition": slab,
             "kernels": {k: {"launches": v["launches"], "ms": v["ms"]} for k, v in ktimes.items()},
         }
         print(json.dumps(line), flush=True)

@@ -69,7 +69,11 @@ def bytes_per_cell(name):
         "mixed_b_init": 16, "mixed_update": 20, "mixed_residual": 24,
         "add_inplace": 24, "div_vel": 32, "vel_corr": 56, "stats": 24,
         "laplace_apply": 16, "jacobi_sweep": 24, "jacobi_prep": 24,
-        "jacobi_residual": 16}
+        "jacobi_residual": 16,
+        # x-slab BiCGStab (FP64, per interior cell): 21 field passes per
+        # iteration in the reference's order of operations
+        "slab_pupdate": 32, "slab_apply_p": 24, "slab_supdate": 48,
+        "slab_apply_s": 16, "slab_final": 48, "slab_init": 64, "slab_add": 24}
     return fixed.get(name)
 
 
@@ -196,3 +200,26 @@ def closure_case(kind, n, reps=2, device="cuda"):
         raise ValueError("kind must be 'mlp' or 'source'")
     torch.cuda.synchronize(device)
     return int(err.item())
+
+
+def slab_case(n, slabs=2, steps=1, device="cuda"):
+    """A small seeded case of the x-slab decomposition for profilers (ncu -k
+    regex:slab_): ``steps`` FP64 decomposed steps of the k0 = 4 spectral field
+    on an n^3 grid split into ``slabs`` slabs on one device (slab.LocalSlabs).
+    Returns the last solve's status.  Usage:
+        python -c "import pyflow_b200.profiling as p; p.slab_case(192)"
+    """
+    import numpy as np
+    import torch
+    from . import initial as ic
+    from .slab import LocalSlabs, SlabDomain
+    f = [torch.tensor(a, device=device) for a in
+         ic.spectral_velocity((n, n, n), k0=4.0, seed=1)]
+    D = SlabDomain((n, n, n), (2 * np.pi / n,) * 3, 0.005, 1.0, 0.0025, LocalSlabs(slabs),
+                   min_res=1e-10, max_it=20000, poll=8)
+    D.set_state(*f)
+    info = None
+    for _ in range(steps):
+        info = D.forward_step()
+    torch.cuda.synchronize()
+    return info.status
