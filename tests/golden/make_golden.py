@@ -34,7 +34,8 @@ run_32.npz         PyFlow.run: 32^3 seeded spectral field (k0 = 4, urms = 1),
                    and monitor statistics.
 ml_16.npz          rhs_NavierStokes.evaluate with the reference's 'source' ML
                    closure (sfsmodel_ML, a seeded random network whose
-                   weights are stored in the fixture) on a 16^3 box.
+                   weights are stored in the fixture) on a 16^3 box, and the
+                   closure's inputs as the RHS hands them over (ci).
 finalize_8.npz     sfsmodel_ML.residual_stress.finalize over seven training
                    windows with seeded gradients (gradient averaging over
                    numSumDistr windows, RMSprop, learning-rate schedule).
@@ -310,9 +311,20 @@ def ml_case(out):
     VISC = torch.ones(n + 4, n + 4, n + 4, dtype=torch.float64) * mu
     rhs = ns.velocity.rhs_NavierStokes(d, S.metric, rho, VISC, ml)
     su, sv, sw = (_state(ns, d, a) for a in (u, v, w))
+    # the closure's own inputs: the ghost-padded cell-centre interpolants
+    # (the states' var_i scratch, whose last ghost layer the interpolation
+    # never writes), recorded as the RHS passes them to the model
+    seen = {}
+    update = ml.update
+
+    def record(a, b, c, requires_grad=False):
+        seen["ci"] = np.stack([t.detach().numpy().copy() for t in (a, b, c)])
+        return update(a, b, c, requires_grad)
+
+    ml.update = record
     rhs.evaluate(su, sv, sw)
     res = dict(shape=np.array([n, n, n]), spacing=np.array([S.geo.dx] * 3), u=u, v=v,
-               w=w, mu=mu, rho=rho,
+               w=w, mu=mu, rho=rho, ci=seen["ci"],
                rhs_ml=np.stack([rhs.rhs_u.numpy(), rhs.rhs_v.numpy(), rhs.rhs_w.numpy()]))
     for k, t in ml.model.state_dict().items():
         res["w_" + k] = t.detach().numpy().copy()
