@@ -223,3 +223,30 @@ def slab_case(n, slabs=2, steps=1, device="cuda"):
         info = D.forward_step()
     torch.cuda.synchronize()
     return info.status
+
+
+def graph_steps_case(n=512, steps=2, prec="mixed_mg", device="cuda"):
+    """Graph-replayed steps of the n^3 decaying-turbulence workload (k0 = 8,
+    nu = 0.0012, dt = 0.001, seed 0) for a launch list of the captured path:
+    one warm-up step, then ``steps`` steps inside an NVTX range "timed"
+    (ncu --nvtx --nvtx-include "timed/" ...).  Returns the plan's statistics.
+        python -c "import pyflow_b200.profiling as p; p.graph_steps_case()"
+    """
+    import numpy as np
+    import torch
+    from . import initial as ic
+    from .plan import StepPlan
+    u, v, w = (t.contiguous() for t in
+               ic.spectral_velocity_device((n, n, n), k0=8.0, seed=0, device=device))
+    p, DP = torch.zeros_like(u), torch.zeros_like(u)
+    plan = StepPlan(u, v, w, p, DP, (2 * np.pi / n,) * 3, 0.0012, 1.0, 0.001, min_res=1e-10,
+                    max_it=20000, prec=prec)
+    plan.launch(1)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    plan.launch(steps)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    st = plan.stats()
+    plan.close()
+    return st
