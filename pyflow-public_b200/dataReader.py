@@ -176,3 +176,97 @@ def readNGArestart_device(fName, device, nvar=None, chunk_bytes=CHUNK_BYTES):
             out.append(field)
     main.synchronize()
     return names[:nv], time, out
+
+
+# --------------------------------------------------------------------------
+# One shared restart file for an x-slab decomposition (slab.SlabDomain): the
+# counterpart of the reference's MPI-IO restart path
+# (src/data/dataReader.py:215-390), where every rank writes and reads its own
+# part of one file.  In the file's Fortran order a rank's planes
+# [x0, x0 + nxl) are, for every (j, k), a run of nxl values, so the file's
+# variables are viewed as [nvar][nz][ny][nx] arrays and a rank reads or
+# writes the x range of its slab.
+
+def _fields_view(fName, nx, ny, nz, nvar, mode):
+    return np.memmap(fName, dtype="<f8", mode=mode, offset=32 + 8 * nvar,
+                     shape=(nvar, nz, ny, nx))
+
+
+def slab_block_write(view, var, x0, block):
+    """Store ``block`` ([nz][ny][nxl], file order) as planes x0 .. x0 + nxl
+    of variable ``var``."""
+    view[var, :, :, x0:x0 + block.shape[2]] = block
+
+
+def slab_block_read(view, var, x0, nxl, halo):
+    """Planes x0 - halo .. x0 + nxl + halo (periodic) of variable ``var`` in
+    file order, [nz][ny][nxl + 2 halo]."""
+    nx = view.shape[3]
+    ix = (np.arange(nxl + 2 * halo) + (x0 - halo)) % nx
+    return np.ascontiguousarray(view[var][:, :, ix])
+
+
+def writeNGArestart_slabs(fName, D, names=("U", "V", "W", "P"), dt=0.0, time=0.0,
+                          barrier=None):
+    """Write the fields of a slab.SlabDomain ``D`` into one restart file.
+    Every process holding slabs calls it with the same arguments;
+    ``barrier`` (e.g. torch.distributed.barrier) separates the header from
+    the ranks' writes and ends the call once every rank has written.  Each
+    slab's interior is transposed to the file's order on the device
+    (pf_restart_pack) and written as the runs of its x range."""
+    import torch
+    from . import ops
+    from .slab import HALO
+    L = _lib()
+    nx, ny, nz = D.shape
+    fields = [n.lower() for n in names]
+    first = D.slabs[0].x0 == 0
+    if first:
+        with open(fName, "wb") as f:
+            f.write(_header(nx, ny, nz, list(names), dt, time))
+            f.truncate(32 + 8 * len(names) + 8 * nx * ny * nz * len(names))
+    if barrier is not None:
+        barrier()
+    view = _fields_view(fName, nx, ny, nz, len(names), "r+")
+    for s in D.slabs:
+        g = ops.grid((s.nxl, ny, nz), (1.0, 1.0, 1.0))
+        scratch = torch.empty(s.nxl * ny * nz, dtype=torch.float64, device=s.u.device)
+        for v, name in enumerate(fields):
+            interior = getattr(s, name)[HALO:HALO + s.nxl]
+            L.check("pf_restart_pack", L.lib().pf_restart_pack(
+                ctypes.byref(g), ops._p(interior), ops._p(scratch), ops._stream(interior)))
+            slab_block_write(view, v, s.x0, scratch.cpu().numpy().reshape(nz, ny, s.nxl))
+    view.flush()
+    del view
+    if barrier is not None:
+        barrier()
+
+
+def readNGArestart_slabs(fName, D, names=("U", "V", "W", "P")):
+    """Fill the held slabs of ``D`` (interior and ghost planes) from one
+    restart file: each slab reads the periodic x range of its extended array
+    and transposes it on the device (pf_restart_unpack).  Returns the file's
+    time."""
+    import torch
+    from . import ops
+    from .slab import HALO
+    L = _lib()
+    (nx, ny, nz, nv), dt, time = readNGArestart_dims(fName)
+    if (nx, ny, nz) != tuple(D.shape):
+        raise ValueError("restart grid %s does not match the domain %s" % ((nx, ny, nz), D.shape))
+    file_names = readNGArestart(fName, headerOnly=True)[0]
+    view = _fields_view(fName, nx, ny, nz, nv, "r")
+    h = HALO
+    for s in D.slabs:
+        ne = s.nxl + 2 * h
+        g = ops.grid((ne, ny, nz), (1.0, 1.0, 1.0))
+        for name in names:
+            v = file_names.index(name)
+            block = torch.from_numpy(slab_block_read(view, v, s.x0, s.nxl, h)).to(s.u.device)
+            dst = getattr(s, name.lower())
+            L.check("pf_restart_unpack", L.lib().pf_restart_unpack(
+                ctypes.byref(g), ops._p(block), ops._p(dst), ops._stream(dst)))
+        s.DP.zero_()
+    torch.cuda.synchronize()
+    del view
+    return time

@@ -1,8 +1,9 @@
 """Host logic of the x-slab decomposition (pyflow_b200.slab), on the CPU:
 the plane split against the reference's formula, the periodic extension of
-a global field, and the ghost exchange and gather of both transports --
+a global field, the ghost exchange and gather of both transports --
 LocalSlabs in one process and DistSlabs over gloo with world sizes 2 and 3
--- against the periodic extension.  No kernel runs here."""
+-- against the periodic extension, and one shared restart file written and
+read by the ranks' blocks.  No kernel runs here."""
 import os
 import socket
 
@@ -113,3 +114,69 @@ def test_dist_exchange_and_gather_gloo(world):
         assert p.exitcode == 0
     got = sorted(q.get(timeout=5) for _ in range(world))
     assert got == [(r, True, True) for r in range(world)]
+
+
+def _io_worker(rank, world, port, path, q):
+    """Each rank writes its slab's block of two variables into one shared
+    restart file (file order computed on the host here, as the device
+    transpose gives it), then reads its extended block back."""
+    import numpy as np
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import pyflow_b200.dataReader as R
+        from pyflow_b200.slab import HALO, plane_ranges
+        nx, ny, nz = 4 * world + 5, 3, 4
+        glob = [np.arange(nx * ny * nz, dtype=np.float64).reshape(nx, ny, nz) * (v + 1)
+                for v in range(2)]
+        x0, nxl = plane_ranges(nx, world)[rank]
+        if rank == 0:
+            with open(path, "wb") as f:
+                f.write(R._header(nx, ny, nz, ["U", "V"], 0.1, 2.5))
+                f.truncate(32 + 16 + 2 * 8 * nx * ny * nz)
+        dist.barrier()
+        view = R._fields_view(path, nx, ny, nz, 2, "r+")
+        for v in range(2):
+            block = np.ascontiguousarray(glob[v][x0:x0 + nxl].transpose(2, 1, 0))
+            R.slab_block_write(view, v, x0, block)
+        view.flush()
+        del view
+        dist.barrier()
+        view = R._fields_view(path, nx, ny, nz, 2, "r")
+        ok = True
+        for v in range(2):
+            got = R.slab_block_read(view, v, x0, nxl, HALO).transpose(2, 1, 0)
+            want = np.pad(glob[v], ((HALO, HALO), (0, 0), (0, 0)), mode="wrap")[
+                x0:x0 + nxl + 2 * HALO]
+            ok = ok and np.array_equal(got, want)
+        q.put((rank, bool(ok)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_restart_shared_file_gloo(world, tmp_path):
+    """One restart file written by every rank's block (the layout of the
+    reference's MPI-IO restart path) reads back with the serial reader, and
+    each rank's periodic extended block reads back from it."""
+    import numpy as np
+    import pyflow_b200.dataReader as R
+    path = str(tmp_path / "restart")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_io_worker, args=(r, world, port, path, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(150)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=5) for _ in range(world))
+    assert got == [(r, True) for r in range(world)]
+    names, time, data = R.readNGArestart(path, headerOnly=False)
+    nx = 4 * world + 5
+    assert names == ["U", "V"] and time == 2.5
+    for v in range(2):
+        want = np.arange(nx * 3 * 4, dtype=np.float64).reshape(nx, 3, 4) * (v + 1)
+        assert np.array_equal(data[..., v], want)
