@@ -141,3 +141,45 @@ def test_step_closure_sizes_and_argument_checks():
     assert h.value is None
     lib.pf_mlp_scales_workspace_bytes.restype = S
     assert lib.pf_mlp_scales_workspace_bytes() == 256 + 1024 * 8
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes structures the Python side passes across the ABI have the
+    C compiler's layout of the header's structs (size and every field
+    offset): pf_grid, pf_solve_info, pf_step_closure, pf_batch_member."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    fields = {
+        "pf_grid": ["nx", "ny", "nz", "dx", "dy", "dz"],
+        "pf_solve_info": ["max_res", "iterations", "outer", "status"],
+        "pf_step_closure": ["kind", "coef", "wpack", "err", "field", "field_bytes"],
+        "pf_batch_member": ["grid", "u", "v", "w", "p", "DP", "mu", "rho", "dt", "min_res",
+                            "max_it", "fresh", "ws", "ws_bytes", "stats"],
+    }
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "pyflow_b200.h"',
+             "int main(void) {"]
+    for st, fs in fields.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (st, st))
+        for f in fs:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (st, f, st, f))
+    lines.append("return 0; }")
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    got = {tuple(ln.split()[:2]): int(ln.split()[2]) for ln in out.splitlines()}
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    import pyflow_b200._lib as L
+    from pyflow_b200.plan import BatchMember, StepClosure
+    py = {"pf_grid": L.Grid, "pf_solve_info": L.SolveInfo, "pf_step_closure": StepClosure,
+          "pf_batch_member": BatchMember}
+    for st, cls in py.items():
+        assert ctypes.sizeof(cls) == got[(st, "size")], st
+        for f in fields[st]:
+            assert getattr(cls, f).offset == got[(st, f)], (st, f)
