@@ -183,3 +183,59 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert ctypes.sizeof(cls) == got[(st, "size")], st
         for f in fields[st]:
             assert getattr(cls, f).offset == got[(st, f)], (st, f)
+
+
+def _c_args(decl):
+    """Argument types of a prototype's parameter list, as (kind, stars,
+    base type) with kind 'ptr', 'int', 'double', 'size_t' or 'void'."""
+    decl = decl.strip()
+    if decl in ("", "void"):
+        return []
+    out = []
+    for a in decl.split(","):
+        toks = a.replace("*", " * ").split()
+        stars = toks.count("*")
+        base = [t for t in toks[:-1] if t not in ("const", "*")]
+        base = base[0] if base else ""
+        if stars:
+            out.append(("ptr", stars, base))
+        else:
+            out.append(({"int": "int", "double": "double", "size_t": "size_t"}.get(base, base),
+                        0, base))
+    return out
+
+
+def test_python_signatures_match_the_header():
+    """Every entry point the Python side registers (argtypes / restype) has
+    the header's parameter count and scalar types; pointer parameters are
+    passed as pointers."""
+    if not os.path.exists(LIB):
+        pytest.skip("library not built")
+    import pyflow_b200._lib as L
+    import pyflow_b200.plan  # noqa: F401  (registers the plan entry points)
+    import pyflow_b200.profiling  # noqa: F401
+    import pyflow_b200.slab  # noqa: F401
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    protos = re.findall(r"([A-Za-z_][\w\s\*]*?)\s*\b(pf_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src)
+    lib = L.lib()
+    scalar = {"int": ctypes.c_int, "double": ctypes.c_double, "size_t": ctypes.c_size_t}
+    checked = 0
+    for ret, name, args in protos:
+        fn = getattr(lib, name)
+        if fn.argtypes is None:
+            continue
+        want = _c_args(args)
+        assert len(fn.argtypes) == len(want), name
+        for i, ((kind, stars, base), got) in enumerate(zip(want, fn.argtypes)):
+            if kind == "ptr":
+                assert got in (ctypes.c_void_p, ctypes.c_char_p) or hasattr(got, "_type_") \
+                    and not isinstance(got._type_, str), (name, i, base)
+            else:
+                assert got is scalar[kind], (name, i, base, got)
+        r = ret.replace("const", "").split()
+        if "*" in ret:
+            assert fn.restype in (ctypes.c_char_p, ctypes.c_void_p), name
+        elif r and r[-1] in scalar:
+            assert fn.restype is scalar[r[-1]], (name, fn.restype)
+        checked += 1
+    assert checked >= 30, checked
