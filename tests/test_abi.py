@@ -212,6 +212,7 @@ def test_python_signatures_match_the_header():
     if not os.path.exists(LIB):
         pytest.skip("library not built")
     import pyflow_b200._lib as L
+    import pyflow_b200.adjoint  # noqa: F401  (registers the adjoint entry points)
     import pyflow_b200.plan  # noqa: F401  (registers the plan entry points)
     import pyflow_b200.profiling  # noqa: F401
     import pyflow_b200.slab  # noqa: F401
