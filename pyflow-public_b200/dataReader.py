@@ -209,9 +209,10 @@ def slab_block_read(view, var, x0, nxl, halo):
 def writeNGArestart_slabs(fName, D, names=("U", "V", "W", "P"), dt=0.0, time=0.0,
                           barrier=None):
     """Write the fields of a slab.SlabDomain ``D`` into one restart file.
-    Every process holding slabs calls it with the same arguments;
-    ``barrier`` (e.g. torch.distributed.barrier) separates the header from
-    the ranks' writes and ends the call once every rank has written.  Each
+    Every process holding slabs calls it with the same arguments; a
+    barrier separates the header from the ranks' writes and ends the call
+    once every rank has written (``barrier``; by default the process group's
+    barrier when the slabs are spread over processes).  Each
     slab's interior is transposed to the file's order on the device
     (pf_restart_pack) and written as the runs of its x range."""
     import torch
@@ -220,6 +221,10 @@ def writeNGArestart_slabs(fName, D, names=("U", "V", "W", "P"), dt=0.0, time=0.0
     L = _lib()
     nx, ny, nz = D.shape
     fields = [n.lower() for n in names]
+    if barrier is None and len(D.slabs) < D.T.size:
+        import torch.distributed as dist
+        group = getattr(D.T, "group", None)
+        barrier = lambda: dist.barrier(group)  # noqa: E731
     first = D.slabs[0].x0 == 0
     if first:
         with open(fName, "wb") as f:
